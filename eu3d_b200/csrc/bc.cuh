@@ -1,0 +1,255 @@
+// Ghost-cell fills and the CFL time step.
+//
+// Reference: Flowfield::FieldBoundary_3dRSBI (src/Flowfield.cpp:559-773),
+// FieldBoundary_3dODM (:378-558), Flowfield::CFLcondition (:242-272).
+// The faces are filled in the reference's order -- x, then y over every i
+// (x ghosts included), then z over every i, j -- one launch per direction so
+// that each launch reads only cells the previous launches have finished.
+#pragma once
+
+#include "common.cuh"
+
+namespace eu3d {
+
+struct GhostArgs {
+    Layout L;
+    double *T, *E;
+    const double *inflow;  // ODM planes: U V W P D T H E G, then NS species planes, each nj*nk
+    int kind;
+};
+
+template <class P>
+__device__ __forceinline__ void ghost_copy(const GhostArgs &a, P *q, long long d, long long s)
+{
+    const long long fs = a.L.fs;
+#pragma unroll
+    for (int f = 0; f < NPRIM; f++) q[f * fs + d] = q[f * fs + s];
+    a.T[d] = a.T[s];
+    a.E[d] = a.E[s];
+}
+
+// mirror with the wall-side thermodynamic recompute of the reflective faces
+// (src/Flowfield.cpp:409-436 pattern): D from P/(T Rgas), H, E, Gamma from T
+template <class P>
+__device__ __forceinline__ void ghost_wall(const GhostArgs &a, P *q, long long d, long long s, bool flipv, bool flipw)
+{
+    const long long fs = a.L.fs;
+    q[PU * fs + d] = q[PU * fs + s];
+    q[PV * fs + d] = flipv ? -q[PV * fs + s] : q[PV * fs + s];
+    q[PW * fs + d] = flipw ? -q[PW * fs + s] : q[PW * fs + s];
+    const P Pp = q[PP * fs + s];
+    q[PP * fs + d] = Pp;
+    const double T = a.T[s];
+    a.T[d] = T;
+    const TPow p = tpow(T);
+    double Y[NS], rg = 0.0, cp = 0.0, h = 0.0, e = 0.0;
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) {
+        Y[sp] = (double)q[(PY + sp) * fs + s];
+        q[(PY + sp) * fs + d] = q[(PY + sp) * fs + s];
+    }
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) {
+        const double cpi = cM.ri[sp] * cp_r(sp, p);
+        const double hi = cM.ri[sp] * h_r(sp, p);
+        const double ei = hi - cM.ri[sp] * T;
+        rg += Y[sp] * cM.ri[sp];
+        cp += cpi * Y[sp];
+        h += Y[sp] * hi;
+        e += Y[sp] * ei;
+    }
+    const double Rgas = rg * 1000;
+    const double Cp = cp * 1000;
+    q[PD * fs + d] = (P)((double)Pp / (T * Rgas));
+    q[PH * fs + d] = (P)(h * 1000);
+    a.E[d] = e * 1000;
+    q[PG * fs + d] = (P)(Cp / (Cp - Rgas));
+}
+
+// x faces: i in [0, bc) and [ni+bc, ni+2bc), j, k interior
+template <class P>
+__global__ void k_ghost_x(GhostArgs a, P *q)
+{
+    const Layout &L = a.L;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = 2 * L.bc;
+    const int n = g * L.nj * L.nk;
+    if (t >= n) return;
+    const int gi = t % g, j = L.bc + (t / g) % L.nj, k = L.bc + t / (g * L.nj);
+    const bool lower = gi < L.bc;
+    const int i = lower ? gi : L.ni + L.bc + (gi - L.bc);
+    const long long d = L.at(i, j, k);
+    if (a.kind == EU3D_BC_RSBI) {
+        const int si = lower ? 2 * L.bc - 1 - i : 2 * (L.ni + L.bc) - 1 - i;
+        ghost_copy(a, q, d, L.at(si, j, k));
+    } else if (a.kind == EU3D_BC_TRANSMISSIVE) {
+        const int si = lower ? L.bc : L.ni + L.bc - 1;
+        ghost_copy(a, q, d, L.at(si, j, k));
+    } else if (a.kind == EU3D_BC_ODM) {
+        if (lower) {
+            const long long p = (long long)(j - L.bc) * L.nk + (k - L.bc), pl = (long long)L.nj * L.nk;
+            const long long fs = L.fs;
+            q[PU * fs + d] = (P)a.inflow[0 * pl + p];
+            q[PV * fs + d] = (P)a.inflow[1 * pl + p];
+            q[PW * fs + d] = (P)a.inflow[2 * pl + p];
+            q[PP * fs + d] = (P)a.inflow[3 * pl + p];
+            q[PD * fs + d] = (P)a.inflow[4 * pl + p];
+            a.T[d] = a.inflow[5 * pl + p];
+            q[PH * fs + d] = (P)a.inflow[6 * pl + p];
+            a.E[d] = a.inflow[7 * pl + p];
+            q[PG * fs + d] = (P)a.inflow[8 * pl + p];
+#pragma unroll
+            for (int s = 0; s < NS; s++) q[(PY + s) * fs + d] = (P)a.inflow[(9 + s) * pl + p];
+        } else {
+            ghost_wall(a, q, d, L.at(2 * (L.ni + L.bc) - 1 - i, j, k), false, false);
+        }
+    }
+}
+
+// y faces: every i, j in the ghost rows, k interior
+template <class P>
+__global__ void k_ghost_y(GhostArgs a, P *q)
+{
+    const Layout &L = a.L;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = 2 * L.bc;
+    const int n = L.NI * g * L.nk;
+    if (t >= n) return;
+    const int i = t % L.NI, gj = (t / L.NI) % g, k = L.bc + t / (L.NI * g);
+    const bool lower = gj < L.bc;
+    const int j = lower ? gj : L.nj + L.bc + (gj - L.bc);
+    const long long d = L.at(i, j, k);
+    const int sj = lower ? 2 * L.bc - 1 - j : 2 * (L.nj + L.bc) - 1 - j;
+    if (a.kind == EU3D_BC_RSBI) {
+        if (lower)
+            ghost_wall(a, q, d, L.at(i, sj, k), false, false);
+        else
+            ghost_copy(a, q, d, L.at(i, sj, k));
+    } else if (a.kind == EU3D_BC_TRANSMISSIVE) {
+        ghost_copy(a, q, d, L.at(i, sj, k));
+    } else if (a.kind == EU3D_BC_ODM) {
+        if (lower)
+            ghost_wall(a, q, d, L.at(i, sj, k), true, false);
+        else
+            ghost_copy(a, q, d, L.at(i, sj, k));
+    }
+}
+
+// z faces: every i, j, k in the ghost planes
+template <class P>
+__global__ void k_ghost_z(GhostArgs a, P *q)
+{
+    const Layout &L = a.L;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = 2 * L.bc;
+    const int n = L.NI * L.NJ * g;
+    if (t >= n) return;
+    const int i = t % L.NI, j = (t / L.NI) % L.NJ, gk = t / (L.NI * L.NJ);
+    const bool lower = gk < L.bc;
+    const int k = lower ? gk : L.nk + L.bc + (gk - L.bc);
+    const long long d = L.at(i, j, k);
+    const int sk = lower ? 2 * L.bc - 1 - k : 2 * (L.nk + L.bc) - 1 - k;
+    if (a.kind == EU3D_BC_ODM)
+        ghost_wall(a, q, d, L.at(i, j, sk), false, true);
+    else
+        ghost_copy(a, q, d, L.at(i, j, sk));
+}
+
+// Wedge immersed boundary (new): solid cells take the state of the fluid
+// cell nearest to their mirror image across the wedge surface, with the
+// velocity reflected about the surface.  Only solid cells are written and
+// only fluid cells are read.
+template <class P>
+__global__ void k_wedge(GhostArgs a, P *q, const double *xn, const double *yn, double x0, double y0, double tn)
+{
+    const Layout &L = a.L;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= L.NI) return;
+    const double x = xn[i], y = yn[j];
+    if (!(x > x0 && (y - y0) < (x - x0) * tn)) return;
+    const double cs = 1.0 / sqrt(1.0 + tn * tn), sn = tn * cs;
+    const double nx = -sn, ny = cs;
+    const double dx = xn[L.bc + 1] - xn[L.bc], dy = yn[L.bc + 1] - yn[L.bc];
+    const double dist = (x - x0) * sn - (y - y0) * cs;
+    const double xi = x + 2.0 * dist * nx, yi = y + 2.0 * dist * ny;
+    int si = (int)floor((xi - xn[0]) / dx + 0.5);
+    int sj = (int)floor((yi - yn[0]) / dy + 0.5);
+    si = si < 0 ? 0 : (si > L.NI - 1 ? L.NI - 1 : si);
+    sj = sj < 0 ? 0 : (sj > L.NJ - 1 ? L.NJ - 1 : sj);
+    while (sj < L.NJ - 1 && xn[si] > x0 && (yn[sj] - y0) < (xn[si] - x0) * tn) sj++;
+    const long long fs = L.fs;
+    for (int k = 0; k < L.NK; k++) {
+        const long long d = L.at(i, j, k), s = L.at(si, sj, k);
+        ghost_copy(a, q, d, s);
+        const double u = (double)q[PU * fs + s], v = (double)q[PV * fs + s];
+        const double un = u * nx + v * ny;
+        q[PU * fs + d] = (P)(u - 2.0 * un * nx);
+        q[PV * fs + d] = (P)(v - 2.0 * un * ny);
+    }
+}
+
+// CFL: block minima of min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C)]) over the
+// interior (solid wedge cells excluded), C = sqrt(Gamma P / D) as the decode
+// defines it.
+template <class P>
+__global__ void k_cfl_partial(Layout L, const P *__restrict__ q, double dx, double dy, double dz, int use_z,
+                              const double *xn, const double *yn, double x0, double y0, double tn, int wedge_on,
+                              double *partial)
+{
+    const long long n = L.interior_cells();
+    double m = 1e10;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = L.bc + (int)(t % L.ni);
+        const int j = L.bc + (int)((t / L.ni) % L.nj);
+        const int k = L.bc + (int)(t / ((long long)L.ni * L.nj));
+        if (wedge_on) {
+            const double x = xn[i], y = yn[j];
+            if (x > x0 && (y - y0) < (x - x0) * tn) continue;
+        }
+        const long long c = L.at(i, j, k);
+        const long long fs = L.fs;
+        const double D = (double)q[PD * fs + c], Pp = (double)q[PP * fs + c], G = (double)q[PG * fs + c];
+        const double C = sqrt(G * Pp / D);
+        const double a = dx / (fabs((double)q[PU * fs + c]) + C), b = dy / (fabs((double)q[PV * fs + c]) + C);
+        double tmp = (b < a) ? b : a;
+        if (use_z) {
+            const double z = dz / (fabs((double)q[PW * fs + c]) + C);
+            tmp = (z < tmp) ? z : tmp;
+        }
+        if (tmp < m) m = tmp;
+    }
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
+        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    }
+}
+
+// dt = cfl * min, clipped so that time + dt does not pass final_time;
+// time += dt (src/Flowfield.cpp:258-271).  scal[0] = dt, scal[1] = time.
+__global__ void k_cfl_final(const double *partial, int nparts, double cfl, double final_time, double *scal)
+{
+    double m = 1e10;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) m = fmin(m, partial[t]);
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
+        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) {
+            double dt = cfl * m;
+            if (scal[1] + dt > final_time) dt = final_time - scal[1];
+            scal[0] = dt;
+            scal[1] += dt;
+        }
+    }
+}
+
+}  // namespace eu3d

@@ -1,0 +1,438 @@
+// Per-cell FP64 kernels: conservative -> primitive decode with the Newton
+// temperature inversion, IMEX diagonal chemistry, point-implicit trapezoid
+// chemistry (field form and adaptive substeps), each fused with the state
+// update that precedes it and the decode that follows it.
+#pragma once
+
+#include "common.cuh"
+
+namespace eu3d {
+
+constexpr int NCHEM_CAP = 1 << 20;  // adaptive substeps per cell per step
+
+struct Decoded {
+    double D, U, V, W, E, T, P, H, G, Cp, Rgas;
+    double Y[NS];
+};
+
+// Flowfield::Update_after_CS per cell (src/Flowfield.cpp:1246-1284) with
+// Flowfield::Get_temp (:1542-1566).  Eold is the E of the previous decode
+// (the Newton target under EU3D_Q_STALE_E); T0 the Newton start.
+__device__ __forceinline__ void decode(const double cs[NV], double T0, double Eold, Decoded &o, int &capped)
+{
+    double D = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) D += cs[s];
+#pragma unroll
+    for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
+    const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
+    const double Enew = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) / D;
+    const double Et = (cM.quirks & EU3D_Q_STALE_E) ? Eold : Enew;
+    double sYR = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) sYR += o.Y[s] * cM.ri[s];
+    double Tn = T0, Tp;
+    int count = 0;
+    while (count < 10) {
+        Tp = Tn;
+        const TPow p = tpow(Tp);
+        double sh = 0.0, scp = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            sh += o.Y[s] * (cM.ri[s] * h_r(s, p));
+            scp += o.Y[s] * (cM.ri[s] * cp_r(s, p));
+        }
+        const double t1 = (sh - Et * 1e-3) - sYR * Tp;
+        const double t2 = scp - sYR;
+        Tn = Tp - t1 / t2;
+        if (fabs(Tn - Tp) < 1e-6) break;
+        count++;
+    }
+    capped = count >= 10;
+    const TPow p = tpow(Tn);
+    double sdiv = 0.0, scp = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        sdiv += o.Y[s] / cM.mw[s];
+        scp += (cM.ri[s] * cp_r(s, p)) * o.Y[s];
+    }
+    const double Wav = 1.0 / sdiv;
+    o.Rgas = R_GAS * 1000 / Wav;
+    o.P = Tn * D * o.Rgas;
+    o.H = o.P / D + Enew;
+    o.Cp = scp * 1000;
+    o.G = o.Cp / (o.Cp - R_GAS * sdiv * 1000);
+    o.D = D;
+    o.U = U;
+    o.V = V;
+    o.W = W;
+    o.E = Enew;
+    o.T = Tn;
+}
+
+template <class P>
+__device__ __forceinline__ void store_prims(const Decoded &o, P *__restrict__ q, long long fs, long long c)
+{
+    q[PD * fs + c] = (P)o.D;
+    q[PU * fs + c] = (P)o.U;
+    q[PV * fs + c] = (P)o.V;
+    q[PW * fs + c] = (P)o.W;
+    q[PP * fs + c] = (P)o.P;
+    q[PH * fs + c] = (P)o.H;
+    q[PG * fs + c] = (P)o.G;
+#pragma unroll
+    for (int s = 0; s < NS; s++) q[(PY + s) * fs + c] = (P)o.Y[s];
+}
+
+// pow(Mc, nu) for the stoichiometric exponents 0, 1, 2 (validated on the
+// host); pow(x, 2) in the reference is the correctly rounded x * x.
+__device__ __forceinline__ double mcpow(double x, double nu)
+{
+    return nu == 0.0 ? 1.0 : (nu == 1.0 ? x : (nu == 2.0 ? x * x : pow(x, nu)));
+}
+
+__device__ __forceinline__ double powT(const TPow &p, double b)
+{
+    return b == 0.0 ? 1.0 : (b == 1.0 ? p.T : pow(p.T, b));
+}
+
+// Reaction-rate quantities of one reaction (src/Reaction.cpp:755-775).
+struct Rxn {
+    double KF, KB, RRF, RRB, RTB, RR;
+};
+
+// rtb_mode: 0 = R_TB defaults to 1 when its sum is 0 (Diagonalized),
+// 1 = left at 0 (field Trapezoid), 2 = every R_TB set to 0 (adaptive).
+__device__ __forceinline__ Rxn rxn(int r, const TPow &p, const double Mc[NS], const double G[NS], int rtb_mode)
+{
+    Rxn x;
+    const double T = p.T;
+    x.KF = cM.af[r] * powT(p, cM.bf[r]) * exp(-cM.eaf[r] / (RU_CAL * T));
+    double dg = 0.0, rf = 1.0, rb = 1.0, tb = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        dg += cM.nu[s][r] * G[s];
+        rf *= mcpow(Mc[s], cM.sf[s][r]);
+        rb *= mcpow(Mc[s], cM.sb[s][r]);
+        tb += Mc[s] * cM.tb[s][r];
+    }
+    const double Kp = exp(-dg / (R_GAS * T)) * cM.p0xr[r];
+    const double xr = cM.xr[r];
+    const double RT = R_GAS * T;
+    const double Kc = Kp * (xr == 0.0 ? 1.0 : (xr == 1.0 ? 1.0 / RT : (xr == -1.0 ? RT : pow(RT, -xr))));
+    x.KB = x.KF / Kc;
+    if (rtb_mode == 0) {
+        if (tb == 0.0) tb = 1.0;
+    } else if (rtb_mode == 2) {
+        tb = 0.0;
+    }
+    x.RRF = rf;
+    x.RRB = rb;
+    x.RTB = tb;
+    x.RR = x.KF * rf - x.KB * rb;
+    return x;
+}
+
+// Gibbs energies G_s = H_s - S_s T in J/mol at one temperature
+__device__ __forceinline__ void gibbs(const TPow &p, double G[NS])
+{
+#pragma unroll
+    for (int s = 0; s < NS; s++) G[s] = R_GAS * h_r(s, p) - (R_GAS * s_r(s, p)) * p.T;
+}
+
+// Reaction::Diagonalized per cell (src/Reaction.cpp:736-811): source CMS and
+// diagonal Jacobian MD of the partial densities.  Mc in mol/cm^3, Di in g/cm^3.
+__device__ __forceinline__ void diagonalized(const TPow &p, const double Mc[NS], const double Di[NS], const double PT[NS],
+                                             double CMS[NS], double MD[NS])
+{
+    double G[NS], Wi[NS];
+    gibbs(p, G);
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Wi[s] = 0.0;
+        MD[s] = 0.0;
+    }
+    const double T = p.T;
+#pragma unroll 1
+    for (int r = 0; r < NR; r++) {
+        const Rxn x = rxn(r, p, Mc, G, 0);
+        const double wjh2 = x.RR * (cM.bf[r] / T + cM.eaf[r] / (RU_CAL * (T * T)));
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const double nu = cM.nu[s][r];
+            Wi[s] += nu * x.RTB * x.RR;
+            const double wjh1 =
+                (Di[s] == 0) ? 0.0 : x.KF * cM.sf[s][r] * x.RRF / Di[s] - x.KB * cM.sb[s][r] * x.RRB / Di[s];
+            MD[s] += nu * ((wjh1 + wjh2 * PT[s]) * x.RTB + x.RR * cM.tb[s][r] / cM.mw[s]);
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        CMS[s] = (cM.mw[s] * Wi[s]) * 1e3;
+        MD[s] = cM.mw[s] * MD[s];
+    }
+}
+
+// Point-implicit trapezoid update of one cell (src/Reaction.cpp:412-485,
+// :489-591): Di in kg/m^3 in and out.  Wi (net production, g/cm^3/s) is
+// returned for the substep prediction.
+__device__ __forceinline__ void trapezoid(const TPow &p, const double cs_di[NS], double dt, int rtb_mode, double out[NS],
+                                          double Wi[NS])
+{
+    double Mc[NS], Di[NS], G[NS], Pv[NS], Qv[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Di[s] = cs_di[s] * 1e-3;
+        Mc[s] = (cs_di[s] / cM.mw[s] * 1000) * 1e-6;
+        Pv[s] = 0.0;
+        Qv[s] = 0.0;
+        Wi[s] = 0.0;
+    }
+    gibbs(p, G);
+#pragma unroll 1
+    for (int r = 0; r < NR; r++) {
+        const Rxn x = rxn(r, p, Mc, G, rtb_mode);
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
+            Qv[s] += (cM.sb[s][r] * x.KF * x.RRF + cM.sf[s][r] * x.KB * x.RRB * x.RTB);
+            Pv[s] += (cM.sb[s][r] * x.KB * x.RRB + cM.sf[s][r] * x.KF * x.RRF * x.RTB);
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Wi[s] = cM.mw[s] * Wi[s];
+        const double q = cM.mw[s] * Qv[s];
+        const double pp = (Mc[s] == 0) ? 0.0 : Pv[s] / Mc[s];
+        out[s] = ((1.0 - dt / 2.0 * pp) * Di[s] + dt * q) / (1.0 + dt / 2.0 * pp) * 1e3;
+    }
+}
+
+// Reaction::TrapezoidPrediction per cell (src/Reaction.cpp:593-670)
+__device__ __forceinline__ int predict_nchem(const TPow &p, const double cs_di[NS], const double Y[NS], double dtm,
+                                             int rtb_mode)
+{
+    double Mc[NS], G[NS], Wi[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Mc[s] = (cs_di[s] / cM.mw[s] * 1000) * 1e-6;
+        Wi[s] = 0.0;
+    }
+    gibbs(p, G);
+#pragma unroll 1
+    for (int r = 0; r < NR; r++) {
+        const Rxn x = rxn(r, p, Mc, G, rtb_mode);
+#pragma unroll
+        for (int s = 0; s < NS; s++) Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
+    }
+    double dt = dtm;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double w = cM.mw[s] * Wi[s];
+        if (Y[s] >= 1e-6 && w != 0) {
+            const double t = fabs(-(cs_di[s] * 1e-3) / w);
+            if (t < dt) dt = t;
+        }
+    }
+    const double n = ceil(dtm / dt);
+    if (!(n >= 1.0)) return 1;
+    return n > (double)NCHEM_CAP ? NCHEM_CAP + 1 : (int)n;
+}
+
+__device__ __forceinline__ void load_cs(const double *__restrict__ cs, long long fs, long long c, double v[NV])
+{
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = cs[q * fs + c];
+}
+
+__device__ __forceinline__ void store_cs(double *__restrict__ cs, long long fs, long long c, const double v[NV])
+{
+#pragma unroll
+    for (int q = 0; q < NV; q++) cs[q * fs + c] = v[q];
+}
+
+__device__ __forceinline__ void warp_count(unsigned long long *ctr, bool flag)
+{
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, flag);
+    if (m && (threadIdx.x & 31) == (__ffs(act) - 1)) atomicAdd(ctr, (unsigned long long)__popc(m));
+}
+
+__device__ __forceinline__ void warp_sum(unsigned long long *ctr, unsigned long long v)
+{
+    const unsigned act = __activemask();
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_down_sync(act, v, o);
+        if (((threadIdx.x & 31) + o) < 32 && ((act >> ((threadIdx.x & 31) + o)) & 1u)) v += w;
+    }
+    if ((threadIdx.x & 31) == (__ffs(act) - 1) && v) atomicAdd(ctr, v);
+}
+
+enum CellMode { M_DECODE = 0, M_ADV = 1, M_IMEX = 2, M_TRAP0 = 3, M_TRAP1 = 4, M_RK_STAGE1 = 5, M_RK_STAGE2 = 6 };
+
+struct CellArgs {
+    Layout L;
+    double *cs, *rhs, *T, *E, *cs0;
+    int *nchem;
+    const double *scal;  // [0] = dt
+    Status *st;
+    const double *xn, *yn;
+    double wedge[3];
+    int wedge_on;
+};
+
+__device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
+{
+    if (!a.wedge_on) return false;
+    const double x = a.xn[i], y = a.yn[j];
+    return x > a.wedge[0] && (y - a.wedge[1]) < (x - a.wedge[0]) * a.wedge[2];
+}
+
+// One thread per interior cell.  MODE selects the reference sequence:
+//  M_DECODE  Update_after_CS
+//  M_ADV     Update_after_Adv (+ decode)
+//  M_IMEX    Diagonalized + Update_IMEX (+ decode, + GetPartial_T for the next step)
+//  M_TRAP0   Update_after_Adv, field Trapezoid, Explicit()
+//  M_TRAP1   Update_after_Adv, TrapezoidPrediction and the per-cell substeps
+//  M_RK_STAGE1/2  SSP-RK2 stage updates (new)
+template <class P, int MODE>
+__global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
+{
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    if (solid_cell(a, i, j)) return;
+    const long long c = L.at(i, j, k);
+    const long long fs = L.fs;
+    const double dt = a.scal[0];
+    double cs[NV];
+    load_cs(a.cs, fs, c, cs);
+    double T = a.T[c], Eold = a.E[c];
+    Decoded o;
+    int capped = 0, capped_any = 0;
+
+    if (MODE == M_IMEX) {
+        // state of the previous decode, recomputed from the stored CS and T
+        double D = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) D += cs[s];
+        const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
+        const TPow p = tpow(T);
+        double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], CMS[NS], MD[NS];
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const double Y = cs[s] / D;
+            sdiv += Y / cM.mw[s];
+            scp += (cM.ri[s] * cp_r(s, p)) * Y;
+        }
+        const double Rgas = R_GAS * 1000 / (1.0 / sdiv);
+        const double CV = scp * 1000 - Rgas;
+        const double ke = 0.5 * (U * U + V * V + W * W);
+        // GetPartial_T, src/Flowfield.cpp:1578-1595
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            PT[s] = (ke - cM.ri[s] * h_r(s, p) + cM.ri[s] * 1e3 * T) / (CV * D);
+            Di[s] = cs[s] * 1e-3;
+            Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;
+        }
+        diagonalized(p, Mc, Di, PT, CMS, MD);
+        // Flowfield::Update_IMEX, src/Flowfield.cpp:1219-1228
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            double r = a.rhs[v * fs + c];
+            if (v < NS) {
+                r = r + CMS[v] * dt;
+                cs[v] = cs[v] + r / (1.0 - dt * MD[v]);
+            } else {
+                cs[v] = cs[v] + r;
+            }
+        }
+        decode(cs, T, Eold, o, capped);
+        capped_any |= capped;
+    } else if (MODE == M_DECODE) {
+        decode(cs, T, Eold, o, capped);
+        capped_any |= capped;
+    } else if (MODE == M_RK_STAGE1 || MODE == M_RK_STAGE2) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            const double r = a.rhs[v * fs + c];
+            if (MODE == M_RK_STAGE1) {
+                a.cs0[v * fs + c] = cs[v];
+                cs[v] = cs[v] + r;
+            } else {
+                cs[v] = 0.5 * a.cs0[v * fs + c] + 0.5 * (cs[v] + r);
+            }
+        }
+        decode(cs, T, Eold, o, capped);
+        capped_any |= capped;
+    } else {
+        // Update_after_Adv, src/Flowfield.cpp:1140-1157
+        const int nv = (cM.quirks & EU3D_Q_ADV_SPECIES_ONLY) ? NS : NV;
+#pragma unroll
+        for (int v = 0; v < NV; v++)
+            if (v < nv) cs[v] = cs[v] + a.rhs[v * fs + c];
+        decode(cs, T, Eold, o, capped);
+        capped_any |= capped;
+        if (MODE == M_TRAP0) {
+            const int rtb = (cM.quirks & EU3D_Q_TRAP_RTB_ZERO) ? 1 : 0;
+            double dn[NS], Wi[NS];
+            trapezoid(tpow(o.T), cs, dt, rtb, dn, Wi);
+            // Flowfield::Explicit(), src/Flowfield.cpp:1169-1186
+            double D = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                cs[s] = dn[s];
+                D += cs[s];
+            }
+            cs[NS] = o.U * D;
+            cs[NS + 1] = o.V * D;
+            const double e = D * o.E + 0.5 * (o.U * o.U + o.V * o.V + o.W * o.W) * D;
+            if (cM.quirks & EU3D_Q_EXPLICIT_ENERGY) {
+                cs[NS + 2] = e;
+            } else {
+                cs[NS + 2] = o.W * D;
+                cs[NS + 3] = e;
+            }
+            const double E1 = o.E;
+            decode(cs, o.T, E1, o, capped);
+            capped_any |= capped;
+        } else if (MODE == M_TRAP1) {
+            const int rtb = (cM.quirks & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
+            int n = predict_nchem(tpow(o.T), cs, o.Y, dt, rtb);
+            const bool over = n > NCHEM_CAP;
+            if (over) n = NCHEM_CAP;
+            if (over) atomicAdd(&a.st->substep_capped, 1);
+            atomicMax(&a.st->nchem_max, n);
+            if (a.nchem) a.nchem[c] = n;
+            const double dts = dt / n;
+            for (int step = 0; step < n; step++) {
+                double dn[NS], Wi[NS];
+                trapezoid(tpow(o.T), cs, dts, rtb, dn, Wi);
+                // Flowfield::Explicit(step, i, j, k), src/Flowfield.cpp:1189-1203
+                double D = 0.0;
+#pragma unroll
+                for (int s = 0; s < NS; s++) {
+                    cs[s] = dn[s];
+                    D += cs[s];
+                }
+                cs[NS] = o.U * D;
+                cs[NS + 1] = o.V * D;
+                cs[NS + 2] = o.W * D;
+                cs[NS + 3] = D * o.E + 0.5 * (o.U * o.U + o.V * o.V + o.W * o.W) * D;
+                decode(cs, o.T, o.E, o, capped);
+                capped_any |= capped;
+            }
+            atomicAdd(&a.st->substeps, (unsigned long long)n);
+        }
+    }
+    store_cs(a.cs, fs, c, cs);
+    a.T[c] = o.T;
+    a.E[c] = o.E;
+    store_prims<P>(o, q, fs, c);
+    warp_count(&a.st->newton_capped, capped_any != 0);
+    warp_count(&a.st->nonfinite, !(isfinite(o.D) && isfinite(o.T)));
+}
+
+}  // namespace eu3d

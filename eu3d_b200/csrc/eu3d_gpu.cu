@@ -1,0 +1,744 @@
+// EU3D B200 hot path: handle, memory, launches and the C ABI declared in
+// include/eu3d_gpu.h.  One translation unit so that the mechanism lives in a
+// single __constant__ object shared by every kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+
+#include "../../include/eu3d_gpu.h"
+#include "bc.cuh"
+#include "cell.cuh"
+#include "common.cuh"
+#include "flux.cuh"
+
+using namespace eu3d;
+
+namespace {
+
+thread_local std::string g_err;
+MechConst g_mech_loaded[1];
+int g_mech_refs = 0;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(EU3D_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct StepKey {
+    int react, type, timeadv, diff, bc_kind;
+    double cfl, final_time;
+    bool operator<(const StepKey &o) const
+    {
+        return std::tie(react, type, timeadv, diff, bc_kind, cfl, final_time) <
+               std::tie(o.react, o.type, o.timeadv, o.diff, o.bc_kind, o.cfl, o.final_time);
+    }
+};
+
+}  // namespace
+
+struct eu3d_handle {
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    Layout L{};
+    int flux_bits = 64;
+    unsigned quirks = 0;
+    double *cs = nullptr, *rhs = nullptr, *cs0 = nullptr, *T = nullptr, *E = nullptr;
+    void *prim = nullptr;
+    int *nchem = nullptr;
+    double *xn = nullptr, *yn = nullptr, *zn = nullptr;
+    double *scal = nullptr;  // [0] dt, [1] time
+    double *partial = nullptr;
+    int nparts = 0;
+    Status *status = nullptr;
+    double *inflow = nullptr;
+    double *stage = nullptr;
+    size_t stage_bytes = 0;
+    double wedge[3] = {0, 0, 0};
+    int wedge_on = 0;
+    std::map<StepKey, cudaGraphExec_t> graphs;
+};
+
+namespace {
+
+int prim_bytes(const eu3d_handle *h) { return h->flux_bits == 64 ? 8 : 4; }
+
+CellArgs cell_args(eu3d_handle *h)
+{
+    CellArgs a;
+    a.L = h->L;
+    a.cs = h->cs;
+    a.rhs = h->rhs;
+    a.T = h->T;
+    a.E = h->E;
+    a.cs0 = h->cs0;
+    a.nchem = h->nchem;
+    a.scal = h->scal;
+    a.st = h->status;
+    a.xn = h->xn;
+    a.yn = h->yn;
+    a.wedge[0] = h->wedge[0];
+    a.wedge[1] = h->wedge[1];
+    a.wedge[2] = h->wedge[2];
+    a.wedge_on = h->wedge_on;
+    return a;
+}
+
+dim3 cell_grid(const Layout &L, int bx) { return dim3((L.ni + bx - 1) / bx, L.nj, L.nk); }
+
+template <class P>
+void launch_cell(eu3d_handle *h, int mode)
+{
+    CellArgs a = cell_args(h);
+    P *q = (P *)h->prim;
+    dim3 g = cell_grid(h->L, 128);
+    switch (mode) {
+    case M_DECODE: k_cell<P, M_DECODE><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_ADV: k_cell<P, M_ADV><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_IMEX: k_cell<P, M_IMEX><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_TRAP0: k_cell<P, M_TRAP0><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_TRAP1: k_cell<P, M_TRAP1><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK_STAGE1: k_cell<P, M_RK_STAGE1><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK_STAGE2: k_cell<P, M_RK_STAGE2><<<g, 128, 0, h->st>>>(a, q); break;
+    }
+}
+
+int cell_op(eu3d_handle *h, int mode)
+{
+    if (h->flux_bits == 64)
+        launch_cell<double>(h, mode);
+    else
+        launch_cell<float>(h, mode);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+template <class P>
+void launch_adv(eu3d_handle *h, int diff)
+{
+    const int sq = (h->quirks & EU3D_Q_SPECIES_FACES) ? 1 : 0;
+    dim3 g = cell_grid(h->L, 128);
+    if (diff == EU3D_DIFF_MUSCL1)
+        k_advection<P, EU3D_DIFF_MUSCL1><<<g, 128, 0, h->st>>>(h->L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                                h->rhs, sq);
+    else
+        k_advection<P, EU3D_DIFF_MUSCL2><<<g, 128, 0, h->st>>>(h->L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                                h->rhs, sq);
+}
+
+int adv_op(eu3d_handle *h, int timeadv, int diff)
+{
+    if (timeadv == EU3D_ADV_TVD_RK3) return EU3D_OK;  // TimeAdv::TVD_RK3 leaves RHS as it is
+    if (h->flux_bits == 64)
+        launch_adv<double>(h, diff);
+    else
+        launch_adv<float>(h, diff);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+template <class P>
+void launch_ghost(eu3d_handle *h, int kind)
+{
+    GhostArgs a;
+    a.L = h->L;
+    a.T = h->T;
+    a.E = h->E;
+    a.inflow = h->inflow;
+    a.kind = kind;
+    P *q = (P *)h->prim;
+    const Layout &L = h->L;
+    const int g = 2 * L.bc;
+    if (kind != EU3D_BC_NONE) {
+        int n = g * L.nj * L.nk;
+        k_ghost_x<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        n = L.NI * g * L.nk;
+        k_ghost_y<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        n = L.NI * L.NJ * g;
+        k_ghost_z<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+    }
+    if (h->wedge_on) {
+        dim3 gw((L.NI + 127) / 128, L.NJ);
+        k_wedge<P><<<gw, 128, 0, h->st>>>(a, q, h->xn, h->yn, h->wedge[0], h->wedge[1], h->wedge[2]);
+    }
+}
+
+int ghost_op(eu3d_handle *h, int kind)
+{
+    if (kind < EU3D_BC_RSBI || kind > EU3D_BC_NONE) return fail(EU3D_ERR_ARG, "unknown boundary kind");
+    if (kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
+    if (h->flux_bits == 64)
+        launch_ghost<double>(h, kind);
+    else
+        launch_ghost<float>(h, kind);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+// node spacings the reference's CFLcondition uses (src/Flowfield.cpp:244-246)
+struct Spacing {
+    double dx, dy, dz;
+};
+
+template <class P>
+void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time)
+{
+    const int use_z = (h->quirks & EU3D_Q_CFL_NO_Z) ? 0 : 1;
+    k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, sp.dx, sp.dy, sp.dz, use_z, h->xn, h->yn,
+                                                   h->wedge[0], h->wedge[1], h->wedge[2], h->wedge_on, h->partial);
+    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, cfl, final_time, h->scal);
+}
+
+Spacing g_spacing(eu3d_handle *h);
+
+int cfl_op(eu3d_handle *h, double cfl, double final_time, const Spacing &sp)
+{
+    if (h->flux_bits == 64)
+        launch_cfl<double>(h, sp, cfl, final_time);
+    else
+        launch_cfl<float>(h, sp, cfl, final_time);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+// host reference layout <-> device SoA layout
+template <class D>
+__global__ void k_h2d(Layout L, const double *__restrict__ stage, int n, D *__restrict__ dst, long long dfs)
+{
+    const long long cells = (long long)L.NI * L.NJ * L.NK;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long hc = t / n;
+        const int s = (int)(t % n);
+        const int k = (int)(hc % L.NK), j = (int)((hc / L.NK) % L.NJ), i = (int)(hc / ((long long)L.NK * L.NJ));
+        dst[s * dfs + L.at(i, j, k)] = (D)stage[t];
+    }
+}
+
+template <class S>
+__global__ void k_d2h(Layout L, const S *__restrict__ src, long long sfs, int n, double *__restrict__ stage)
+{
+    const long long cells = (long long)L.NI * L.NJ * L.NK;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long hc = t / n;
+        const int s = (int)(t % n);
+        const int k = (int)(hc % L.NK), j = (int)((hc / L.NK) % L.NJ), i = (int)(hc / ((long long)L.NK * L.NJ));
+        stage[t] = (double)src[s * sfs + L.at(i, j, k)];
+    }
+}
+
+// derived download fields: C = sqrt(G P / D); Mc = CS_s / Mw * 1000; Di = CS_s
+template <class P>
+__global__ void k_derive(Layout L, const P *__restrict__ q, const double *__restrict__ cs, int what, double *stage, int n)
+{
+    const long long cells = (long long)L.NI * L.NJ * L.NK;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * n;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long hc = t / n;
+        const int s = (int)(t % n);
+        const int k = (int)(hc % L.NK), j = (int)((hc / L.NK) % L.NJ), i = (int)(hc / ((long long)L.NK * L.NJ));
+        const long long c = L.at(i, j, k);
+        double v;
+        if (what == EU3D_FIELD_C)
+            v = sqrt((double)q[PG * L.fs + c] * (double)q[PP * L.fs + c] / (double)q[PD * L.fs + c]);
+        else if (what == EU3D_FIELD_MC)
+            v = cs[s * L.fs + c] / cM.mw[s] * 1000;
+        else
+            v = cs[s * L.fs + c];
+        stage[t] = v;
+    }
+}
+
+int field_shape(int field, int *n)
+{
+    switch (field) {
+    case EU3D_FIELD_YI:
+    case EU3D_FIELD_MC:
+    case EU3D_FIELD_DI: *n = NS; return 0;
+    case EU3D_FIELD_CS:
+    case EU3D_FIELD_RHS: *n = NV; return 0;
+    default:
+        if (field < 0 || field >= EU3D_FIELD_COUNT) return -1;
+        *n = 1;
+        return 0;
+    }
+}
+
+int prim_index(int field)
+{
+    switch (field) {
+    case EU3D_FIELD_U: return PU;
+    case EU3D_FIELD_V: return PV;
+    case EU3D_FIELD_W: return PW;
+    case EU3D_FIELD_P: return PP;
+    case EU3D_FIELD_D: return PD;
+    case EU3D_FIELD_H: return PH;
+    case EU3D_FIELD_GAMMA: return PG;
+    case EU3D_FIELD_YI: return PY;
+    default: return -1;
+    }
+}
+
+int grid_blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 32); }
+
+Spacing g_spacing(eu3d_handle *h)
+{
+    // the reference reads node(1) - node(0) of each axis (src/Flowfield.cpp:244-246)
+    Spacing s;
+    double x[2], y[2], z[2];
+    cudaMemcpy(x, h->xn, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(y, h->yn, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(z, h->zn, 2 * sizeof(double), cudaMemcpyDeviceToHost);
+    s.dx = x[1] - x[0];
+    s.dy = y[1] - y[0];
+    s.dz = z[1] - z[0];
+    return s;
+}
+
+int validate_mech(const eu3d_desc *d, MechConst &m)
+{
+    memset(&m, 0, sizeof(m));
+    for (int r = 0; r < 2; r++)
+        for (int k = 0; k < 9; k++)
+            for (int s = 0; s < NS; s++) m.c[r][k][s] = (r ? d->coeff1 : d->coeff0)[k * NS + s];
+    for (int s = 0; s < NS; s++) {
+        if (!(d->mw[s] > 0)) return fail(EU3D_ERR_ARG, "molar masses must be positive");
+        m.mw[s] = d->mw[s];
+        m.ri[s] = R_GAS / d->mw[s];
+    }
+    for (int r = 0; r < NR; r++) {
+        m.af[r] = d->af[r];
+        m.bf[r] = d->bf[r];
+        m.eaf[r] = d->eaf[r];
+        double xr = 0.0;
+        int tb = 0;
+        for (int s = 0; s < NS; s++) {
+            const double f = d->stoi_f[s * NR + r], b = d->stoi_b[s * NR + r];
+            if (!(f == 0 || f == 1 || f == 2) || !(b == 0 || b == 1 || b == 2))
+                return fail(EU3D_ERR_ARG, "stoichiometric coefficients must be 0, 1 or 2");
+            m.sf[s][r] = f;
+            m.sb[s][r] = b;
+            m.tb[s][r] = d->react_tb[s * NR + r];
+            m.nu[s][r] = b - f;
+            xr += (b - f);
+            tb |= d->react_tb[s * NR + r] != 0;
+        }
+        m.xr[r] = xr;
+        m.p0xr[r] = pow((P0 * 1e-6), xr);
+        m.has_tb[r] = tb;
+        if (!(xr == 0 || xr == 1 || xr == -1)) return fail(EU3D_ERR_ARG, "net molecularity change must be -1, 0 or 1");
+    }
+    m.quirks = d->quirks;
+    return EU3D_OK;
+}
+
+void free_handle(eu3d_handle *h)
+{
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    void *ptrs[] = {h->cs, h->rhs, h->cs0, h->T, h->E, h->prim, h->nchem, h->xn, h->yn, h->zn, h->scal, h->partial,
+                    h->status, h->inflow, h->stage};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+int ensure_stage(eu3d_handle *h, size_t bytes)
+{
+    if (h->stage_bytes >= bytes) return EU3D_OK;
+    if (h->stage) cudaFree(h->stage);
+    h->stage = nullptr;
+    h->stage_bytes = 0;
+    CK(cudaMalloc(&h->stage, bytes));
+    h->stage_bytes = bytes;
+    return EU3D_OK;
+}
+
+int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
+{
+    int rc;
+    if (s->cfl != 0 && (rc = cfl_op(h, s->cfl, s->final_time, sp))) return rc;
+    if ((rc = ghost_op(h, s->bc_kind))) return rc;
+    if (s->timeadv == EU3D_ADV_SSPRK2) {
+        if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
+        if ((rc = cell_op(h, M_RK_STAGE1))) return rc;
+        if ((rc = ghost_op(h, s->bc_kind))) return rc;
+        if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
+        if ((rc = cell_op(h, M_RK_STAGE2))) return rc;
+        CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
+    } else {
+        if ((rc = adv_op(h, s->timeadv, s->diff))) return rc;
+    }
+    switch (s->react) {
+    case EU3D_REACT_IMEX: return cell_op(h, M_IMEX);
+    case EU3D_REACT_TRAPEZOID: return cell_op(h, s->type == 0 ? M_TRAP0 : M_TRAP1);
+    case EU3D_REACT_NONE:
+        // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
+        return cell_op(h, M_ADV);
+    default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *eu3d_last_error(void) { return g_err.c_str(); }
+
+int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
+{
+    if (!d || !out) return fail(EU3D_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (d->NS != NS || d->NR != NR) return fail(EU3D_ERR_ARG, "this build supports NS=9, NR=19");
+    if (d->bc != 2) return fail(EU3D_ERR_ARG, "ghost width bc must be 2");
+    if (d->ni < 1 || d->nj < 1 || d->nk < 1) return fail(EU3D_ERR_ARG, "grid extents must be positive");
+    if (d->flux_bits != 64 && d->flux_bits != 32) return fail(EU3D_ERR_ARG, "flux_bits must be 64 or 32");
+    if (!d->xnode || !d->ynode || !d->znode || !d->stoi_f || !d->stoi_b || !d->react_tb || !d->af || !d->bf ||
+        !d->eaf || !d->coeff0 || !d->coeff1 || !d->mw)
+        return fail(EU3D_ERR_ARG, "null table pointer");
+    MechConst m;
+    int rc = validate_mech(d, m);
+    if (rc) return rc;
+    CK(cudaSetDevice(d->device));
+    if (g_mech_refs > 0 && memcmp(&m, &g_mech_loaded[0], sizeof(m)) != 0)
+        return fail(EU3D_ERR_MECH, "a handle with different mechanism tables or quirks is alive");
+
+    eu3d_handle *h = new eu3d_handle();
+    h->dev = d->device;
+    h->flux_bits = d->flux_bits;
+    h->quirks = d->quirks;
+    Layout &L = h->L;
+    L.ni = d->ni;
+    L.nj = d->nj;
+    L.nk = d->nk;
+    L.bc = d->bc;
+    L.NI = d->ni + 2 * d->bc;
+    L.NJ = d->nj + 2 * d->bc;
+    L.NK = d->nk + 2 * d->bc;
+    L.px = (L.NI + 31) / 32 * 32;
+    L.fs = (long long)L.px * L.NJ * L.NK;
+    const size_t f8 = (size_t)L.fs * sizeof(double);
+#define ALLOC(p, bytes)                                                                    \
+    do {                                                                                   \
+        if (cudaMalloc((void **)&(p), (bytes)) != cudaSuccess) {                           \
+            free_handle(h);                                                                \
+            cudaGetLastError();                                                            \
+            return fail(EU3D_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed"); \
+        }                                                                                  \
+    } while (0)
+    if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return fail(EU3D_ERR_CUDA, "stream creation failed");
+    }
+    ALLOC(h->cs, NV * f8);
+    ALLOC(h->rhs, NV * f8);
+    ALLOC(h->T, f8);
+    ALLOC(h->E, f8);
+    ALLOC(h->prim, (size_t)NPRIM * L.fs * prim_bytes(h));
+    ALLOC(h->nchem, (size_t)L.fs * sizeof(int));
+    ALLOC(h->xn, L.NI * sizeof(double));
+    ALLOC(h->yn, L.NJ * sizeof(double));
+    ALLOC(h->zn, L.NK * sizeof(double));
+    ALLOC(h->scal, 8 * sizeof(double));
+    h->nparts = 148 * 4;
+    ALLOC(h->partial, h->nparts * sizeof(double));
+    ALLOC(h->status, sizeof(Status));
+#undef ALLOC
+    cudaMemsetAsync(h->cs, 0, NV * f8, h->st);
+    cudaMemsetAsync(h->rhs, 0, NV * f8, h->st);
+    cudaMemsetAsync(h->T, 0, f8, h->st);
+    cudaMemsetAsync(h->E, 0, f8, h->st);
+    cudaMemsetAsync(h->prim, 0, (size_t)NPRIM * L.fs * prim_bytes(h), h->st);
+    cudaMemsetAsync(h->nchem, 0, (size_t)L.fs * sizeof(int), h->st);
+    cudaMemsetAsync(h->scal, 0, 8 * sizeof(double), h->st);
+    cudaMemsetAsync(h->status, 0, sizeof(Status), h->st);
+    cudaMemcpyAsync(h->xn, d->xnode, L.NI * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->yn, d->ynode, L.NJ * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    cudaMemcpyAsync(h->zn, d->znode, L.NK * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    if (g_mech_refs == 0) {
+        cudaError_t e = cudaMemcpyToSymbol(cM, &m, sizeof(m));
+        if (e != cudaSuccess) {
+            free_handle(h);
+            return fail(EU3D_ERR_CUDA, std::string("mechanism upload: ") + cudaGetErrorString(e));
+        }
+        g_mech_loaded[0] = m;
+    }
+    g_mech_refs++;
+    cudaError_t e = cudaStreamSynchronize(h->st);
+    if (e != cudaSuccess) {
+        g_mech_refs--;
+        free_handle(h);
+        return fail(EU3D_ERR_CUDA, std::string("create: ") + cudaGetErrorString(e));
+    }
+    *out = h;
+    return EU3D_OK;
+}
+
+int eu3d_destroy(eu3d_handle *h)
+{
+    if (!h) return EU3D_OK;
+    cudaSetDevice(h->dev);
+    cudaStreamSynchronize(h->st);
+    free_handle(h);
+    if (g_mech_refs > 0) g_mech_refs--;
+    return EU3D_OK;
+}
+
+void *eu3d_stream(eu3d_handle *h) { return h ? (void *)h->st : nullptr; }
+
+int eu3d_upload_field(eu3d_handle *h, int field, const double *host)
+{
+    if (!h || !host) return fail(EU3D_ERR_ARG, "null argument");
+    int n;
+    if (field_shape(field, &n) || field > EU3D_FIELD_RHS) return fail(EU3D_ERR_ARG, "field cannot be uploaded");
+    const Layout &L = h->L;
+    const long long cells = (long long)L.NI * L.NJ * L.NK;
+    const size_t bytes = (size_t)cells * n * sizeof(double);
+    int rc = ensure_stage(h, bytes);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h->stage, host, bytes, cudaMemcpyHostToDevice, h->st));
+    const int gb = grid_blocks(cells * n);
+    const int pi = prim_index(field);
+    if (pi >= 0) {
+        if (h->flux_bits == 64)
+            k_h2d<double><<<gb, 256, 0, h->st>>>(L, h->stage, n, (double *)h->prim + pi * L.fs, L.fs);
+        else
+            k_h2d<float><<<gb, 256, 0, h->st>>>(L, h->stage, n, (float *)h->prim + pi * L.fs, L.fs);
+    } else {
+        double *dst = field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
+        k_h2d<double><<<gb, 256, 0, h->st>>>(L, h->stage, n, dst, L.fs);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_download_field(eu3d_handle *h, int field, double *host)
+{
+    if (!h || !host) return fail(EU3D_ERR_ARG, "null argument");
+    int n;
+    if (field_shape(field, &n)) return fail(EU3D_ERR_ARG, "unknown field");
+    const Layout &L = h->L;
+    const long long cells = (long long)L.NI * L.NJ * L.NK;
+    const size_t bytes = (size_t)cells * n * sizeof(double);
+    int rc = ensure_stage(h, bytes);
+    if (rc) return rc;
+    const int gb = grid_blocks(cells * n);
+    const int pi = prim_index(field);
+    if (pi >= 0) {
+        if (h->flux_bits == 64)
+            k_d2h<double><<<gb, 256, 0, h->st>>>(L, (const double *)h->prim + pi * L.fs, L.fs, n, h->stage);
+        else
+            k_d2h<float><<<gb, 256, 0, h->st>>>(L, (const float *)h->prim + pi * L.fs, L.fs, n, h->stage);
+    } else if (field == EU3D_FIELD_C || field == EU3D_FIELD_MC || field == EU3D_FIELD_DI) {
+        if (h->flux_bits == 64)
+            k_derive<double><<<gb, 256, 0, h->st>>>(L, (const double *)h->prim, h->cs, field, h->stage, n);
+        else
+            k_derive<float><<<gb, 256, 0, h->st>>>(L, (const float *)h->prim, h->cs, field, h->stage, n);
+    } else if (field == EU3D_FIELD_NCHEM) {
+        k_d2h<int><<<gb, 256, 0, h->st>>>(L, h->nchem, L.fs, 1, h->stage);
+    } else {
+        const double *src =
+            field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
+        k_d2h<double><<<gb, 256, 0, h->st>>>(L, src, L.fs, n, h->stage);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, h->stage, bytes, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_set_inflow(eu3d_handle *h, const double *U, const double *V, const double *W, const double *Pp,
+                    const double *D, const double *T, const double *H, const double *E, const double *G,
+                    const double *Y)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    const size_t pl = (size_t)h->L.nj * h->L.nk;
+    if (!h->inflow) {
+        CK(cudaMalloc(&h->inflow, (9 + NS) * pl * sizeof(double)));
+        CK(cudaMemsetAsync(h->inflow, 0, (9 + NS) * pl * sizeof(double), h->st));
+    }
+    const double *src[9] = {U, V, W, Pp, D, T, H, E, G};
+    for (int f = 0; f < 9; f++)
+        if (src[f]) CK(cudaMemcpyAsync(h->inflow + f * pl, src[f], pl * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (Y) {
+        // host Yint is (nj, nk, NS); device planes are species-major
+        double *tmp = (double *)malloc(NS * pl * sizeof(double));
+        if (!tmp) return fail(EU3D_ERR_NOMEM, "host allocation failed");
+        for (size_t p = 0; p < pl; p++)
+            for (int s = 0; s < NS; s++) tmp[s * pl + p] = Y[p * NS + s];
+        cudaError_t e = cudaMemcpy(h->inflow + 9 * pl, tmp, NS * pl * sizeof(double), cudaMemcpyHostToDevice);
+        free(tmp);
+        if (e != cudaSuccess) return fail(EU3D_ERR_CUDA, cudaGetErrorString(e));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_set_wedge(eu3d_handle *h, double x0, double y0, double tan_angle, int enabled)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    h->wedge[0] = x0;
+    h->wedge[1] = y0;
+    h->wedge[2] = tan_angle;
+    h->wedge_on = enabled ? 1 : 0;
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    return EU3D_OK;
+}
+
+int eu3d_set_dt(eu3d_handle *h, double dt)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    CK(cudaMemcpyAsync(h->scal, &dt, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_set_time(eu3d_handle *h, double t)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    CK(cudaMemcpyAsync(h->scal + 1, &t, sizeof(double), cudaMemcpyHostToDevice, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_get_dt(eu3d_handle *h, double *dt)
+{
+    if (!h || !dt) return fail(EU3D_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(dt, h->scal, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_cfl(eu3d_handle *h, double cfl, double final_time, double *dt_out)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    int rc = cfl_op(h, cfl, final_time, g_spacing(h));
+    if (rc) return rc;
+    return dt_out ? eu3d_get_dt(h, dt_out) : EU3D_OK;
+}
+
+int eu3d_boundary(eu3d_handle *h, int kind)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    return ghost_op(h, kind);
+}
+
+int eu3d_advection(eu3d_handle *h, int timeadv, int diff)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (timeadv != EU3D_ADV_EE && timeadv != EU3D_ADV_TVD_RK3) return fail(EU3D_ERR_ARG, "timeadv must be EE or TVD_RK3");
+    if (diff != EU3D_DIFF_MUSCL1 && diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
+    return adv_op(h, timeadv, diff);
+}
+
+int eu3d_update_after_adv(eu3d_handle *h) { return h ? cell_op(h, M_ADV) : fail(EU3D_ERR_ARG, "null handle"); }
+int eu3d_update_after_cs(eu3d_handle *h) { return h ? cell_op(h, M_DECODE) : fail(EU3D_ERR_ARG, "null handle"); }
+int eu3d_react_imex(eu3d_handle *h) { return h ? cell_op(h, M_IMEX) : fail(EU3D_ERR_ARG, "null handle"); }
+int eu3d_react_trapezoid(eu3d_handle *h, int type)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (type != 0 && type != 1) return fail(EU3D_ERR_ARG, "trapezoid type must be 0 or 1");
+    return cell_op(h, type == 0 ? M_TRAP0 : M_TRAP1);
+}
+
+int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
+{
+    if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
+    if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "unknown time scheme");
+    if (s->diff != EU3D_DIFF_MUSCL1 && s->diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
+    if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE)
+        return fail(EU3D_ERR_ARG, "unsupported reaction scheme");
+    if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
+    if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
+    StepKey key{s->react, s->type, s->timeadv, s->diff, s->bc_kind, s->cfl, s->final_time};
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+        const Spacing sp = g_spacing(h);
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h, s, sp);
+        cudaError_t e = cudaStreamEndCapture(h->st, &g);
+        if (rc) {
+            if (e == cudaSuccess) cudaGraphDestroy(g);
+            return rc;
+        }
+        CK(e);
+        cudaGraphExec_t ex;
+        e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+        it = h->graphs.emplace(key, ex).first;
+    }
+    CK(cudaGraphLaunch(it->second, h->st));
+    return EU3D_OK;
+}
+
+int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time)
+{
+    for (int n = 0; n < nsteps; n++) {
+        int rc = eu3d_step(h, s);
+        if (rc) return rc;
+        if (check_time) {
+            double sc[2];
+            CK(cudaMemcpyAsync(sc, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+            CK(cudaStreamSynchronize(h->st));
+            if (!(sc[1] < s->final_time)) break;
+        }
+    }
+    return EU3D_OK;
+}
+
+int eu3d_synchronize(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+int eu3d_get_status(eu3d_handle *h, eu3d_status *o)
+{
+    if (!h || !o) return fail(EU3D_ERR_ARG, "null argument");
+    Status s;
+    double sc[2];
+    CK(cudaMemcpyAsync(&s, h->status, sizeof(Status), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(sc, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    o->nonfinite_cells = (long long)s.nonfinite;
+    o->newton_capped = (long long)s.newton_capped;
+    o->substeps = (long long)s.substeps;
+    o->nchem_max = s.nchem_max;
+    o->substep_capped = s.substep_capped;
+    o->surrogate_cells = (long long)s.sur_cells;
+    o->surrogate_fallback = (long long)s.sur_fallback;
+    o->dt = sc[0];
+    o->time = sc[1];
+    return EU3D_OK;
+}
+
+int eu3d_reset_status(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    CK(cudaMemsetAsync(h->status, 0, sizeof(Status), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
+}  // extern "C"

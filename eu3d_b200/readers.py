@@ -232,3 +232,13 @@ def assert_finite(a: np.ndarray, what: str) -> None:
 
 __all__ = ["Mechanism", "read_mechanism", "read_keyvalue", "Grid", "make_grid", "read_grid",
            "stoichiometric_h2_air", "molar_to_mass", "R_UNIVERSAL", "assert_finite", "math"]
+
+
+def load_h2_ja919() -> Mechanism:
+    """The H2_JA919 mechanism with the thermo.dat tables, as parsed from the
+    reference's input files into eu3d_b200/data/h2_ja919.json."""
+    import json
+    import os
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "h2_ja919.json")
+    with open(p) as fh:
+        return Mechanism.from_json(json.load(fh))

@@ -1,0 +1,157 @@
+/*
+ * EU3D B200 hot path: C ABI.
+ *
+ * A device-resident flowfield for one rank of the EU3D reactive Euler solver,
+ * advanced by hand-written sm_100a CUDA kernels.  Each entry point replaces
+ * one member function of the reference's Flowfield / Reaction / TimeAdv
+ * classes or one step of Euler::Computing; the reference interface it stands
+ * in for is cited beside it.  A host C++ caller keeps its own readers and
+ * arrays (Mesh, FileReader, Reaction::ReactionRead) and hands the library
+ * plain pointers.
+ *
+ * Conventions
+ *  - Every function returns 0 (EU3D_OK) or a negative EU3D_ERR_* code; no
+ *    exception crosses the ABI.  eu3d_last_error() gives a text for the last
+ *    failure on the calling thread.
+ *  - Host arrays use the reference layout (ARRAY::Array, include/Array.hpp:33-43):
+ *    row-major over the ghosted extents NI = ni + 2 bc, NJ, NK with the last
+ *    index fastest; per-cell vectors (species, conserved variables) innermost.
+ *  - The library owns all device memory of a handle; the caller owns every
+ *    host pointer.  Calls on one handle are issued on the handle's own CUDA
+ *    stream and are not thread-safe per handle (the reference's ranks are
+ *    single-threaded).
+ *  - The mechanism tables of all handles in one process must be identical:
+ *    they live in the device's constant memory.
+ */
+#ifndef EU3D_GPU_H
+#define EU3D_GPU_H
+
+#include <stddef.h>
+#include "eu3d_quirks.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EU3D_OK 0
+#define EU3D_ERR_ARG (-1)       /* invalid argument or unsupported size */
+#define EU3D_ERR_CUDA (-2)      /* a CUDA call failed */
+#define EU3D_ERR_NOMEM (-3)     /* device allocation failed */
+#define EU3D_ERR_MECH (-4)      /* mechanism differs from the one already loaded */
+#define EU3D_ERR_STATE (-5)     /* call not valid in the handle's current state */
+#define EU3D_ERR_NONFINITE (-6) /* a NaN/Inf density or temperature was found */
+
+/* Interior node counts, ghost width and node coordinates come from the
+   reference's Mesh (include/Mesh.hpp:22-46, src/Mesh.cpp:75-130); the
+   mechanism tables from Reaction::ReactionRead (src/Reaction.cpp:150-326).
+   This build supports NS = 9, NR = 19 (the H2_JA919 mechanism). */
+typedef struct {
+    int ni, nj, nk, bc;
+    const double *xnode, *ynode, *znode; /* lengths ni+2bc, nj+2bc, nk+2bc */
+    int NS, NR;
+    const double *stoi_f, *stoi_b, *react_tb; /* (NS, NR) row-major */
+    const double *af, *bf, *eaf;             /* (NR) Arrhenius A, b, Ea[cal/mol] */
+    const double *coeff0, *coeff1;           /* (9, NS): a1..a7, b1, b2 per range */
+    const double *mw;                        /* (NS) g/mol */
+    unsigned quirks;                         /* EU3D_Q_* bit set */
+    int flux_bits;                           /* 64: FP64 reconstruction/AUSM; 32: FP32 */
+    int device;                              /* CUDA device ordinal */
+} eu3d_desc;
+
+typedef struct eu3d_handle eu3d_handle;
+
+/* Field identifiers for upload/download.  Shapes (reference layout):
+   3D fields NI*NJ*NK; EU3D_FIELD_YI/MC/DI NI*NJ*NK*NS; CS/RHS NI*NJ*NK*(NS+4). */
+enum {
+    EU3D_FIELD_U = 0, EU3D_FIELD_V, EU3D_FIELD_W, EU3D_FIELD_P, EU3D_FIELD_D, EU3D_FIELD_T,
+    EU3D_FIELD_H, EU3D_FIELD_GAMMA, EU3D_FIELD_E,
+    EU3D_FIELD_YI, EU3D_FIELD_CS, EU3D_FIELD_RHS,
+    /* download only: recomputed from the state */
+    EU3D_FIELD_C, EU3D_FIELD_MC, EU3D_FIELD_DI, EU3D_FIELD_NCHEM /* substep counts, as doubles */,
+    EU3D_FIELD_COUNT
+};
+
+typedef struct {
+    int react;      /* EU3D_REACT_* */
+    int type;       /* trapezoid: 0 field form, 1 adaptive substeps */
+    int timeadv;    /* EU3D_ADV_* */
+    int diff;       /* EU3D_DIFF_* */
+    int bc_kind;    /* EU3D_BC_* */
+    double cfl;     /* 0: use the dt set by eu3d_set_dt */
+    double final_time;
+} eu3d_step_desc;
+
+typedef struct {
+    long long nonfinite_cells;   /* cells whose D or T became NaN/Inf */
+    long long newton_capped;     /* decodes that used all 10 Newton iterations */
+    long long substeps;          /* adaptive-trapezoid substeps taken */
+    int nchem_max;               /* largest per-cell substep count since the last reset */
+    int substep_capped;          /* cells whose substep count hit the cap */
+    long long surrogate_cells;   /* cells advanced by the learned surrogate */
+    long long surrogate_fallback;/* cells sent back to the integrator */
+    double dt, time;             /* device copies of Flowfield::dt / ::time */
+} eu3d_status;
+
+const char *eu3d_last_error(void);
+
+/* Flowfield::Construction + the member copies FieldInitial makes
+   (src/Flowfield.cpp:72-150, :166-169); Reaction::ReactionConstruction. */
+int eu3d_create(const eu3d_desc *desc, eu3d_handle **out);
+int eu3d_destroy(eu3d_handle *h);
+
+/* Host <-> device copies with the reference-layout transpose. */
+int eu3d_upload_field(eu3d_handle *h, int field, const double *host);
+int eu3d_download_field(eu3d_handle *h, int field, double *host);
+/* Inflow planes of FieldBoundary_3dODM (Uint..Yint, include/Flowfield.hpp:105-106):
+   nj*nk each (Y: nj*nk*NS); any pointer may be NULL to keep the old plane. */
+int eu3d_set_inflow(eu3d_handle *h, const double *U, const double *V, const double *W, const double *P,
+                    const double *D, const double *T, const double *H, const double *E, const double *G,
+                    const double *Y);
+/* Wedge immersed boundary (new): solid where x > x0 and y - y0 < (x - x0) tan. */
+int eu3d_set_wedge(eu3d_handle *h, double x0, double y0, double tan_angle, int enabled);
+
+int eu3d_set_dt(eu3d_handle *h, double dt);   /* Flowfield::dt */
+int eu3d_set_time(eu3d_handle *h, double t);  /* Flowfield::time */
+int eu3d_get_dt(eu3d_handle *h, double *dt);
+
+/* Flowfield::CFLcondition, src/Flowfield.cpp:242-272 (device reduction;
+   dt_out may be NULL to keep the result on the device) */
+int eu3d_cfl(eu3d_handle *h, double cfl, double final_time, double *dt_out);
+/* FieldBoundary_3dRSBI / _3dODM, src/Flowfield.cpp:378-773, plus the
+   transmissive and wedge fills (new) */
+int eu3d_boundary(eu3d_handle *h, int kind);
+/* Flowfield::Advection(TimeAdv, Diff), src/Flowfield.cpp:1096-1128, with
+   Flowfield::AUSM x3 (:1330-1502), MUSCL_1/MUSCL_2 (include/Differ.hpp:110-238)
+   and TimeAdv::EE / TVD_RK3 (src/TimeAdv.cpp:29-67): fills RHS */
+int eu3d_advection(eu3d_handle *h, int timeadv, int diff);
+/* Flowfield::Update_after_Adv, src/Flowfield.cpp:1140-1157 */
+int eu3d_update_after_adv(eu3d_handle *h);
+/* Flowfield::Update_after_CS, src/Flowfield.cpp:1246-1284 (with Get_temp :1542-1566) */
+int eu3d_update_after_cs(eu3d_handle *h);
+/* Euler::IMEX = Reaction::Diagonalized + Flowfield::Update_IMEX (+ GetPartial_T),
+   src/Euler.cpp:748-760, src/Reaction.cpp:736-811, src/Flowfield.cpp:1215-1234, :1578-1595 */
+int eu3d_react_imex(eu3d_handle *h);
+/* Euler::Trapezoid(type), src/Euler.cpp:357-737: Update_after_Adv, then
+   Reaction::Trapezoid field form (type 0, src/Reaction.cpp:412-485) + Explicit(),
+   or TrapezoidPrediction + per-cell substeps (type 1, :489-670) on the device
+   work queue */
+int eu3d_react_trapezoid(eu3d_handle *h, int type);
+/* One pass of Euler::Computing's loop body, src/Euler.cpp:266-333 (CFL, ghost
+   fill, advection, chemistry), recorded once and replayed as a CUDA graph. */
+int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s);
+/* nsteps passes; stops early once time reaches final_time (checked on the host
+   after each step only when check_time is nonzero). */
+int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time);
+int eu3d_synchronize(eu3d_handle *h);
+/* Status counters; a D/T NaN scan replaces D.IsNan()/T.IsNan() (src/Euler.cpp:319-331). */
+int eu3d_get_status(eu3d_handle *h, eu3d_status *st);
+int eu3d_reset_status(eu3d_handle *h);
+
+/* Pointer to the handle's CUDA stream (cudaStream_t), for callers that
+   interleave their own work. */
+void *eu3d_stream(eu3d_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -20,6 +20,8 @@ static const double ORC_R = 8.31434;  /* Flowfield/Reaction `R`, include/Reactio
 static const double ORC_RU = 1.987;   /* include/Reaction.hpp:270 */
 static const double ORC_P0 = 101325;  /* include/Reaction.hpp:271 */
 
+#define ORC_NCHEM_CAP 1048576.0
+
 #define ID3(f, i, j, k) (((size_t)(i) * (f)->NJ + (size_t)(j)) * (f)->NK + (size_t)(k))
 #define ID4(f, i, j, k, s, n) (ID3(f, i, j, k) * (size_t)(n) + (size_t)(s))
 
@@ -572,7 +574,13 @@ void orc_prediction(orc_field *f, const orc_mech *m)
                             dt_temp = fabs(-Di[s] / ip.Wi[s]);
                             if (dt_temp < dt) dt = dt_temp;
                         }
-                f->Nchem[c] = (int)(ceil(dtm / dt));
+                /* the reference aborts when the count overflows int
+                   (src/Reaction.cpp:662-668); here, as on the device, the
+                   count is clamped to ORC_NCHEM_CAP */
+                double n = ceil(dtm / dt);
+                if (!(n >= 1.0)) n = 1.0;
+                if (n > ORC_NCHEM_CAP) n = ORC_NCHEM_CAP;
+                f->Nchem[c] = (int)n;
             }
 }
 
