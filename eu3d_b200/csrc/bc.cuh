@@ -13,6 +13,7 @@ namespace eu3d {
 
 struct GhostArgs {
     Layout L;
+    unsigned quirks;
     double *T, *E;
     const double *inflow;  // ODM planes: U V W P D T H E G, then NS species planes, each nj*nk
     int kind;
@@ -41,7 +42,7 @@ __device__ __forceinline__ void ghost_wall(const GhostArgs &a, P *q, long long d
     q[PP * fs + d] = Pp;
     const double T = a.T[s];
     a.T[d] = T;
-    const TPow p = tpow(T);
+    const TPow p = tpow(T, a.quirks);
     double Y[NS], rg = 0.0, cp = 0.0, h = 0.0, e = 0.0;
 #pragma unroll
     for (int sp = 0; sp < NS; sp++) {

@@ -18,7 +18,8 @@ struct Decoded {
 // Flowfield::Update_after_CS per cell (src/Flowfield.cpp:1246-1284) with
 // Flowfield::Get_temp (:1542-1566).  Eold is the E of the previous decode
 // (the Newton target under EU3D_Q_STALE_E); T0 the Newton start.
-__device__ __forceinline__ void decode(const double cs[NV], double T0, double Eold, Decoded &o, int &capped)
+__device__ __forceinline__ void decode(const double cs[NV], double T0, double Eold, unsigned q, Decoded &o,
+                                       int &capped)
 {
     double D = 0.0;
 #pragma unroll
@@ -27,7 +28,7 @@ __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eo
     for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
     const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
     const double Enew = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) / D;
-    const double Et = (cM.quirks & EU3D_Q_STALE_E) ? Eold : Enew;
+    const double Et = (q & EU3D_Q_STALE_E) ? Eold : Enew;
     double sYR = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) sYR += o.Y[s] * cM.ri[s];
@@ -35,7 +36,7 @@ __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eo
     int count = 0;
     while (count < 10) {
         Tp = Tn;
-        const TPow p = tpow(Tp);
+        const TPow p = tpow(Tp, q);
         double sh = 0.0, scp = 0.0;
 #pragma unroll
         for (int s = 0; s < NS; s++) {
@@ -49,7 +50,7 @@ __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eo
         count++;
     }
     capped = count >= 10;
-    const TPow p = tpow(Tn);
+    const TPow p = tpow(Tn, q);
     double sdiv = 0.0, scp = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
@@ -268,10 +269,20 @@ __device__ __forceinline__ void warp_sum(unsigned long long *ctr, unsigned long 
     if ((threadIdx.x & 31) == (__ffs(act) - 1) && v) atomicAdd(ctr, v);
 }
 
-enum CellMode { M_DECODE = 0, M_ADV = 1, M_IMEX = 2, M_TRAP0 = 3, M_TRAP1 = 4, M_RK_STAGE1 = 5, M_RK_STAGE2 = 6 };
+enum CellMode {
+    M_DECODE = 0,
+    M_ADV = 1,
+    M_IMEX = 2,
+    M_TRAP0 = 3,
+    M_TRAP1 = 4,
+    M_RK_STAGE1 = 5,
+    M_RK_STAGE2 = 6,
+    M_NOCHEM = 7
+};
 
 struct CellArgs {
     Layout L;
+    unsigned quirks;
     double *cs, *rhs, *T, *E, *cs0;
     int *nchem;
     const double *scal;  // [0] = dt
@@ -295,6 +306,7 @@ __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
 //  M_TRAP0   Update_after_Adv, field Trapezoid, Explicit()
 //  M_TRAP1   Update_after_Adv, TrapezoidPrediction and the per-cell substeps
 //  M_RK_STAGE1/2  SSP-RK2 stage updates (new)
+//  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
 template <class P, int MODE>
 __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
 {
@@ -306,6 +318,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
     if (solid_cell(a, i, j)) return;
     const long long c = L.at(i, j, k);
     const long long fs = L.fs;
+    const unsigned qk = a.quirks;
     const double dt = a.scal[0];
     double cs[NV];
     load_cs(a.cs, fs, c, cs);
@@ -319,7 +332,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
 #pragma unroll
         for (int s = 0; s < NS; s++) D += cs[s];
         const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
-        const TPow p = tpow(T);
+        const TPow p = tpow(T, qk);
         double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], CMS[NS], MD[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) {
@@ -349,10 +362,10 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
                 cs[v] = cs[v] + r;
             }
         }
-        decode(cs, T, Eold, o, capped);
+        decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
     } else if (MODE == M_DECODE) {
-        decode(cs, T, Eold, o, capped);
+        decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
     } else if (MODE == M_RK_STAGE1 || MODE == M_RK_STAGE2) {
 #pragma unroll
@@ -365,20 +378,25 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
                 cs[v] = 0.5 * a.cs0[v * fs + c] + 0.5 * (cs[v] + r);
             }
         }
-        decode(cs, T, Eold, o, capped);
+        decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
     } else {
         // Update_after_Adv, src/Flowfield.cpp:1140-1157
-        const int nv = (cM.quirks & EU3D_Q_ADV_SPECIES_ONLY) ? NS : NV;
+        const int nv = (qk & EU3D_Q_ADV_SPECIES_ONLY) ? NS : NV;
 #pragma unroll
         for (int v = 0; v < NV; v++)
             if (v < nv) cs[v] = cs[v] + a.rhs[v * fs + c];
-        decode(cs, T, Eold, o, capped);
+        decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
-        if (MODE == M_TRAP0) {
-            const int rtb = (cM.quirks & EU3D_Q_TRAP_RTB_ZERO) ? 1 : 0;
+        if (MODE == M_TRAP0 || MODE == M_NOCHEM) {
             double dn[NS], Wi[NS];
-            trapezoid(tpow(o.T), cs, dt, rtb, dn, Wi);
+            if (MODE == M_TRAP0) {
+                const int rtb = (qk & EU3D_Q_TRAP_RTB_ZERO) ? 1 : 0;
+                trapezoid(tpow(o.T, qk), cs, dt, rtb, dn, Wi);
+            } else {
+#pragma unroll
+                for (int s = 0; s < NS; s++) dn[s] = cs[s];
+            }
             // Flowfield::Explicit(), src/Flowfield.cpp:1169-1186
             double D = 0.0;
 #pragma unroll
@@ -389,18 +407,18 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
             cs[NS] = o.U * D;
             cs[NS + 1] = o.V * D;
             const double e = D * o.E + 0.5 * (o.U * o.U + o.V * o.V + o.W * o.W) * D;
-            if (cM.quirks & EU3D_Q_EXPLICIT_ENERGY) {
+            if (qk & EU3D_Q_EXPLICIT_ENERGY) {
                 cs[NS + 2] = e;
             } else {
                 cs[NS + 2] = o.W * D;
                 cs[NS + 3] = e;
             }
             const double E1 = o.E;
-            decode(cs, o.T, E1, o, capped);
+            decode(cs, o.T, E1, qk, o, capped);
             capped_any |= capped;
         } else if (MODE == M_TRAP1) {
-            const int rtb = (cM.quirks & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
-            int n = predict_nchem(tpow(o.T), cs, o.Y, dt, rtb);
+            const int rtb = (qk & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
+            int n = predict_nchem(tpow(o.T, qk), cs, o.Y, dt, rtb);
             const bool over = n > NCHEM_CAP;
             if (over) n = NCHEM_CAP;
             if (over) atomicAdd(&a.st->substep_capped, 1);
@@ -409,7 +427,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
             const double dts = dt / n;
             for (int step = 0; step < n; step++) {
                 double dn[NS], Wi[NS];
-                trapezoid(tpow(o.T), cs, dts, rtb, dn, Wi);
+                trapezoid(tpow(o.T, qk), cs, dts, rtb, dn, Wi);
                 // Flowfield::Explicit(step, i, j, k), src/Flowfield.cpp:1189-1203
                 double D = 0.0;
 #pragma unroll
@@ -421,7 +439,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
                 cs[NS + 1] = o.V * D;
                 cs[NS + 2] = o.W * D;
                 cs[NS + 3] = D * o.E + 0.5 * (o.U * o.U + o.V * o.V + o.W * o.W) * D;
-                decode(cs, o.T, o.E, o, capped);
+                decode(cs, o.T, o.E, qk, o, capped);
                 capped_any |= capped;
             }
             atomicAdd(&a.st->substeps, (unsigned long long)n);

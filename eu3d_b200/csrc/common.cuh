@@ -43,7 +43,6 @@ struct MechConst {
     double xr[NR];       // sum over species of (sb - sf)
     double p0xr[NR];     // pow(P0 * 1e-6, xr), evaluated on the host
     int has_tb[NR];      // reaction has third-body efficiencies
-    unsigned quirks;
 };
 
 // defined once: every kernel lives in the single translation unit eu3d_gpu.cu
@@ -63,9 +62,11 @@ struct Status {
 struct TPow {
     double T, lnT, tm1, tm2, t2, t3, t4, t5;
     int hi;  // 1 when T >= 1000 K (high-range table)
+    int rb;  // table the integration constants b1, b2 come from
 };
 
-__device__ __forceinline__ TPow tpow(double T)
+// q: the handle's EU3D_Q_* set (the b1/b2 defect selects rb)
+__device__ __forceinline__ TPow tpow(double T, unsigned q)
 {
     TPow p;
     p.T = T;
@@ -77,6 +78,7 @@ __device__ __forceinline__ TPow tpow(double T)
     p.t4 = p.t2 * p.t2;
     p.t5 = p.t4 * T;
     p.hi = !(T < 1000.0);
+    p.rb = (q & EU3D_Q_THERMO_B12_LOW) ? 0 : p.hi;
     return p;
 }
 
@@ -92,8 +94,7 @@ __device__ __forceinline__ double cp_r(int s, const TPow &p)
 // takes the integration constant from the low range above 1000 K.
 __device__ __forceinline__ double h_r(int s, const TPow &p)
 {
-    const int r = p.hi;
-    const int rb = (cM.quirks & EU3D_Q_THERMO_B12_LOW) ? 0 : r;
+    const int r = p.hi, rb = p.rb;
     return -cM.c[r][0][s] * p.tm1 + cM.c[r][1][s] * p.lnT + cM.c[r][2][s] * p.T + cM.c[r][3][s] * p.t2 * 0.5 +
            cM.c[r][4][s] * p.t3 * (1.0 / 3.0) + cM.c[r][5][s] * p.t4 * 0.25 + cM.c[r][6][s] * p.t5 * 0.2 +
            cM.c[rb][7][s];
@@ -102,8 +103,7 @@ __device__ __forceinline__ double h_r(int s, const TPow &p)
 // S/R, Reaction::GetSi bracket (src/Reaction.cpp:938-948)
 __device__ __forceinline__ double s_r(int s, const TPow &p)
 {
-    const int r = p.hi;
-    const int rb = (cM.quirks & EU3D_Q_THERMO_B12_LOW) ? 0 : r;
+    const int r = p.hi, rb = p.rb;
     return -cM.c[r][0][s] * p.tm2 * 0.5 - cM.c[r][1][s] * p.tm1 + cM.c[r][2][s] * p.lnT + cM.c[r][3][s] * p.T +
            cM.c[r][4][s] * p.t2 * 0.5 + cM.c[r][5][s] * p.t3 * (1.0 / 3.0) + cM.c[r][6][s] * p.t4 * 0.25 +
            cM.c[rb][8][s];

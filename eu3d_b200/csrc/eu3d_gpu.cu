@@ -11,6 +11,7 @@
 #include <map>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "../../include/eu3d_gpu.h"
 #include "bc.cuh"
@@ -71,16 +72,61 @@ struct eu3d_handle {
     double wedge[3] = {0, 0, 0};
     int wedge_on = 0;
     std::map<StepKey, cudaGraphExec_t> graphs;
+    // per-kernel CUDA-event timing (eu3d_profile_enable)
+    bool profile = false;
+    struct ProfRec {
+        const char *name;
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    std::map<std::string, std::pair<double, long long>> prof_acc;
 };
 
 namespace {
 
 int prim_bytes(const eu3d_handle *h) { return h->flux_bits == 64 ? 8 : 4; }
 
+cudaEvent_t prof_event(eu3d_handle *h)
+{
+    if (!h->prof_pool.empty()) {
+        cudaEvent_t e = h->prof_pool.back();
+        h->prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one kernel launch with CUDA events on the handle's stream while
+// profiling is enabled (eu3d_step then runs without its graph).
+struct ProfScope {
+    eu3d_handle *h;
+    const char *name;
+    cudaEvent_t a = nullptr;
+    ProfScope(eu3d_handle *hh, const char *n) : h(hh), name(n)
+    {
+        if (h->profile) {
+            a = prof_event(h);
+            cudaEventRecord(a, h->st);
+        }
+    }
+    ~ProfScope()
+    {
+        if (h->profile && a) {
+            cudaEvent_t b = prof_event(h);
+            cudaEventRecord(b, h->st);
+            h->prof_pending.push_back({name, a, b});
+        }
+    }
+};
+
 CellArgs cell_args(eu3d_handle *h)
 {
     CellArgs a;
     a.L = h->L;
+    a.quirks = h->quirks;
     a.cs = h->cs;
     a.rhs = h->rhs;
     a.T = h->T;
@@ -106,6 +152,9 @@ void launch_cell(eu3d_handle *h, int mode)
     CellArgs a = cell_args(h);
     P *q = (P *)h->prim;
     dim3 g = cell_grid(h->L, 128);
+    static const char *names[] = {"cell_decode", "cell_adv", "cell_imex", "cell_trap0", "cell_trap1", "cell_rk1",
+                                  "cell_rk2", "cell_nochem"};
+    ProfScope ps(h, names[mode]);
     switch (mode) {
     case M_DECODE: k_cell<P, M_DECODE><<<g, 128, 0, h->st>>>(a, q); break;
     case M_ADV: k_cell<P, M_ADV><<<g, 128, 0, h->st>>>(a, q); break;
@@ -114,6 +163,7 @@ void launch_cell(eu3d_handle *h, int mode)
     case M_TRAP1: k_cell<P, M_TRAP1><<<g, 128, 0, h->st>>>(a, q); break;
     case M_RK_STAGE1: k_cell<P, M_RK_STAGE1><<<g, 128, 0, h->st>>>(a, q); break;
     case M_RK_STAGE2: k_cell<P, M_RK_STAGE2><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_NOCHEM: k_cell<P, M_NOCHEM><<<g, 128, 0, h->st>>>(a, q); break;
     }
 }
 
@@ -132,6 +182,7 @@ void launch_adv(eu3d_handle *h, int diff)
 {
     const int sq = (h->quirks & EU3D_Q_SPECIES_FACES) ? 1 : 0;
     dim3 g = cell_grid(h->L, 128);
+    ProfScope ps(h, "advection");
     if (diff == EU3D_DIFF_MUSCL1)
         k_advection<P, EU3D_DIFF_MUSCL1><<<g, 128, 0, h->st>>>(h->L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
                                                                 h->rhs, sq);
@@ -156,6 +207,7 @@ void launch_ghost(eu3d_handle *h, int kind)
 {
     GhostArgs a;
     a.L = h->L;
+    a.quirks = h->quirks;
     a.T = h->T;
     a.E = h->E;
     a.inflow = h->inflow;
@@ -165,14 +217,24 @@ void launch_ghost(eu3d_handle *h, int kind)
     const int g = 2 * L.bc;
     if (kind != EU3D_BC_NONE) {
         int n = g * L.nj * L.nk;
-        k_ghost_x<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        {
+            ProfScope ps(h, "ghost_x");
+            k_ghost_x<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        }
         n = L.NI * g * L.nk;
-        k_ghost_y<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        {
+            ProfScope ps(h, "ghost_y");
+            k_ghost_y<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        }
         n = L.NI * L.NJ * g;
-        k_ghost_z<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        {
+            ProfScope ps(h, "ghost_z");
+            k_ghost_z<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
+        }
     }
     if (h->wedge_on) {
         dim3 gw((L.NI + 127) / 128, L.NJ);
+        ProfScope ps(h, "wedge");
         k_wedge<P><<<gw, 128, 0, h->st>>>(a, q, h->xn, h->yn, h->wedge[0], h->wedge[1], h->wedge[2]);
     }
 }
@@ -198,8 +260,13 @@ template <class P>
 void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time)
 {
     const int use_z = (h->quirks & EU3D_Q_CFL_NO_Z) ? 0 : 1;
-    k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, sp.dx, sp.dy, sp.dz, use_z, h->xn, h->yn,
-                                                   h->wedge[0], h->wedge[1], h->wedge[2], h->wedge_on, h->partial);
+    {
+        ProfScope ps(h, "cfl_partial");
+        k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, sp.dx, sp.dy, sp.dz, use_z, h->xn,
+                                                       h->yn, h->wedge[0], h->wedge[1], h->wedge[2], h->wedge_on,
+                                                       h->partial);
+    }
+    ProfScope ps(h, "cfl_final");
     k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, cfl, final_time, h->scal);
 }
 
@@ -261,6 +328,51 @@ __global__ void k_derive(Layout L, const P *__restrict__ q, const double *__rest
         else
             v = cs[s * L.fs + c];
         stage[t] = v;
+    }
+}
+
+// FieldInitial's completion of a primitive state (src/Flowfield.cpp:193-229)
+struct Uniform {
+    double P, T, U, V, W, Y[NS];
+};
+
+template <class P>
+__global__ void k_init_uniform(Layout L, Uniform u, unsigned quirks, P *q, double *cs, double *T, double *E)
+{
+    const long long cells = (long long)L.NK * L.NJ * L.px;
+    const TPow p = tpow(u.T, quirks);
+    double sdiv = 0.0, cp = 0.0, h = 0.0, e = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double cpi = cM.ri[s] * cp_r(s, p), hi = cM.ri[s] * h_r(s, p);
+        sdiv += u.Y[s] / cM.mw[s];
+        cp += cpi * u.Y[s];
+        h += u.Y[s] * hi;
+        e += u.Y[s] * (hi - cM.ri[s] * u.T);
+    }
+    const double Rgas = R_GAS * 1000 / (1.0 / sdiv);
+    const double D = u.P / (Rgas * u.T);
+    const double Cp = cp * 1000, H = h * 1000, En = e * 1000;
+    const double G = Cp / (Cp - R_GAS * sdiv * 1000);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cells; c += (long long)gridDim.x * blockDim.x) {
+        q[PD * L.fs + c] = (P)D;
+        q[PU * L.fs + c] = (P)u.U;
+        q[PV * L.fs + c] = (P)u.V;
+        q[PW * L.fs + c] = (P)u.W;
+        q[PP * L.fs + c] = (P)u.P;
+        q[PH * L.fs + c] = (P)H;
+        q[PG * L.fs + c] = (P)G;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            q[(PY + s) * L.fs + c] = (P)u.Y[s];
+            cs[s * L.fs + c] = D * u.Y[s];
+        }
+        cs[NS * L.fs + c] = D * u.U;
+        cs[(NS + 1) * L.fs + c] = D * u.V;
+        cs[(NS + 2) * L.fs + c] = D * u.W;
+        cs[(NS + 3) * L.fs + c] = D * En + 0.5 * (u.U * u.U + u.V * u.V + u.W * u.W) * D;
+        T[c] = u.T;
+        E[c] = En;
     }
 }
 
@@ -343,12 +455,16 @@ int validate_mech(const eu3d_desc *d, MechConst &m)
         m.has_tb[r] = tb;
         if (!(xr == 0 || xr == 1 || xr == -1)) return fail(EU3D_ERR_ARG, "net molecularity change must be -1, 0 or 1");
     }
-    m.quirks = d->quirks;
     return EU3D_OK;
 }
 
 void free_handle(eu3d_handle *h)
 {
+    for (auto &r : h->prof_pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->prof_pool) cudaEventDestroy(e);
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     void *ptrs[] = {h->cs, h->rhs, h->cs0, h->T, h->E, h->prim, h->nchem, h->xn, h->yn, h->zn, h->scal, h->partial,
@@ -390,7 +506,7 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
     case EU3D_REACT_TRAPEZOID: return cell_op(h, s->type == 0 ? M_TRAP0 : M_TRAP1);
     case EU3D_REACT_NONE:
         // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
-        return cell_op(h, M_ADV);
+        return cell_op(h, M_NOCHEM);
     default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
     }
 }
@@ -417,7 +533,7 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     if (rc) return rc;
     CK(cudaSetDevice(d->device));
     if (g_mech_refs > 0 && memcmp(&m, &g_mech_loaded[0], sizeof(m)) != 0)
-        return fail(EU3D_ERR_MECH, "a handle with different mechanism tables or quirks is alive");
+        return fail(EU3D_ERR_MECH, "a handle with different mechanism tables is alive");
 
     eu3d_handle *h = new eu3d_handle();
     h->dev = d->device;
@@ -591,6 +707,27 @@ int eu3d_set_inflow(eu3d_handle *h, const double *U, const double *V, const doub
     return EU3D_OK;
 }
 
+int eu3d_init_uniform(eu3d_handle *h, double P, double T, double U, double V, double W, const double *Y)
+{
+    if (!h || !Y) return fail(EU3D_ERR_ARG, "null argument");
+    if (!(P > 0) || !(T > 0)) return fail(EU3D_ERR_ARG, "pressure and temperature must be positive");
+    Uniform u;
+    u.P = P;
+    u.T = T;
+    u.U = U;
+    u.V = V;
+    u.W = W;
+    for (int s = 0; s < NS; s++) u.Y[s] = Y[s];
+    const int gb = grid_blocks((long long)h->L.fs);
+    if (h->flux_bits == 64)
+        k_init_uniform<double><<<gb, 256, 0, h->st>>>(h->L, u, h->quirks, (double *)h->prim, h->cs, h->T, h->E);
+    else
+        k_init_uniform<float><<<gb, 256, 0, h->st>>>(h->L, u, h->quirks, (float *)h->prim, h->cs, h->T, h->E);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->st));
+    return EU3D_OK;
+}
+
 int eu3d_set_wedge(eu3d_handle *h, double x0, double y0, double tan_angle, int enabled)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
@@ -668,6 +805,7 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
         return fail(EU3D_ERR_ARG, "unsupported reaction scheme");
     if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
     if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
+    if (h->profile) return enqueue_step(h, s, g_spacing(h));
     StepKey key{s->react, s->type, s->timeadv, s->diff, s->bc_kind, s->cfl, s->final_time};
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
@@ -703,6 +841,49 @@ int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time
             if (!(sc[1] < s->final_time)) break;
         }
     }
+    return EU3D_OK;
+}
+
+int eu3d_profile_enable(eu3d_handle *h, int on)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    h->profile = on != 0;
+    return EU3D_OK;
+}
+
+int eu3d_profile_read(eu3d_handle *h, char *names, size_t names_cap, double *ms, long long *counts, int max_kernels,
+                      int *n_out)
+{
+    if (!h || !n_out) return fail(EU3D_ERR_ARG, "null argument");
+    CK(cudaStreamSynchronize(h->st));
+    for (auto &r : h->prof_pending) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, r.a, r.b));
+        auto &acc = h->prof_acc[r.name];
+        acc.first += t;
+        acc.second += 1;
+        h->prof_pool.push_back(r.a);
+        h->prof_pool.push_back(r.b);
+    }
+    h->prof_pending.clear();
+    int n = 0;
+    size_t used = 0;
+    for (auto &kv : h->prof_acc) {
+        if (n >= max_kernels) break;
+        const size_t len = kv.first.size() + 1;
+        if (names) {
+            if (used + len > names_cap) break;
+            memcpy(names + used, kv.first.c_str(), len - 1);
+            names[used + len - 1] = '\n';
+        }
+        used += len;
+        if (ms) ms[n] = kv.second.first;
+        if (counts) counts[n] = kv.second.second;
+        n++;
+    }
+    if (names && used < names_cap) names[used] = 0;
+    *n_out = n;
+    h->prof_acc.clear();
     return EU3D_OK;
 }
 

@@ -31,10 +31,10 @@ FIELDS = {"U": 0, "V": 1, "W": 2, "P": 3, "D": 4, "T": 5, "H": 6, "Gamma": 7, "E
 UPLOADABLE = ("U", "V", "W", "P", "D", "T", "H", "Gamma", "E", "Yi", "CS", "RHS")
 
 EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field", "eu3d_download_field",
-           "eu3d_set_inflow", "eu3d_set_wedge", "eu3d_set_dt", "eu3d_set_time", "eu3d_get_dt", "eu3d_cfl",
+           "eu3d_set_inflow", "eu3d_init_uniform", "eu3d_set_wedge", "eu3d_set_dt", "eu3d_set_time", "eu3d_get_dt", "eu3d_cfl",
            "eu3d_boundary", "eu3d_advection", "eu3d_update_after_adv", "eu3d_update_after_cs", "eu3d_react_imex",
            "eu3d_react_trapezoid", "eu3d_step", "eu3d_run", "eu3d_synchronize", "eu3d_get_status",
-           "eu3d_reset_status", "eu3d_stream"]
+           "eu3d_reset_status", "eu3d_stream", "eu3d_profile_enable", "eu3d_profile_read"]
 
 
 class Eu3dError(RuntimeError):
@@ -83,6 +83,7 @@ def load_library(path: Optional[str] = None):
     L.eu3d_download_field.argtypes = h + [C.c_int, _dp]
     L.eu3d_set_inflow.argtypes = h + [_dp] * 10
     L.eu3d_set_wedge.argtypes = h + [C.c_double, C.c_double, C.c_double, C.c_int]
+    L.eu3d_init_uniform.argtypes = h + [C.c_double] * 5 + [_dp]
     L.eu3d_set_dt.argtypes = h + [C.c_double]
     L.eu3d_set_time.argtypes = h + [C.c_double]
     L.eu3d_get_dt.argtypes = h + [_dp]
@@ -98,6 +99,9 @@ def load_library(path: Optional[str] = None):
     L.eu3d_get_status.argtypes = h + [C.POINTER(Status)]
     L.eu3d_stream.argtypes = h
     L.eu3d_stream.restype = C.c_void_p
+    L.eu3d_profile_enable.argtypes = h + [C.c_int]
+    L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
+                                        C.POINTER(C.c_int)]
     for fn in EXPORTS:
         if fn not in ("eu3d_last_error", "eu3d_stream"):
             getattr(L, fn).restype = C.c_int
@@ -184,6 +188,10 @@ class DeviceFlowfield:
         args = [np.ascontiguousarray(x, dtype=np.float64) for x in (U, V, W, P, D, T, H, E, G, Y)]
         _check(self.L.eu3d_set_inflow(self.h, *[x.ctypes.data_as(_dp) for x in args]))
 
+    def init_uniform(self, P, T, U, V, W, Y):
+        y = np.ascontiguousarray(Y, dtype=np.float64)
+        _check(self.L.eu3d_init_uniform(self.h, P, T, U, V, W, y.ctypes.data_as(_dp)))
+
     def set_wedge(self, x0, y0, tan_angle, enabled=True):
         _check(self.L.eu3d_set_wedge(self.h, x0, y0, tan_angle, 1 if enabled else 0))
 
@@ -244,6 +252,20 @@ class DeviceFlowfield:
 
     def reset_status(self):
         _check(self.L.eu3d_reset_status(self.h))
+
+    def profile(self, on: bool = True):
+        _check(self.L.eu3d_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (total ms, launches)} since the previous read."""
+        cap, mk = 4096, 64
+        names = C.create_string_buffer(cap)
+        ms = (C.c_double * mk)()
+        cnt = (C.c_longlong * mk)()
+        n = C.c_int()
+        _check(self.L.eu3d_profile_read(self.h, names, cap, ms, cnt, mk, C.byref(n)))
+        keys = names.value.decode().split("\n")
+        return {keys[i]: (ms[i], cnt[i]) for i in range(n.value)}
 
     @property
     def stream(self) -> int:

@@ -21,7 +21,8 @@
  *    stream and are not thread-safe per handle (the reference's ranks are
  *    single-threaded).
  *  - The mechanism tables of all handles in one process must be identical:
- *    they live in the device's constant memory.
+ *    they live in the device's constant memory.  Quirk policies and every
+ *    other setting are per handle.
  */
 #ifndef EU3D_GPU_H
 #define EU3D_GPU_H
@@ -107,6 +108,10 @@ int eu3d_download_field(eu3d_handle *h, int field, double *host);
 int eu3d_set_inflow(eu3d_handle *h, const double *U, const double *V, const double *W, const double *P,
                     const double *D, const double *T, const double *H, const double *E, const double *G,
                     const double *Y);
+/* Uniform state in every cell, ghosts included (new; the reference's
+   FieldInitial hard-codes its RSBI state): P, T, velocity and NS mass
+   fractions, completed with FieldInitial's arithmetic (src/Flowfield.cpp:193-229). */
+int eu3d_init_uniform(eu3d_handle *h, double P, double T, double U, double V, double W, const double *Y);
 /* Wedge immersed boundary (new): solid where x > x0 and y - y0 < (x - x0) tan. */
 int eu3d_set_wedge(eu3d_handle *h, double x0, double y0, double tan_angle, int enabled);
 
@@ -143,6 +148,15 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s);
    after each step only when check_time is nonzero). */
 int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time);
 int eu3d_synchronize(eu3d_handle *h);
+/* Per-kernel timing with CUDA events on the handle's stream (replaces the
+   reference's MPI_Wtime phase timers, src/Euler.cpp:256-344).  While enabled,
+   eu3d_step launches its kernels directly instead of replaying its graph.
+   eu3d_profile_read synchronises, then reports per kernel name (newline
+   separated in `names`) the summed milliseconds and launch counts since the
+   previous read. */
+int eu3d_profile_enable(eu3d_handle *h, int on);
+int eu3d_profile_read(eu3d_handle *h, char *names, size_t names_cap, double *ms, long long *counts,
+                      int max_kernels, int *n_out);
 /* Status counters; a D/T NaN scan replaces D.IsNan()/T.IsNan() (src/Euler.cpp:319-331). */
 int eu3d_get_status(eu3d_handle *h, eu3d_status *st);
 int eu3d_reset_status(eu3d_handle *h);
