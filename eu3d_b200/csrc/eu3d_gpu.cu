@@ -513,6 +513,89 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Allocation-free CFL time step (eu3d_cfl_noalloc).
+//
+// Some callers cannot allocate device memory: code that runs while another
+// framework owns the device memory pool and forbids allocations, or code that
+// must not call cudaMalloc/cudaFree because those calls synchronise the device
+// and would stall work in flight.  For them this entry point computes the CFL
+// step from device fields the caller already holds, writing dt and time into
+// caller-owned device memory, and allocates nothing: its one piece of scratch
+// memory -- the per-block partial minima of the reduction -- is the
+// file-scope device array below.  Every GPU that loads the library keeps this
+// array (8 KB) until the process exits.
+namespace {
+
+constexpr int NOALLOC_CFL_MAX_BLOCKS = 1024;
+constexpr int NOALLOC_CFL_DEFAULT_BLOCKS = 148 * 4;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_cfl_scratch[NOALLOC_CFL_MAX_BLOCKS];
+
+// Device address of g_cfl_scratch per device.  In host code the symbol
+// g_cfl_scratch names a host-side stand-in, not device memory, so kernels are
+// given this address, obtained once per device with that device current.
+double *g_cfl_scratch_dev[NOALLOC_MAX_DEVICES] = {};
+
+struct CflFields {
+    const double *D, *U, *V, *W, *P, *G;
+    int ni, nj, nk, bc;
+    long long pitch, plane;
+};
+
+__global__ void k_cfl_fields_partial(CflFields f, double dx, double dy, double dz, int use_z, double *partial)
+{
+    const long long n = (long long)f.ni * f.nj * f.nk;
+    double m = 1e10;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = f.bc + (int)(t % f.ni);
+        const int j = f.bc + (int)((t / f.ni) % f.nj);
+        const int k = f.bc + (int)(t / ((long long)f.ni * f.nj));
+        const long long c = k * f.plane + j * f.pitch + i;
+        const double C = sqrt(f.G[c] * f.P[c] / f.D[c]);
+        const double a = dx / (fabs(f.U[c]) + C), b = dy / (fabs(f.V[c]) + C);
+        double tmp = (b < a) ? b : a;
+        if (use_z) {
+            const double z = dz / (fabs(f.W[c]) + C);
+            tmp = (z < tmp) ? z : tmp;
+        }
+        if (tmp < m) m = tmp;
+    }
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
+        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    }
+}
+
+__global__ void k_cfl_fields_final(const double *partial, int nparts, double cfl, double final_time, double *dt_out,
+                                   double *time_inout)
+{
+    double m = 1e10;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) m = fmin(m, partial[t]);
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
+        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) {
+            double dt = cfl * m;
+            if (*time_inout + dt > final_time) dt = final_time - *time_inout;
+            *dt_out = dt;
+            *time_inout += dt;
+        }
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *eu3d_last_error(void) { return g_err.c_str(); }
@@ -884,6 +967,35 @@ int eu3d_profile_read(eu3d_handle *h, char *names, size_t names_cap, double *ms,
     if (names && used < names_cap) names[used] = 0;
     *n_out = n;
     h->prof_acc.clear();
+    return EU3D_OK;
+}
+
+int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const double *W, const double *Pp,
+                     const double *Gamma, int ni, int nj, int nk, int bc, long long pitch, long long plane, double dx,
+                     double dy, double dz, int use_z, double cfl, double final_time, double *time_inout,
+                     double *dt_out, int nblocks, void *stream)
+{
+    if (!D || !U || !V || !W || !Pp || !Gamma || !time_inout || !dt_out) return fail(EU3D_ERR_ARG, "null argument");
+    if (ni < 1 || nj < 1 || nk < 1 || bc < 0) return fail(EU3D_ERR_ARG, "grid extents must be positive");
+    if (pitch < ni + 2LL * bc || plane < pitch * (nj + 2LL * bc))
+        return fail(EU3D_ERR_ARG, "pitch/plane stride smaller than the ghosted extents");
+    if (nblocks <= 0) nblocks = NOALLOC_CFL_DEFAULT_BLOCKS;
+    if (nblocks > NOALLOC_CFL_MAX_BLOCKS)
+        return fail(EU3D_ERR_ARG, "nblocks exceeds the 1024-entry scratch array of eu3d_cfl_noalloc");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(EU3D_ERR_ARG, "device ordinal beyond 63");
+    if (!g_cfl_scratch_dev[dev]) {
+        void *p = nullptr;
+        CK(cudaGetSymbolAddress(&p, g_cfl_scratch));
+        g_cfl_scratch_dev[dev] = (double *)p;
+    }
+    double *scratch = g_cfl_scratch_dev[dev];
+    CflFields f{D, U, V, W, Pp, Gamma, ni, nj, nk, bc, pitch, plane};
+    cudaStream_t st = (cudaStream_t)stream;
+    k_cfl_fields_partial<<<nblocks, 256, 0, st>>>(f, dx, dy, dz, use_z, scratch);
+    k_cfl_fields_final<<<1, 1024, 0, st>>>(scratch, nblocks, cfl, final_time, dt_out, time_inout);
+    CK(cudaGetLastError());
     return EU3D_OK;
 }
 

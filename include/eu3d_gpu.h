@@ -161,6 +161,28 @@ int eu3d_profile_read(eu3d_handle *h, char *names, size_t names_cap, double *ms,
 int eu3d_get_status(eu3d_handle *h, eu3d_status *st);
 int eu3d_reset_status(eu3d_handle *h);
 
+/* CFL time step that allocates nothing (no counterpart in the reference).
+   For callers that cannot allocate device memory -- code running while
+   another framework owns the memory pool and forbids allocations, or code
+   that must not call cudaMalloc/cudaFree because they synchronise the device.
+   The caller passes FP64 device fields D, U, V, W, P, Gamma on the ghosted
+   grid (index k*plane + j*pitch + i, x fastest) and caller-owned device
+   doubles time_inout and dt_out; the result follows CFLcondition
+   (src/Flowfield.cpp:242-272): dt = cfl * min over interior cells of
+   min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C) if use_z]), C = sqrt(Gamma P / D),
+   clipped so that time does not pass final_time, then time += dt.
+   Scratch: a fixed 1024-double device array inside the library (kept by every
+   GPU that loads it until exit); nblocks (reduction blocks, 0 = 592) above
+   1024 is rejected with EU3D_ERR_ARG.  The first call on a device looks up
+   that array's device address with the device current, so make it before any
+   stream capture.  All calls share the array: calls that overlap on the GPU
+   race.  Work is queued on `stream` (a cudaStream_t; NULL = default stream)
+   and the call does not synchronise. */
+int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const double *W, const double *P,
+                     const double *Gamma, int ni, int nj, int nk, int bc, long long pitch, long long plane,
+                     double dx, double dy, double dz, int use_z, double cfl, double final_time,
+                     double *time_inout, double *dt_out, int nblocks, void *stream);
+
 /* Pointer to the handle's CUDA stream (cudaStream_t), for callers that
    interleave their own work. */
 void *eu3d_stream(eu3d_handle *h);
