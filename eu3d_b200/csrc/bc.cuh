@@ -166,6 +166,7 @@ __global__ void k_wedge(GhostArgs a, P *q, const double *xn, const double *yn, d
     const Layout &L = a.L;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
+    const int k = blockIdx.z;
     if (i >= L.NI) return;
     const double x = xn[i], y = yn[j];
     if (!(x > x0 && (y - y0) < (x - x0) * tn)) return;
@@ -180,14 +181,12 @@ __global__ void k_wedge(GhostArgs a, P *q, const double *xn, const double *yn, d
     sj = sj < 0 ? 0 : (sj > L.NJ - 1 ? L.NJ - 1 : sj);
     while (sj < L.NJ - 1 && xn[si] > x0 && (yn[sj] - y0) < (xn[si] - x0) * tn) sj++;
     const long long fs = L.fs;
-    for (int k = 0; k < L.NK; k++) {
-        const long long d = L.at(i, j, k), s = L.at(si, sj, k);
-        ghost_copy(a, q, d, s);
-        const double u = (double)q[PU * fs + s], v = (double)q[PV * fs + s];
-        const double un = u * nx + v * ny;
-        q[PU * fs + d] = (P)(u - 2.0 * un * nx);
-        q[PV * fs + d] = (P)(v - 2.0 * un * ny);
-    }
+    const long long d = L.at(i, j, k), s = L.at(si, sj, k);
+    ghost_copy(a, q, d, s);
+    const double u = (double)q[PU * fs + s], v = (double)q[PV * fs + s];
+    const double un = u * nx + v * ny;
+    q[PU * fs + d] = (P)(u - 2.0 * un * nx);
+    q[PV * fs + d] = (P)(v - 2.0 * un * ny);
 }
 
 // CFL: block minima of min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C)]) over the

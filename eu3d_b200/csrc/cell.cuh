@@ -5,6 +5,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "mech_h2_ja919.cuh"
 
 namespace eu3d {
 
@@ -15,34 +16,61 @@ struct Decoded {
     double Y[NS];
 };
 
+// Mixture-averaged NASA-9 coefficients sum_s (Y_s Ri_s) a_k,s of the range
+// `hi`, b1 taken from range `rb` (the reference's high-range defect selects 0).
+__device__ __forceinline__ void mix_coeffs(const double yr[NS], int hi, int rb, double A[8])
+{
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        double a = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) a += yr[s] * cM.c[hi][k][s];
+        A[k] = a;
+    }
+    double b = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) b += yr[s] * cM.c[rb][7][s];
+    A[7] = b;
+}
+
 // Flowfield::Update_after_CS per cell (src/Flowfield.cpp:1246-1284) with
 // Flowfield::Get_temp (:1542-1566).  Eold is the E of the previous decode
-// (the Newton target under EU3D_Q_STALE_E); T0 the Newton start.
+// (the Newton target under EU3D_Q_STALE_E); T0 the Newton start.  The
+// reference sums Y_s Ri_s h_s(T) species by species at every iteration; the
+// same sums are formed here once per cell as mixture polynomial
+// coefficients, so an iteration evaluates one polynomial instead of nine
+// (equal up to rounding).
 __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eold, unsigned q, Decoded &o,
                                        int &capped)
 {
     double D = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) D += cs[s];
+    double yr[NS], sYR = 0.0, sdiv = 0.0;
 #pragma unroll
-    for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
+    for (int s = 0; s < NS; s++) {
+        o.Y[s] = cs[s] / D;
+        yr[s] = o.Y[s] * cM.ri[s];
+        sYR += yr[s];
+        sdiv += o.Y[s] / cM.mw[s];
+    }
     const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
     const double Enew = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) / D;
     const double Et = (q & EU3D_Q_STALE_E) ? Eold : Enew;
-    double sYR = 0.0;
-#pragma unroll
-    for (int s = 0; s < NS; s++) sYR += o.Y[s] * cM.ri[s];
+    double A[8];
+    int cur = -1;
     double Tn = T0, Tp;
     int count = 0;
     while (count < 10) {
         Tp = Tn;
         const TPow p = tpow(Tp, q);
-        double sh = 0.0, scp = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            sh += o.Y[s] * (cM.ri[s] * h_r(s, p));
-            scp += o.Y[s] * (cM.ri[s] * cp_r(s, p));
+        if (p.hi != cur) {
+            cur = p.hi;
+            mix_coeffs(yr, p.hi, p.rb, A);
         }
+        const double sh = -A[0] * p.tm1 + A[1] * p.lnT + A[2] * p.T + A[3] * p.t2 * 0.5 +
+                          A[4] * p.t3 * (1.0 / 3.0) + A[5] * p.t4 * 0.25 + A[6] * p.t5 * 0.2 + A[7];
+        const double scp = A[0] * p.tm2 + A[1] * p.tm1 + A[2] + A[3] * p.T + A[4] * p.t2 + A[5] * p.t3 + A[6] * p.t4;
         const double t1 = (sh - Et * 1e-3) - sYR * Tp;
         const double t2 = scp - sYR;
         Tn = Tp - t1 / t2;
@@ -51,12 +79,8 @@ __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eo
     }
     capped = count >= 10;
     const TPow p = tpow(Tn, q);
-    double sdiv = 0.0, scp = 0.0;
-#pragma unroll
-    for (int s = 0; s < NS; s++) {
-        sdiv += o.Y[s] / cM.mw[s];
-        scp += (cM.ri[s] * cp_r(s, p)) * o.Y[s];
-    }
+    if (p.hi != cur) mix_coeffs(yr, p.hi, p.rb, A);
+    const double scp = A[0] * p.tm2 + A[1] * p.tm1 + A[2] + A[3] * p.T + A[4] * p.t2 + A[5] * p.t3 + A[6] * p.t4;
     const double Wav = 1.0 / sdiv;
     o.Rgas = R_GAS * 1000 / Wav;
     o.P = Tn * D * o.Rgas;
@@ -143,11 +167,10 @@ __device__ __forceinline__ void gibbs(const TPow &p, double G[NS])
 
 // Reaction::Diagonalized per cell (src/Reaction.cpp:736-811): source CMS and
 // diagonal Jacobian MD of the partial densities.  Mc in mol/cm^3, Di in g/cm^3.
-__device__ __forceinline__ void diagonalized(const TPow &p, const double Mc[NS], const double Di[NS], const double PT[NS],
-                                             double CMS[NS], double MD[NS])
+__device__ __forceinline__ void diagonalized(const TPow &p, const double G[NS], const double Mc[NS], const double Di[NS],
+                                             const double PT[NS], double CMS[NS], double MD[NS])
 {
-    double G[NS], Wi[NS];
-    gibbs(p, G);
+    double Wi[NS];
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         Wi[s] = 0.0;
@@ -177,10 +200,11 @@ __device__ __forceinline__ void diagonalized(const TPow &p, const double Mc[NS],
 // Point-implicit trapezoid update of one cell (src/Reaction.cpp:412-485,
 // :489-591): Di in kg/m^3 in and out.  Wi (net production, g/cm^3/s) is
 // returned for the substep prediction.
+template <bool SPEC>
 __device__ __forceinline__ void trapezoid(const TPow &p, const double cs_di[NS], double dt, int rtb_mode, double out[NS],
                                           double Wi[NS])
 {
-    double Mc[NS], Di[NS], G[NS], Pv[NS], Qv[NS];
+    double Mc[NS], Di[NS], Pv[NS], Qv[NS];
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         Di[s] = cs_di[s] * 1e-3;
@@ -189,20 +213,26 @@ __device__ __forceinline__ void trapezoid(const TPow &p, const double cs_di[NS],
         Qv[s] = 0.0;
         Wi[s] = 0.0;
     }
-    gibbs(p, G);
+    if (SPEC) {
+        h2ja919::trap_rates_spec(p, Mc, rtb_mode, Wi, Pv, Qv);
+    } else {
+        double G[NS];
+        gibbs(p, G);
 #pragma unroll 1
-    for (int r = 0; r < NR; r++) {
-        const Rxn x = rxn(r, p, Mc, G, rtb_mode);
+        for (int r = 0; r < NR; r++) {
+            const Rxn x = rxn(r, p, Mc, G, rtb_mode);
 #pragma unroll
-        for (int s = 0; s < NS; s++) {
-            Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
-            Qv[s] += (cM.sb[s][r] * x.KF * x.RRF + cM.sf[s][r] * x.KB * x.RRB * x.RTB);
-            Pv[s] += (cM.sb[s][r] * x.KB * x.RRB + cM.sf[s][r] * x.KF * x.RRF * x.RTB);
+            for (int s = 0; s < NS; s++) {
+                Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
+                Qv[s] += (cM.sb[s][r] * x.KF * x.RRF + cM.sf[s][r] * x.KB * x.RRB * x.RTB);
+                Pv[s] += (cM.sb[s][r] * x.KB * x.RRB + cM.sf[s][r] * x.KF * x.RRF * x.RTB);
+            }
         }
+#pragma unroll
+        for (int s = 0; s < NS; s++) Wi[s] = cM.mw[s] * Wi[s];
     }
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        Wi[s] = cM.mw[s] * Wi[s];
         const double q = cM.mw[s] * Qv[s];
         const double pp = (Mc[s] == 0) ? 0.0 : Pv[s] / Mc[s];
         out[s] = ((1.0 - dt / 2.0 * pp) * Di[s] + dt * q) / (1.0 + dt / 2.0 * pp) * 1e3;
@@ -210,26 +240,35 @@ __device__ __forceinline__ void trapezoid(const TPow &p, const double cs_di[NS],
 }
 
 // Reaction::TrapezoidPrediction per cell (src/Reaction.cpp:593-670)
+template <bool SPEC>
 __device__ __forceinline__ int predict_nchem(const TPow &p, const double cs_di[NS], const double Y[NS], double dtm,
                                              int rtb_mode)
 {
-    double Mc[NS], G[NS], Wi[NS];
+    double Mc[NS], Wi[NS];
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         Mc[s] = (cs_di[s] / cM.mw[s] * 1000) * 1e-6;
         Wi[s] = 0.0;
     }
-    gibbs(p, G);
+    if (SPEC) {
+        double Pv[NS], Qv[NS];
+        h2ja919::trap_rates_spec(p, Mc, rtb_mode, Wi, Pv, Qv);
+    } else {
+        double G[NS];
+        gibbs(p, G);
 #pragma unroll 1
-    for (int r = 0; r < NR; r++) {
-        const Rxn x = rxn(r, p, Mc, G, rtb_mode);
+        for (int r = 0; r < NR; r++) {
+            const Rxn x = rxn(r, p, Mc, G, rtb_mode);
 #pragma unroll
-        for (int s = 0; s < NS; s++) Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
+            for (int s = 0; s < NS; s++) Wi[s] += cM.nu[s][r] * x.RTB * x.RR;
+        }
+#pragma unroll
+        for (int s = 0; s < NS; s++) Wi[s] = cM.mw[s] * Wi[s];
     }
     double dt = dtm;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        const double w = cM.mw[s] * Wi[s];
+        const double w = Wi[s];
         if (Y[s] >= 1e-6 && w != 0) {
             const double t = fabs(-(cs_di[s] * 1e-3) / w);
             if (t < dt) dt = t;
@@ -307,7 +346,7 @@ __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
 //  M_TRAP1   Update_after_Adv, TrapezoidPrediction and the per-cell substeps
 //  M_RK_STAGE1/2  SSP-RK2 stage updates (new)
 //  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
-template <class P, int MODE>
+template <class P, int MODE, bool SPEC>
 __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
 {
     const Layout &L = a.L;
@@ -333,24 +372,39 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
         for (int s = 0; s < NS; s++) D += cs[s];
         const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
         const TPow p = tpow(T, qk);
-        double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], CMS[NS], MD[NS];
+        double hr[NS], sr[NS], cpr[NS];
+        if (SPEC) {
+            h2ja919::thermo_spec(p, hr, sr, cpr);
+        } else {
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                hr[s] = h_r(s, p);
+                sr[s] = s_r(s, p);
+                cpr[s] = cp_r(s, p);
+            }
+        }
+        double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], G[NS], CMS[NS], MD[NS];
 #pragma unroll
         for (int s = 0; s < NS; s++) {
             const double Y = cs[s] / D;
             sdiv += Y / cM.mw[s];
-            scp += (cM.ri[s] * cp_r(s, p)) * Y;
+            scp += (cM.ri[s] * cpr[s]) * Y;
         }
         const double Rgas = R_GAS * 1000 / (1.0 / sdiv);
         const double CV = scp * 1000 - Rgas;
         const double ke = 0.5 * (U * U + V * V + W * W);
-        // GetPartial_T, src/Flowfield.cpp:1578-1595
+        // GetPartial_T, src/Flowfield.cpp:1578-1595; Gibbs energies for the rates
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-            PT[s] = (ke - cM.ri[s] * h_r(s, p) + cM.ri[s] * 1e3 * T) / (CV * D);
+            PT[s] = (ke - cM.ri[s] * hr[s] + cM.ri[s] * 1e3 * T) / (CV * D);
+            G[s] = R_GAS * hr[s] - (R_GAS * sr[s]) * T;
             Di[s] = cs[s] * 1e-3;
             Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;
         }
-        diagonalized(p, Mc, Di, PT, CMS, MD);
+        if (SPEC)
+            h2ja919::diagonalized_spec(p, G, Mc, Di, PT, CMS, MD);
+        else
+            diagonalized(p, G, Mc, Di, PT, CMS, MD);
         // Flowfield::Update_IMEX, src/Flowfield.cpp:1219-1228
 #pragma unroll
         for (int v = 0; v < NV; v++) {
@@ -392,7 +446,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
             double dn[NS], Wi[NS];
             if (MODE == M_TRAP0) {
                 const int rtb = (qk & EU3D_Q_TRAP_RTB_ZERO) ? 1 : 0;
-                trapezoid(tpow(o.T, qk), cs, dt, rtb, dn, Wi);
+                trapezoid<SPEC>(tpow(o.T, qk), cs, dt, rtb, dn, Wi);
             } else {
 #pragma unroll
                 for (int s = 0; s < NS; s++) dn[s] = cs[s];
@@ -418,7 +472,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
             capped_any |= capped;
         } else if (MODE == M_TRAP1) {
             const int rtb = (qk & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
-            int n = predict_nchem(tpow(o.T, qk), cs, o.Y, dt, rtb);
+            int n = predict_nchem<SPEC>(tpow(o.T, qk), cs, o.Y, dt, rtb);
             const bool over = n > NCHEM_CAP;
             if (over) n = NCHEM_CAP;
             if (over) atomicAdd(&a.st->substep_capped, 1);
@@ -427,7 +481,7 @@ __global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
             const double dts = dt / n;
             for (int step = 0; step < n; step++) {
                 double dn[NS], Wi[NS];
-                trapezoid(tpow(o.T, qk), cs, dts, rtb, dn, Wi);
+                trapezoid<SPEC>(tpow(o.T, qk), cs, dts, rtb, dn, Wi);
                 // Flowfield::Explicit(step, i, j, k), src/Flowfield.cpp:1189-1203
                 double D = 0.0;
 #pragma unroll

@@ -71,6 +71,8 @@ struct eu3d_handle {
     size_t stage_bytes = 0;
     double wedge[3] = {0, 0, 0};
     int wedge_on = 0;
+    bool spec = false;  // mechanism equals the compiled-in H2_JA919 tables
+    int flux_kz = 16;   // z planes walked by one flux block
     std::map<StepKey, cudaGraphExec_t> graphs;
     // per-kernel CUDA-event timing (eu3d_profile_enable)
     bool profile = false;
@@ -146,8 +148,8 @@ CellArgs cell_args(eu3d_handle *h)
 
 dim3 cell_grid(const Layout &L, int bx) { return dim3((L.ni + bx - 1) / bx, L.nj, L.nk); }
 
-template <class P>
-void launch_cell(eu3d_handle *h, int mode)
+template <class P, bool SPEC>
+void launch_cell_t(eu3d_handle *h, int mode)
 {
     CellArgs a = cell_args(h);
     P *q = (P *)h->prim;
@@ -156,15 +158,24 @@ void launch_cell(eu3d_handle *h, int mode)
                                   "cell_rk2", "cell_nochem"};
     ProfScope ps(h, names[mode]);
     switch (mode) {
-    case M_DECODE: k_cell<P, M_DECODE><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_ADV: k_cell<P, M_ADV><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_IMEX: k_cell<P, M_IMEX><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_TRAP0: k_cell<P, M_TRAP0><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_TRAP1: k_cell<P, M_TRAP1><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_RK_STAGE1: k_cell<P, M_RK_STAGE1><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_RK_STAGE2: k_cell<P, M_RK_STAGE2><<<g, 128, 0, h->st>>>(a, q); break;
-    case M_NOCHEM: k_cell<P, M_NOCHEM><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_DECODE: k_cell<P, M_DECODE, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_ADV: k_cell<P, M_ADV, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_IMEX: k_cell<P, M_IMEX, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_TRAP0: k_cell<P, M_TRAP0, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_TRAP1: k_cell<P, M_TRAP1, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK_STAGE1: k_cell<P, M_RK_STAGE1, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK_STAGE2: k_cell<P, M_RK_STAGE2, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_NOCHEM: k_cell<P, M_NOCHEM, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     }
+}
+
+template <class P>
+void launch_cell(eu3d_handle *h, int mode)
+{
+    if (h->spec)
+        launch_cell_t<P, true>(h, mode);
+    else
+        launch_cell_t<P, false>(h, mode);
 }
 
 int cell_op(eu3d_handle *h, int mode)
@@ -181,14 +192,18 @@ template <class P>
 void launch_adv(eu3d_handle *h, int diff)
 {
     const int sq = (h->quirks & EU3D_Q_SPECIES_FACES) ? 1 : 0;
-    dim3 g = cell_grid(h->L, 128);
+    const Layout &L = h->L;
+    const int kz = h->flux_kz;
+    constexpr int TY = FluxTile<P>::TY;
+    dim3 g((L.ni + FT_X - 1) / FT_X, (L.nj + TY - 1) / TY, (L.nk + kz - 1) / kz);
+    dim3 b(FT_X, TY);
     ProfScope ps(h, "advection");
     if (diff == EU3D_DIFF_MUSCL1)
-        k_advection<P, EU3D_DIFF_MUSCL1><<<g, 128, 0, h->st>>>(h->L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                                h->rhs, sq);
+        k_flux_tile<P, EU3D_DIFF_MUSCL1><<<g, b, 0, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                              h->rhs, sq, kz);
     else
-        k_advection<P, EU3D_DIFF_MUSCL2><<<g, 128, 0, h->st>>>(h->L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                                h->rhs, sq);
+        k_flux_tile<P, EU3D_DIFF_MUSCL2><<<g, b, 0, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                              h->rhs, sq, kz);
 }
 
 int adv_op(eu3d_handle *h, int timeadv, int diff)
@@ -233,7 +248,7 @@ void launch_ghost(eu3d_handle *h, int kind)
         }
     }
     if (h->wedge_on) {
-        dim3 gw((L.NI + 127) / 128, L.NJ);
+        dim3 gw((L.NI + 127) / 128, L.NJ, L.NK);
         ProfScope ps(h, "wedge");
         k_wedge<P><<<gw, 128, 0, h->st>>>(a, q, h->xn, h->yn, h->wedge[0], h->wedge[1], h->wedge[2]);
     }
@@ -620,6 +635,17 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
 
     eu3d_handle *h = new eu3d_handle();
     h->dev = d->device;
+    {
+        using namespace h2ja919;
+        bool same = true;
+        for (int q = 0; q < NS * NR; q++)
+            same = same && d->stoi_f[q] == K_STOI_F[q] && d->stoi_b[q] == K_STOI_B[q] && d->react_tb[q] == K_TB[q];
+        for (int r = 0; r < NR; r++) same = same && d->af[r] == K_AF[r] && d->bf[r] == K_BF[r] && d->eaf[r] == K_EAF[r];
+        for (int q = 0; q < 9 * NS; q++) same = same && d->coeff0[q] == K_C0[q] && d->coeff1[q] == K_C1[q];
+        for (int q = 0; q < NS; q++) same = same && d->mw[q] == K_MW[q];
+        const char *env = getenv("EU3D_GENERIC_CHEM");
+        h->spec = same && !(env && env[0] == '1');
+    }
     h->flux_bits = d->flux_bits;
     h->quirks = d->quirks;
     Layout &L = h->L;

@@ -7,13 +7,14 @@
 //
 // The reference materialises left/right states of 16 primitives per
 // direction into full-size arrays, then face fluxes F, G, Q, then RHS.  Here
-// no intermediate array exists: k_advection gives each interior cell one
-// thread, which reconstructs the two faces of the cell in each direction from
-// the primitives (read through the read-only cache) and writes only the
-// residual
+// no intermediate array exists: k_flux_tile computes each face flux once per
+// step (x and y faces of a block's tile through shared memory, z faces in
+// registers while the block walks its z planes) and writes only the residual
 //     RHS = -dt/dx (F_i - F_{i-1}) - dt/dy (G_j - G_{j-1}) - dt/dz (Q_k - Q_{k-1})
 // accumulated in FP64 in the reference's operation order.  Reconstruction
 // and AUSM run in P (double or float); differences and the residual in FP64.
+// k_advection (one thread per cell, both faces per direction) is the
+// straightforward form, kept for cross-checking the tiled kernel.
 #pragma once
 
 #include "common.cuh"
@@ -45,6 +46,30 @@ __device__ __forceinline__ void recon(P a, P b, P c, P d, P &L, P &R)
     P L1 = minmod_lim(Lr), L2 = minmod_lim(P(1.0) / Lr), R1 = minmod_lim(Rr), R2 = minmod_lim(P(1.0) / Rr);
     L = b + P(0.25) * ((P(1.0) - kk) * L1 + (P(1) + kk) * L2 * Lr) * A0;
     R = c - P(0.25) * ((P(1.0) - kk) * R1 + (P(1) + kk) * R2 * Rr) * A2;
+}
+
+// One side of recon(): the left state from f(i-1), f(i), f(i+1) or the right
+// state from f(i), f(i+1), f(i+2) (identical arithmetic).
+template <class P, int DIFF>
+__device__ __forceinline__ P recon_left(P a, P b, P c)
+{
+    if (DIFF == EU3D_DIFF_MUSCL1) return b;
+    const P kk = P(1.0) / P(3.0);
+    P A0 = b - a, A1 = c - b;
+    P Lr = A1 / (A0 + P(1e-12));
+    P L1 = minmod_lim(Lr), L2 = minmod_lim(P(1.0) / Lr);
+    return b + P(0.25) * ((P(1.0) - kk) * L1 + (P(1) + kk) * L2 * Lr) * A0;
+}
+
+template <class P, int DIFF>
+__device__ __forceinline__ P recon_right(P b, P c, P d)
+{
+    if (DIFF == EU3D_DIFF_MUSCL1) return c;
+    const P kk = P(1.0) / P(3.0);
+    P A1 = c - b, A2 = d - c;
+    P Rr = A1 / (A2 + P(1e-12));
+    P R1 = minmod_lim(Rr), R2 = minmod_lim(P(1.0) / Rr);
+    return c - P(0.25) * ((P(1.0) - kk) * R1 + (P(1) + kk) * R2 * Rr) * A2;
 }
 
 // AUSM face flux (src/Flowfield.cpp:1395-1500) from reconstructed states.
@@ -113,6 +138,140 @@ __device__ __forceinline__ void face_flux_g(const P *__restrict__ q, long long f
         }
     }
     ausm<P, DIR>(ql, qr, yl, yr, out);
+}
+
+// Face flux between cells a and a+1 (cells a-1 .. a+2 along the direction,
+// element stride st, c0 the index of cell a-1).  Only the states AUSM reads
+// are reconstructed: both sides of P, D, gamma and the normal velocity (they
+// set the interface Mach number), then only the upwind side of the
+// tangential velocities, H and the species.  Same values as face_flux_g.
+template <class P, int DIR, int DIFF>
+__device__ __forceinline__ void face_flux_up(const P *__restrict__ q, long long fs, long long c0, long long st,
+                                             bool zspec, P out[NV])
+{
+    auto rc = [&](int f, P &L, P &R) {
+        const P *b = q + f * fs + c0;
+        recon<P, DIFF>(__ldg(b), __ldg(b + st), __ldg(b + 2 * st), __ldg(b + 3 * st), L, R);
+    };
+    constexpr int FN = DIR == 1 ? PU : DIR == 2 ? PV : PW;
+    P DL, DR, PL, PR, GL, GR, NL, NR;
+    rc(PD, DL, DR);
+    rc(PP, PL, PR);
+    rc(PG, GL, GR);
+    rc(FN, NL, NR);
+    const P CL = sqrt(GL * PL / DL);
+    const P CR = sqrt(GR * PR / DR);
+    const P CI = P(0.5) * (CL + CR);
+    const P MaL = NL / CI, MaR = NR / CI;
+    P B1, G1, B2, G2;
+    if (fabs(MaL) < P(1.0)) {
+        P mp = MaL + P(1.0), m2 = MaL * MaL - P(1.0);
+        B1 = P(0.25) * (mp * mp) + P(0.125) * (m2 * m2);
+        G1 = P(0.25) * (mp * mp) * (P(2.0) - MaL) + P(3.0) / P(16.0) * MaL * (m2 * m2);
+    } else {
+        B1 = P(0.5) * (MaL + fabs(MaL));
+        G1 = B1 / MaL;
+    }
+    if (fabs(MaR) < P(1.0)) {
+        P mm = MaR - P(1.0), m2 = MaR * MaR - P(1.0);
+        B2 = P(-0.25) * (mm * mm) - P(0.125) * (m2 * m2);
+        G2 = P(0.25) * (mm * mm) * (P(2.0) + MaR) - P(3.0) / P(16.0) * MaR * (m2 * m2);
+    } else {
+        B2 = P(0.5) * (MaR - fabs(MaR));
+        G2 = B2 / MaR;
+    }
+    const P VI = (B1 + B2) * CI;
+    const bool left = VI >= P(0.0);
+    // upwind-side reconstruction of one field
+    auto up = [&](int f) -> P {
+        const P *b = q + f * fs + c0;
+        return left ? recon_left<P, DIFF>(__ldg(b), __ldg(b + st), __ldg(b + 2 * st))
+                    : recon_right<P, DIFF>(__ldg(b + st), __ldg(b + 2 * st), __ldg(b + 3 * st));
+    };
+    const P Ds = left ? DL : DR;
+    const P Us = DIR == 1 ? (left ? NL : NR) : up(PU);
+    const P Vs = DIR == 2 ? (left ? NL : NR) : up(PV);
+    const P Ws = DIR == 3 ? (left ? NL : NR) : up(PW);
+    const P Hs = up(PH);
+    const P VD = VI * Ds;
+#pragma unroll
+    for (int s = 0; s < NS; s++) out[s] = zspec ? P(0) * VD : VD * up(PY + s);
+    out[NS] = VD * Us;
+    out[NS + 1] = VD * Vs;
+    out[NS + 2] = VD * Ws;
+    if (DIR == 1) out[NS] = VD * Us + G1 * PL + G2 * PR;
+    if (DIR == 2) out[NS + 1] = VD * Vs + G1 * PL + G2 * PR;
+    if (DIR == 3) out[NS + 2] = VD * Ws + G1 * PL + G2 * PR;
+    out[NS + 3] = VI * (Ds * Hs + P(0.5) * Ds * (Us * Us + Vs * Vs + Ws * Ws));
+}
+
+constexpr int FT_X = 32;
+// tile height: 8 rows for FP32 primitives, 4 for FP64 (static shared memory)
+template <class P>
+struct FluxTile {
+    static constexpr int TY = sizeof(P) == 8 ? 4 : 8;
+};
+
+// Tiled flux + residual kernel.  A block owns a 32 x TY tile of x-y columns
+// and walks `kz` z planes.  At each plane every x face and y face of the tile
+// is computed once (by one thread) into shared memory, every z face once in
+// registers (the face below a cell is the face above the previous plane's
+// cell), and each thread then forms its cell's residual in the reference's
+// order ((-dt/dx dF - dt/dy dG) - dt/dz dQ) in FP64.
+template <class P, int DIFF>
+__global__ void __launch_bounds__(FT_X * FluxTile<P>::TY) k_flux_tile(
+    Layout L, const P *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
+    const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
+{
+    constexpr int TY = FluxTile<P>::TY;
+    __shared__ P fx[TY][FT_X + 1][NV];
+    __shared__ P fy[TY + 1][FT_X][NV];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
+    const int kb = L.bc + blockIdx.z * kz;
+    const int ke = min(kb + kz, L.nk + L.bc);
+    const int i = i0 + tx, j = j0 + ty;
+    const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
+    const bool act = i <= ilast && j <= jlast;
+    const long long fs = L.fs, sy = L.px, sz = (long long)L.px * L.NJ;
+    const double dt = *dtp;
+    const bool zs_cell = species_quirk && i >= L.ni;
+    P qb[NV], qa[NV];
+    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
+    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    if (act) face_flux_up<P, 3, DIFF>(q, fs, L.at(i, j, kb) - 2 * sz, sz, zs_cell, qb);
+    for (int k = kb; k < ke; k++) {
+        // x faces of row j: face f sits between a = i0+f-1 and a+1 and is
+        // needed when a <= ilast; it reads cells a-1 .. a+2
+        if (j <= jlast) {
+            for (int f = tx; f <= FT_X; f += FT_X) {
+                const int a = i0 + f - 1;
+                if (a <= ilast)
+                    face_flux_up<P, 1, DIFF>(q, fs, L.at(a - 1, j, k), 1, species_quirk && a >= L.ni, fx[ty][f]);
+            }
+        }
+        // y faces of column i: face g sits between b = j0+g-1 and b+1
+        if (i <= ilast) {
+            for (int g = ty; g <= TY; g += TY) {
+                const int b = j0 + g - 1;
+                if (b <= jlast) face_flux_up<P, 2, DIFF>(q, fs, L.at(i, b - 1, k), sy, zs_cell, fy[g][tx]);
+            }
+        }
+        if (act) face_flux_up<P, 3, DIFF>(q, fs, L.at(i, j, k) - sz, sz, zs_cell, qa);
+        __syncthreads();
+        if (act) {
+            const double cz = dt / (zn[k] - zn[k - 1]);
+            const long long c = L.at(i, j, k);
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                double r = ax * ((double)fx[ty][tx + 1][v] - (double)fx[ty][tx][v]);
+                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
+                rhs[v * fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
+                qb[v] = qa[v];
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // One thread per interior cell; both faces of each direction are evaluated
