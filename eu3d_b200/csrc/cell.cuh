@@ -347,7 +347,7 @@ __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
 //  M_RK_STAGE1/2  SSP-RK2 stage updates (new)
 //  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
 template <class P, int MODE, bool SPEC>
-__global__ void __launch_bounds__(128) k_cell(CellArgs a, P *__restrict__ q)
+__global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
 {
     const Layout &L = a.L;
     const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;

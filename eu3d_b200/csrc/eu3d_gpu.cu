@@ -197,13 +197,14 @@ void launch_adv(eu3d_handle *h, int diff)
     constexpr int TY = FluxTile<P>::TY;
     dim3 g((L.ni + FT_X - 1) / FT_X, (L.nj + TY - 1) / TY, (L.nk + kz - 1) / kz);
     dim3 b(FT_X, TY);
+    constexpr size_t smem = FluxTile<P>::SMEM;
     ProfScope ps(h, "advection");
     if (diff == EU3D_DIFF_MUSCL1)
-        k_flux_tile<P, EU3D_DIFF_MUSCL1><<<g, b, 0, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                              h->rhs, sq, kz);
+        k_flux_tile<P, EU3D_DIFF_MUSCL1><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                                 h->rhs, sq, kz);
     else
-        k_flux_tile<P, EU3D_DIFF_MUSCL2><<<g, b, 0, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                              h->rhs, sq, kz);
+        k_flux_tile<P, EU3D_DIFF_MUSCL2><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
+                                                                 h->rhs, sq, kz);
 }
 
 int adv_op(eu3d_handle *h, int timeadv, int diff)
@@ -658,6 +659,10 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     L.NK = d->nk + 2 * d->bc;
     L.px = (L.NI + 31) / 32 * 32;
     L.fs = (long long)L.px * L.NJ * L.NK;
+    if ((long long)NPRIM * L.fs >= (1LL << 31)) {
+        delete h;
+        return fail(EU3D_ERR_ARG, "grid too large for one handle (primitive fields exceed 2^31 elements)");
+    }
     const size_t f8 = (size_t)L.fs * sizeof(double);
 #define ALLOC(p, bytes)                                                                    \
     do {                                                                                   \
@@ -696,6 +701,17 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     cudaMemcpyAsync(h->xn, d->xnode, L.NI * sizeof(double), cudaMemcpyHostToDevice, h->st);
     cudaMemcpyAsync(h->yn, d->ynode, L.NJ * sizeof(double), cudaMemcpyHostToDevice, h->st);
     cudaMemcpyAsync(h->zn, d->znode, L.NK * sizeof(double), cudaMemcpyHostToDevice, h->st);
+    {
+        // dynamic shared memory of the tiled flux kernels (above the 48 KB default)
+        cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxTile<float>::SMEM);
+        cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxTile<float>::SMEM);
+        cudaFuncSetAttribute(k_flux_tile<double, EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxTile<double>::SMEM);
+        cudaFuncSetAttribute(k_flux_tile<double, EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxTile<double>::SMEM);
+    }
     if (g_mech_refs == 0) {
         cudaError_t e = cudaMemcpyToSymbol(cM, &m, sizeof(m));
         if (e != cudaSuccess) {

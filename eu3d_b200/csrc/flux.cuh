@@ -72,6 +72,32 @@ __device__ __forceinline__ P recon_right(P b, P c, P d)
     return c - P(0.25) * ((P(1.0) - kk) * R1 + (P(1) + kk) * R2 * Rr) * A2;
 }
 
+// FP32 path: the same limited states without divisions.  With the minmod
+// limiter and kappa = 1/3, recon() reduces to
+//     left  = f_i   + 0.5 * (L >= 1 ? A0 : L A0),  L = A1 / (A0 + 1e-12) > 0, else f_i
+//     right = f_i+1 - 0.5 * (R >= 1 ? A2 : R A2),  R = A1 / (A2 + 1e-12) > 0, else f_i+1
+// and L A0 = A1 A0 / (A0 + 1e-12) is taken as A1 (relative difference
+// 1e-12 / |A0|, far below FP32 resolution unless the slope itself is ~1e-12).
+template <>
+__device__ __forceinline__ float recon_left<float, EU3D_DIFF_MUSCL2>(float a, float b, float c)
+{
+    const float A0 = b - a, A1 = c - b, d = A0 + 1e-12f;
+    if (!(A1 * d > 0.f)) return b;
+    return b + 0.5f * (fabsf(A1) >= fabsf(d) ? A0 : A1);
+}
+
+template <>
+__device__ __forceinline__ float recon_right<float, EU3D_DIFF_MUSCL2>(float b, float c, float d)
+{
+    const float A1 = c - b, A2 = d - c, e = A2 + 1e-12f;
+    if (!(A1 * e > 0.f)) return c;
+    return c - 0.5f * (fabsf(A1) >= fabsf(e) ? A2 : A1);
+}
+
+// a / b: IEEE in FP64 (parity path), the fast approximate form in FP32
+__device__ __forceinline__ double pdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float pdiv(float a, float b) { return __fdividef(a, b); }
+
 // AUSM face flux (src/Flowfield.cpp:1395-1500) from reconstructed states.
 // ql/qr hold D U V W P H G; species are passed through yl/yr.
 template <class P, int DIR>
@@ -146,23 +172,25 @@ __device__ __forceinline__ void face_flux_g(const P *__restrict__ q, long long f
 // set the interface Mach number), then only the upwind side of the
 // tangential velocities, H and the species.  Same values as face_flux_g.
 template <class P, int DIR, int DIFF>
-__device__ __forceinline__ void face_flux_up(const P *__restrict__ q, long long fs, long long c0, long long st,
-                                             bool zspec, P out[NV])
+__device__ __forceinline__ void face_flux_up(const P *__restrict__ qc, int fs, int st, bool zspec, P out[NV])
 {
-    auto rc = [&](int f, P &L, P &R) {
-        const P *b = q + f * fs + c0;
-        recon<P, DIFF>(__ldg(b), __ldg(b + st), __ldg(b + 2 * st), __ldg(b + 3 * st), L, R);
+    // qc points at cell a-1 of field 0; field f of cell a-1+n is qc[f * fs + n * st]
+    auto ld = [&](int f, int n) -> P { return __ldg(qc + f * fs + n * st); };
+    auto both = [&](int f, P &L, P &R) {
+        const P v0 = ld(f, 0), v1 = ld(f, 1), v2 = ld(f, 2), v3 = ld(f, 3);
+        L = recon_left<P, DIFF>(v0, v1, v2);
+        R = recon_right<P, DIFF>(v1, v2, v3);
     };
     constexpr int FN = DIR == 1 ? PU : DIR == 2 ? PV : PW;
     P DL, DR, PL, PR, GL, GR, NL, NR;
-    rc(PD, DL, DR);
-    rc(PP, PL, PR);
-    rc(PG, GL, GR);
-    rc(FN, NL, NR);
-    const P CL = sqrt(GL * PL / DL);
-    const P CR = sqrt(GR * PR / DR);
+    both(PD, DL, DR);
+    both(PP, PL, PR);
+    both(PG, GL, GR);
+    both(FN, NL, NR);
+    const P CL = sqrt(pdiv(GL * PL, DL));
+    const P CR = sqrt(pdiv(GR * PR, DR));
     const P CI = P(0.5) * (CL + CR);
-    const P MaL = NL / CI, MaR = NR / CI;
+    const P MaL = pdiv(NL, CI), MaR = pdiv(NR, CI);
     P B1, G1, B2, G2;
     if (fabs(MaL) < P(1.0)) {
         P mp = MaL + P(1.0), m2 = MaL * MaL - P(1.0);
@@ -170,7 +198,7 @@ __device__ __forceinline__ void face_flux_up(const P *__restrict__ q, long long 
         G1 = P(0.25) * (mp * mp) * (P(2.0) - MaL) + P(3.0) / P(16.0) * MaL * (m2 * m2);
     } else {
         B1 = P(0.5) * (MaL + fabs(MaL));
-        G1 = B1 / MaL;
+        G1 = pdiv(B1, MaL);
     }
     if (fabs(MaR) < P(1.0)) {
         P mm = MaR - P(1.0), m2 = MaR * MaR - P(1.0);
@@ -178,15 +206,13 @@ __device__ __forceinline__ void face_flux_up(const P *__restrict__ q, long long 
         G2 = P(0.25) * (mm * mm) * (P(2.0) + MaR) - P(3.0) / P(16.0) * MaR * (m2 * m2);
     } else {
         B2 = P(0.5) * (MaR - fabs(MaR));
-        G2 = B2 / MaR;
+        G2 = pdiv(B2, MaR);
     }
     const P VI = (B1 + B2) * CI;
     const bool left = VI >= P(0.0);
     // upwind-side reconstruction of one field
     auto up = [&](int f) -> P {
-        const P *b = q + f * fs + c0;
-        return left ? recon_left<P, DIFF>(__ldg(b), __ldg(b + st), __ldg(b + 2 * st))
-                    : recon_right<P, DIFF>(__ldg(b + st), __ldg(b + 2 * st), __ldg(b + 3 * st));
+        return left ? recon_left<P, DIFF>(ld(f, 0), ld(f, 1), ld(f, 2)) : recon_right<P, DIFF>(ld(f, 1), ld(f, 2), ld(f, 3));
     };
     const P Ds = left ? DL : DR;
     const P Us = DIR == 1 ? (left ? NL : NR) : up(PU);
@@ -206,10 +232,14 @@ __device__ __forceinline__ void face_flux_up(const P *__restrict__ q, long long 
 }
 
 constexpr int FT_X = 32;
-// tile height: 8 rows for FP32 primitives, 4 for FP64 (static shared memory)
+// tile height: 8 rows for FP32 primitives, 4 for FP64; face fluxes live in
+// dynamic shared memory (two buffers of x and y faces)
 template <class P>
 struct FluxTile {
     static constexpr int TY = sizeof(P) == 8 ? 4 : 8;
+    static constexpr int FX = TY * (FT_X + 1) * NV;  // elements of one x-face buffer
+    static constexpr int FY = (TY + 1) * FT_X * NV;  // elements of one y-face buffer
+    static constexpr size_t SMEM = sizeof(P) * 2 * (FX + FY);
 };
 
 // Tiled flux + residual kernel.  A block owns a 32 x TY tile of x-y columns
@@ -219,13 +249,15 @@ struct FluxTile {
 // cell), and each thread then forms its cell's residual in the reference's
 // order ((-dt/dx dF - dt/dy dG) - dt/dz dQ) in FP64.
 template <class P, int DIFF>
-__global__ void __launch_bounds__(FT_X * FluxTile<P>::TY) k_flux_tile(
+__global__ void __launch_bounds__(FT_X * FluxTile<P>::TY, 3) k_flux_tile(
     Layout L, const P *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
     const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
 {
     constexpr int TY = FluxTile<P>::TY;
-    __shared__ P fx[TY][FT_X + 1][NV];
-    __shared__ P fy[TY + 1][FT_X][NV];
+    // two buffers: plane k+1 may fill one while slow threads still read plane k
+    extern __shared__ __align__(16) unsigned char flux_smem[];
+    auto fx = reinterpret_cast<P(*)[TY][FT_X + 1][NV]>(flux_smem);
+    auto fy = reinterpret_cast<P(*)[TY + 1][FT_X][NV]>(flux_smem + sizeof(P) * 2 * FluxTile<P>::FX);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
     const int kb = L.bc + blockIdx.z * kz;
@@ -233,44 +265,43 @@ __global__ void __launch_bounds__(FT_X * FluxTile<P>::TY) k_flux_tile(
     const int i = i0 + tx, j = j0 + ty;
     const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
     const bool act = i <= ilast && j <= jlast;
-    const long long fs = L.fs, sy = L.px, sz = (long long)L.px * L.NJ;
+    const int fs = (int)L.fs, sy = L.px, sz = L.px * L.NJ;
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
     P qb[NV], qa[NV];
     const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
     const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
-    if (act) face_flux_up<P, 3, DIFF>(q, fs, L.at(i, j, kb) - 2 * sz, sz, zs_cell, qb);
-    for (int k = kb; k < ke; k++) {
+    if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
+    for (int k = kb, it = 0; k < ke; k++, it ^= 1) {
         // x faces of row j: face f sits between a = i0+f-1 and a+1 and is
         // needed when a <= ilast; it reads cells a-1 .. a+2
         if (j <= jlast) {
             for (int f = tx; f <= FT_X; f += FT_X) {
                 const int a = i0 + f - 1;
                 if (a <= ilast)
-                    face_flux_up<P, 1, DIFF>(q, fs, L.at(a - 1, j, k), 1, species_quirk && a >= L.ni, fx[ty][f]);
+                    face_flux_up<P, 1, DIFF>(q + L.at(a - 1, j, k), fs, 1, species_quirk && a >= L.ni, fx[it][ty][f]);
             }
         }
         // y faces of column i: face g sits between b = j0+g-1 and b+1
         if (i <= ilast) {
             for (int g = ty; g <= TY; g += TY) {
                 const int b = j0 + g - 1;
-                if (b <= jlast) face_flux_up<P, 2, DIFF>(q, fs, L.at(i, b - 1, k), sy, zs_cell, fy[g][tx]);
+                if (b <= jlast) face_flux_up<P, 2, DIFF>(q + L.at(i, b - 1, k), fs, sy, zs_cell, fy[it][g][tx]);
             }
         }
-        if (act) face_flux_up<P, 3, DIFF>(q, fs, L.at(i, j, k) - sz, sz, zs_cell, qa);
+        if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, k) - sz, fs, sz, zs_cell, qa);
         __syncthreads();
         if (act) {
             const double cz = dt / (zn[k] - zn[k - 1]);
             const long long c = L.at(i, j, k);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
-                double r = ax * ((double)fx[ty][tx + 1][v] - (double)fx[ty][tx][v]);
-                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
-                rhs[v * fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
+                double r = ax * ((double)fx[it][ty][tx + 1][v] - (double)fx[it][ty][tx][v]);
+                r = r - by * ((double)fy[it][ty + 1][tx][v] - (double)fy[it][ty][tx][v]);
+                rhs[v * L.fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
                 qb[v] = qa[v];
             }
         }
-        __syncthreads();
     }
 }
 
