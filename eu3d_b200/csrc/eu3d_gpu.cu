@@ -18,6 +18,7 @@
 #include "cell.cuh"
 #include "common.cuh"
 #include "flux.cuh"
+#include "mlp.cuh"
 
 using namespace eu3d;
 
@@ -1037,6 +1038,24 @@ int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const do
     cudaStream_t st = (cudaStream_t)stream;
     k_cfl_fields_partial<<<nblocks, 256, 0, st>>>(f, dx, dy, dz, use_z, scratch);
     k_cfl_fields_final<<<1, 1024, 0, st>>>(scratch, nblocks, cfl, final_time, dt_out, time_inout);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int accumulate, int *err,
+                   void *stream)
+{
+    if (!A || !B || !C) return fail(EU3D_ERR_ARG, "null argument");
+    if (M <= 0 || M % 128 || N < 16 || N > 256 || N % 16 || K <= 0 || K % 16)
+        return fail(EU3D_ERR_ARG, "gemm shape: M % 128 == 0, N in [16, 256] with N % 16 == 0, K % 16 == 0");
+    if (((uintptr_t)A | (uintptr_t)B) & 15) return fail(EU3D_ERR_ARG, "gemm operands must be 16-byte aligned");
+    static bool attr = false;
+    if (!attr) {
+        CK(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem_bytes()));
+        attr = true;
+    }
+    k_gemm_tc<<<M / 128, 128, gemm_smem_bytes(), (cudaStream_t)stream>>>(
+        (const __nv_bfloat16 *)A, (const __nv_bfloat16 *)B, C, M, N, K, accumulate, err);
     CK(cudaGetLastError());
     return EU3D_OK;
 }

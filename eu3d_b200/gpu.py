@@ -34,7 +34,8 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_set_inflow", "eu3d_init_uniform", "eu3d_set_wedge", "eu3d_set_dt", "eu3d_set_time", "eu3d_get_dt", "eu3d_cfl",
            "eu3d_boundary", "eu3d_advection", "eu3d_update_after_adv", "eu3d_update_after_cs", "eu3d_react_imex",
            "eu3d_react_trapezoid", "eu3d_step", "eu3d_run", "eu3d_synchronize", "eu3d_get_status",
-           "eu3d_reset_status", "eu3d_stream", "eu3d_profile_enable", "eu3d_profile_read", "eu3d_cfl_noalloc"]
+           "eu3d_reset_status", "eu3d_stream", "eu3d_profile_enable", "eu3d_profile_read", "eu3d_cfl_noalloc",
+           "eu3d_gemm_bf16"]
 
 
 class Eu3dError(RuntimeError):
@@ -101,6 +102,8 @@ def load_library(path: Optional[str] = None):
     L.eu3d_stream.restype = C.c_void_p
     L.eu3d_cfl_noalloc.argtypes = [C.c_void_p] * 6 + [C.c_int] * 4 + [C.c_longlong] * 2 + [C.c_double] * 3 + \
         [C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    L.eu3d_gemm_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_void_p, C.c_void_p]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]

@@ -183,6 +183,15 @@ int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const do
                      double dx, double dy, double dz, int use_z, double cfl, double final_time,
                      double *time_inout, double *dt_out, int nblocks, void *stream);
 
+/* Learned chemistry surrogate (new; the reference's "DNN" mode has no model,
+   src/Euler.cpp:773-780).  Tensor-core GEMM used by the surrogate's training:
+   C (M x N, f32, row-major) = [C +] A B^T with A (M x K) and B (N x K) bf16
+   row-major, all device pointers; M % 128 == 0, N % 16 == 0 with 16 <= N <= 256,
+   K % 16 == 0.  *err (device int, may be NULL) is set when a tensor-core wait
+   ran out of its bound.  Queued on `stream`, no synchronisation. */
+int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int accumulate, int *err,
+                   void *stream);
+
 /* Pointer to the handle's CUDA stream (cudaStream_t), for callers that
    interleave their own work. */
 void *eu3d_stream(eu3d_handle *h);
