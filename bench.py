@@ -69,7 +69,7 @@ def _ref_slab_worker(args):
     if use_ref:
         rc = pyoracle.RefCase(mech, g, fixed=False)
     else:
-        rc = pyoracle.Oracle(mech, g, 0x0FF)
+        rc = pyoracle.Oracle(mech, g, 0x1FF)
     NI, NJ, NK = g.ni + 4, g.nj + 4, g.nk + 4
     shp = (NI, NJ, NK)
     Y = np.broadcast_to(case.Y, shp + (mech.NS,))

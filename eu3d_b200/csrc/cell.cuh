@@ -396,7 +396,8 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         // GetPartial_T, src/Flowfield.cpp:1578-1595; Gibbs energies for the rates
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-            PT[s] = (ke - cM.ri[s] * hr[s] + cM.ri[s] * 1e3 * T) / (CV * D);
+            const double hs = (qk & EU3D_Q_PARTIAL_T_UNITS) ? cM.ri[s] * hr[s] : (cM.ri[s] * hr[s]) * 1e3;
+            PT[s] = (ke - hs + cM.ri[s] * 1e3 * T) / (CV * D);
             G[s] = R_GAS * hr[s] - (R_GAS * sr[s]) * T;
             Di[s] = cs[s] * 1e-3;
             Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;

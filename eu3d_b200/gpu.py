@@ -19,7 +19,7 @@ from . import build as _build
 _dp = C.POINTER(C.c_double)
 
 # constants mirrored from include/eu3d_quirks.h and include/eu3d_gpu.h
-QUIRKS_REF = 0x0FF
+QUIRKS_REF = 0x1FF
 QUIRKS_FIXED = 0x000
 BC_RSBI, BC_ODM, BC_TRANSMISSIVE, BC_NONE = 0, 1, 2, 3
 REACT_TRAPEZOID, REACT_IMEX, REACT_NONE, REACT_SURROGATE = 0, 1, 2, 3

@@ -34,7 +34,11 @@
    the internal energy of the PREVIOUS decode (src/Flowfield.cpp:1264-1268). */
 #define EU3D_Q_STALE_E 0x080u
 
-#define EU3D_QUIRKS_REF 0x0ffu
+/* GetPartial_T adds the species enthalpy in kJ/kg to terms in J/kg
+   (src/Flowfield.cpp:1590); corrected, the enthalpy is scaled to J/kg. */
+#define EU3D_Q_PARTIAL_T_UNITS 0x100u
+
+#define EU3D_QUIRKS_REF 0x1ffu
 #define EU3D_QUIRKS_FIXED 0x000u
 
 /* Ghost-fill kinds */

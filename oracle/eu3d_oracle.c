@@ -360,6 +360,7 @@ void orc_get_partial_t(orc_field *f, const orc_mech *m)
                 double CV = f->Cp[c] - f->Rgas[c];
                 for (int s = 0; s < NS; s++) {
                     double Hi = orc_gethi(m, f->T[c], m->ri[s], s, f->quirks);
+                    if (!(f->quirks & EU3D_Q_PARTIAL_T_UNITS)) Hi = Hi * 1e3;
                     f->Partion_T[c * (NS + 4) + s] =
                         (0.5 * (pow(f->U[c], 2) + pow(f->V[c], 2) + pow(f->W[c], 2)) - Hi + m->ri[s] * 1e3 * f->T[c]) /
                         (CV * f->D[c]);

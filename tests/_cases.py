@@ -15,7 +15,7 @@ import numpy as np
 from eu3d_b200.readers import make_grid
 from pyoracle import Oracle
 
-QUIRKS_REF = 0x0FF
+QUIRKS_REF = 0x1FF
 QUIRKS_FIXED = 0x000
 
 
