@@ -308,6 +308,54 @@ __device__ __forceinline__ void warp_sum(unsigned long long *ctr, unsigned long 
     if ((threadIdx.x & 31) == (__ffs(act) - 1) && v) atomicAdd(ctr, v);
 }
 
+// Reaction::Diagonalized for the state of the previous decode (the stored CS
+// and T), with GetPartial_T (src/Flowfield.cpp:1578-1595) for its Jacobian:
+// source CMS (kg/m^3/s) and diagonal MD of the partial densities.
+template <bool SPEC>
+__device__ __forceinline__ void imex_source(const double cs[NV], double T, unsigned qk, double CMS[NS], double MD[NS])
+{
+    // state of the previous decode, recomputed from the stored CS and T
+    double D = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) D += cs[s];
+    const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
+    const TPow p = tpow(T, qk);
+    double hr[NS], sr[NS], cpr[NS];
+    if (SPEC) {
+        h2ja919::thermo_spec(p, hr, sr, cpr);
+    } else {
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            hr[s] = h_r(s, p);
+            sr[s] = s_r(s, p);
+            cpr[s] = cp_r(s, p);
+        }
+    }
+    double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], G[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double Y = cs[s] / D;
+        sdiv += Y / cM.mw[s];
+        scp += (cM.ri[s] * cpr[s]) * Y;
+    }
+    const double Rgas = R_GAS * 1000 / (1.0 / sdiv);
+    const double CV = scp * 1000 - Rgas;
+    const double ke = 0.5 * (U * U + V * V + W * W);
+    // GetPartial_T, src/Flowfield.cpp:1578-1595; Gibbs energies for the rates
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double hs = (qk & EU3D_Q_PARTIAL_T_UNITS) ? cM.ri[s] * hr[s] : (cM.ri[s] * hr[s]) * 1e3;
+        PT[s] = (ke - hs + cM.ri[s] * 1e3 * T) / (CV * D);
+        G[s] = R_GAS * hr[s] - (R_GAS * sr[s]) * T;
+        Di[s] = cs[s] * 1e-3;
+        Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;
+    }
+    if (SPEC)
+        h2ja919::diagonalized_spec(p, G, Mc, Di, PT, CMS, MD);
+    else
+        diagonalized(p, G, Mc, Di, PT, CMS, MD);
+}
+
 enum CellMode {
     M_DECODE = 0,
     M_ADV = 1,
@@ -316,8 +364,20 @@ enum CellMode {
     M_TRAP1 = 4,
     M_RK_STAGE1 = 5,
     M_RK_STAGE2 = 6,
-    M_NOCHEM = 7
+    M_NOCHEM = 7,
+    M_TRAP1_PREDICT = 8
 };
+
+// Work queue of the adaptive trapezoid: cells binned by floor(log2 Nchem),
+// listed heaviest bin first so that the warps that pull them together get
+// similar substep counts, and pulled 32 at a time by persistent warps.
+constexpr int QBINS = 32;
+struct ChemQueue {
+    int *list;   // interior cells in bin order
+    int *bins;   // [0, 32) counts, [32, 64) start offsets, [64, 96) fill cursors, [96] work cursor, [97] total
+};
+
+__device__ __forceinline__ int nchem_bin(int n) { return 31 - __clz(max(n, 1)); }
 
 struct CellArgs {
     Layout L;
@@ -329,6 +389,7 @@ struct CellArgs {
     const double *xn, *yn;
     double wedge[3];
     int wedge_on;
+    int *qbins;  // work-queue bin counts (M_TRAP1_PREDICT)
 };
 
 __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
@@ -366,46 +427,8 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
     int capped = 0, capped_any = 0;
 
     if (MODE == M_IMEX) {
-        // state of the previous decode, recomputed from the stored CS and T
-        double D = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; s++) D += cs[s];
-        const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
-        const TPow p = tpow(T, qk);
-        double hr[NS], sr[NS], cpr[NS];
-        if (SPEC) {
-            h2ja919::thermo_spec(p, hr, sr, cpr);
-        } else {
-#pragma unroll
-            for (int s = 0; s < NS; s++) {
-                hr[s] = h_r(s, p);
-                sr[s] = s_r(s, p);
-                cpr[s] = cp_r(s, p);
-            }
-        }
-        double sdiv = 0.0, scp = 0.0, Mc[NS], Di[NS], PT[NS], G[NS], CMS[NS], MD[NS];
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            const double Y = cs[s] / D;
-            sdiv += Y / cM.mw[s];
-            scp += (cM.ri[s] * cpr[s]) * Y;
-        }
-        const double Rgas = R_GAS * 1000 / (1.0 / sdiv);
-        const double CV = scp * 1000 - Rgas;
-        const double ke = 0.5 * (U * U + V * V + W * W);
-        // GetPartial_T, src/Flowfield.cpp:1578-1595; Gibbs energies for the rates
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            const double hs = (qk & EU3D_Q_PARTIAL_T_UNITS) ? cM.ri[s] * hr[s] : (cM.ri[s] * hr[s]) * 1e3;
-            PT[s] = (ke - hs + cM.ri[s] * 1e3 * T) / (CV * D);
-            G[s] = R_GAS * hr[s] - (R_GAS * sr[s]) * T;
-            Di[s] = cs[s] * 1e-3;
-            Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;
-        }
-        if (SPEC)
-            h2ja919::diagonalized_spec(p, G, Mc, Di, PT, CMS, MD);
-        else
-            diagonalized(p, G, Mc, Di, PT, CMS, MD);
+        double CMS[NS], MD[NS];
+        imex_source<SPEC>(cs, T, qk, CMS, MD);
         // Flowfield::Update_IMEX, src/Flowfield.cpp:1219-1228
 #pragma unroll
         for (int v = 0; v < NV; v++) {
@@ -471,7 +494,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
             const double E1 = o.E;
             decode(cs, o.T, E1, qk, o, capped);
             capped_any |= capped;
-        } else if (MODE == M_TRAP1) {
+        } else if (MODE == M_TRAP1 || MODE == M_TRAP1_PREDICT) {
             const int rtb = (qk & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
             int n = predict_nchem<SPEC>(tpow(o.T, qk), cs, o.Y, dt, rtb);
             const bool over = n > NCHEM_CAP;
@@ -479,6 +502,18 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
             if (over) atomicAdd(&a.st->substep_capped, 1);
             atomicMax(&a.st->nchem_max, n);
             if (a.nchem) a.nchem[c] = n;
+            if (MODE == M_TRAP1_PREDICT) {
+                // the substeps run later on the work queue (k_trap1_work)
+                store_cs(a.cs, fs, c, cs);
+                a.T[c] = o.T;
+                a.E[c] = o.E;
+                const unsigned act = __activemask();
+                const int b = nchem_bin(n);
+                const unsigned peers = __match_any_sync(act, b);
+                if ((threadIdx.x & 31) == (__ffs(peers) - 1)) atomicAdd(a.qbins + b, __popc(peers));
+                warp_count(&a.st->newton_capped, capped_any != 0);
+                return;
+            }
             const double dts = dt / n;
             for (int step = 0; step < n; step++) {
                 double dn[NS], Wi[NS];
@@ -506,6 +541,122 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
     store_prims<P>(o, q, fs, c);
     warp_count(&a.st->newton_capped, capped_any != 0);
     warp_count(&a.st->nonfinite, !(isfinite(o.D) && isfinite(o.T)));
+}
+
+// Bin offsets of the adaptive-trapezoid queue, heaviest bin first (one warp).
+__global__ void k_queue_scan(ChemQueue qu)
+{
+    const int b = 31 - (int)threadIdx.x;  // lane 0 takes the heaviest bin
+    const int cnt = qu.bins[b];
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)threadIdx.x >= o) incl += v;
+    }
+    qu.bins[QBINS + b] = incl - cnt;
+    qu.bins[2 * QBINS + b] = 0;
+    if (threadIdx.x == 31) {
+        qu.bins[3 * QBINS] = 0;
+        qu.bins[3 * QBINS + 1] = incl;
+    }
+}
+
+// Lists each interior cell in its bin.
+__global__ void k_queue_scatter(CellArgs a, ChemQueue qu)
+{
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    if (solid_cell(a, i, j)) return;
+    const long long c = L.at(i, j, k);
+    const int b = nchem_bin(a.nchem[c]);
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, b);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(qu.bins + 2 * QBINS + b, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    qu.list[qu.bins[QBINS + b] + base + __popc(peers & ((1u << lane) - 1u))] = (int)c;
+}
+
+// One listed cell of the adaptive-trapezoid queue.
+template <class P, bool SPEC>
+__device__ __forceinline__ void trap1_cell(const CellArgs &a, P *__restrict__ q, long long c, double dt, int rtb)
+{
+    const long long fs = a.L.fs;
+    const unsigned qk = a.quirks;
+    {
+        double cs[NV];
+        load_cs(a.cs, fs, c, cs);
+        // the decoded state of M_TRAP1_PREDICT, re-derived from CS and T
+        Decoded o;
+        double D = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) D += cs[s];
+#pragma unroll
+        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
+        o.U = cs[NS] / D;
+        o.V = cs[NS + 1] / D;
+        o.W = cs[NS + 2] / D;
+        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) / D;
+        o.T = a.T[c];
+        o.D = D;
+        const int n = a.nchem[c];
+        const double dts = dt / n;
+        int capped = 0, capped_any = 0;
+        for (int step = 0; step < n; step++) {
+            double dn[NS], Wi[NS];
+            trapezoid<SPEC>(tpow(o.T, qk), cs, dts, rtb, dn, Wi);
+            double Dn = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                cs[s] = dn[s];
+                Dn += cs[s];
+            }
+            cs[NS] = o.U * Dn;
+            cs[NS + 1] = o.V * Dn;
+            cs[NS + 2] = o.W * Dn;
+            cs[NS + 3] = Dn * o.E + 0.5 * (o.U * o.U + o.V * o.V + o.W * o.W) * Dn;
+            decode(cs, o.T, o.E, qk, o, capped);
+            capped_any |= capped;
+        }
+        if (n == 0) {
+            int cp = 0;
+            decode(cs, o.T, o.E, qk, o, cp);
+        }
+        store_cs(a.cs, fs, c, cs);
+        a.T[c] = o.T;
+        a.E[c] = o.E;
+        store_prims<P>(o, q, fs, c);
+        atomicAdd(&a.st->substeps, (unsigned long long)n);
+        if (capped_any) atomicAdd(&a.st->newton_capped, 1ull);
+        if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
+    }
+}
+
+// Persistent workers of the adaptive trapezoid: each warp pulls 32 listed
+// cells and runs their TrapezoidPrediction substeps (src/Reaction.cpp:489-591)
+// with the re-encode and decode of Flowfield::Explicit(step, i, j, k)
+// (src/Flowfield.cpp:1189-1203) after each, from the decoded state that
+// M_TRAP1_PREDICT stored.
+template <class P, bool SPEC>
+__global__ void __launch_bounds__(128, 3) k_trap1_work(CellArgs a, P *__restrict__ q, ChemQueue qu)
+{
+    const int lane = threadIdx.x & 31;
+    const int total = qu.bins[3 * QBINS + 1];
+    const unsigned qk = a.quirks;
+    const double dt = a.scal[0];
+    const int rtb = (qk & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(qu.bins + 3 * QBINS, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int slot = base + lane;
+        if (slot < total) trap1_cell<P, SPEC>(a, q, qu.list[slot], dt, rtb);
+    }
 }
 
 }  // namespace eu3d

@@ -56,6 +56,8 @@ struct Status {
     int substep_capped;
     unsigned long long sur_cells;
     unsigned long long sur_fallback;
+    unsigned long long audit_cells;        // surrogate cells also run through the integrator
+    unsigned long long audit_max_dT_bits;  // largest |T_surrogate - T_integrator| (double bits)
 };
 
 // Powers of T shared by every species' polynomial at one temperature.

@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "flux.cuh"
 #include "mlp.cuh"
+#include "surrogate.cuh"
 
 using namespace eu3d;
 
@@ -74,6 +75,9 @@ struct eu3d_handle {
     int wedge_on = 0;
     bool spec = false;  // mechanism equals the compiled-in H2_JA919 tables
     int flux_kz = 16;   // z planes walked by one flux block
+    int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
+    int queue_blocks = 3;  // resident queue blocks per SM
+    int *qlist = nullptr, *qbins = nullptr;
     std::map<StepKey, cudaGraphExec_t> graphs;
     // per-kernel CUDA-event timing (eu3d_profile_enable)
     bool profile = false;
@@ -84,6 +88,13 @@ struct eu3d_handle {
     std::vector<ProfRec> prof_pending;
     std::vector<cudaEvent_t> prof_pool;
     std::map<std::string, std::pair<double, long long>> prof_acc;
+    // learned chemistry (eu3d_set_surrogate): network outputs, fallback list
+    eu3d_surrogate *sur = nullptr;
+    float *sur_out = nullptr;
+    int *sur_list = nullptr, *sur_count = nullptr;
+    double *sur_audit = nullptr;
+    long long sur_cap = 0;
+    int sur_audit_stride = 0;
 };
 
 namespace {
@@ -144,6 +155,7 @@ CellArgs cell_args(eu3d_handle *h)
     a.wedge[1] = h->wedge[1];
     a.wedge[2] = h->wedge[2];
     a.wedge_on = h->wedge_on;
+    a.qbins = h->qbins;
     return a;
 }
 
@@ -170,13 +182,60 @@ void launch_cell_t(eu3d_handle *h, int mode)
     }
 }
 
+int queue_grid(const eu3d_handle *h)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+    return sms * h->queue_blocks;
+}
+
+// Adaptive trapezoid on the work queue: predict + bin, offsets, list, workers.
+template <class P, bool SPEC>
+void launch_trap1_queue(eu3d_handle *h)
+{
+    CellArgs a = cell_args(h);
+    P *q = (P *)h->prim;
+    dim3 g = cell_grid(h->L, 128);
+    ChemQueue qu{h->qlist, h->qbins};
+    cudaMemsetAsync(h->qbins, 0, QBINS * sizeof(int), h->st);
+    {
+        ProfScope ps(h, "trap1_predict");
+        k_cell<P, M_TRAP1_PREDICT, SPEC><<<g, 128, 0, h->st>>>(a, q);
+    }
+    {
+        ProfScope ps(h, "trap1_list");
+        k_queue_scan<<<1, 32, 0, h->st>>>(qu);
+        k_queue_scatter<<<g, 128, 0, h->st>>>(a, qu);
+    }
+    {
+        ProfScope ps(h, "trap1_work");
+        k_trap1_work<P, SPEC><<<queue_grid(h), 128, 0, h->st>>>(a, q, qu);
+    }
+}
+
 template <class P>
 void launch_cell(eu3d_handle *h, int mode)
 {
+    if (mode == M_TRAP1 && h->chem_queue && h->qlist) {
+        if (h->spec)
+            launch_trap1_queue<P, true>(h);
+        else
+            launch_trap1_queue<P, false>(h);
+        return;
+    }
     if (h->spec)
         launch_cell_t<P, true>(h, mode);
     else
         launch_cell_t<P, false>(h, mode);
+}
+
+int ensure_queue(eu3d_handle *h)
+{
+    if (h->qlist) return EU3D_OK;
+    CK(cudaMalloc(&h->qlist, (size_t)h->L.interior_cells() * sizeof(int)));
+    CK(cudaMalloc(&h->qbins, (3 * QBINS + 2) * sizeof(int)));
+    CK(cudaMemset(h->qbins, 0, (3 * QBINS + 2) * sizeof(int)));
+    return EU3D_OK;
 }
 
 int cell_op(eu3d_handle *h, int mode)
@@ -197,7 +256,7 @@ void launch_adv(eu3d_handle *h, int diff)
     const int kz = h->flux_kz;
     constexpr int TY = FluxTile<P>::TY;
     dim3 g((L.ni + FT_X - 1) / FT_X, (L.nj + TY - 1) / TY, (L.nk + kz - 1) / kz);
-    dim3 b(FT_X, TY);
+    dim3 b(FT_X, TY + 2);
     constexpr size_t smem = FluxTile<P>::SMEM;
     ProfScope ps(h, "advection");
     if (diff == EU3D_DIFF_MUSCL1)
@@ -484,8 +543,10 @@ void free_handle(eu3d_handle *h)
     for (auto e : h->prof_pool) cudaEventDestroy(e);
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
-    void *ptrs[] = {h->cs, h->rhs, h->cs0, h->T, h->E, h->prim, h->nchem, h->xn, h->yn, h->zn, h->scal, h->partial,
-                    h->status, h->inflow, h->stage};
+    void *ptrs[] = {h->cs,      h->rhs,    h->cs0,    h->T,       h->E,         h->prim,
+                    h->nchem,   h->xn,     h->yn,     h->zn,      h->scal,      h->partial,
+                    h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
+                    h->sur_audit, h->qlist,   h->qbins};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
@@ -502,6 +563,8 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
     h->stage_bytes = bytes;
     return EU3D_OK;
 }
+
+int sur_chem_op(eu3d_handle *h);  // learned chemistry step, sur_host.cuh
 
 int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
 {
@@ -524,6 +587,7 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
     case EU3D_REACT_NONE:
         // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
         return cell_op(h, M_NOCHEM);
+    case EU3D_REACT_SURROGATE: return sur_chem_op(h);
     default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
     }
 }
@@ -919,6 +983,8 @@ int eu3d_react_trapezoid(eu3d_handle *h, int type)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
     if (type != 0 && type != 1) return fail(EU3D_ERR_ARG, "trapezoid type must be 0 or 1");
+    int rc;
+    if (type == 1 && h->chem_queue && (rc = ensure_queue(h))) return rc;
     return cell_op(h, type == 0 ? M_TRAP0 : M_TRAP1);
 }
 
@@ -927,10 +993,18 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "unknown time scheme");
     if (s->diff != EU3D_DIFF_MUSCL1 && s->diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
-    if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE)
+    if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE &&
+        s->react != EU3D_REACT_SURROGATE)
         return fail(EU3D_ERR_ARG, "unsupported reaction scheme");
+    if (s->react == EU3D_REACT_SURROGATE && !h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached");
+    if (s->react == EU3D_REACT_SURROGATE && s->timeadv == EU3D_ADV_SSPRK2)
+        return fail(EU3D_ERR_ARG, "the surrogate step follows the EE update");
     if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
     if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
+    if (s->react == EU3D_REACT_TRAPEZOID && s->type == 1 && h->chem_queue) {
+        int rc = ensure_queue(h);
+        if (rc) return rc;
+    }
     if (h->profile) return enqueue_step(h, s, g_spacing(h));
     StepKey key{s->react, s->type, s->timeadv, s->diff, s->bc_kind, s->cfl, s->final_time};
     auto it = h->graphs.find(key);
@@ -1060,6 +1134,105 @@ int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, 
     return EU3D_OK;
 }
 
+int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
+{
+    if (!h || !t) return fail(EU3D_ERR_ARG, "null argument");
+    if (t->flux_kz < 1 || t->flux_kz > 256) return fail(EU3D_ERR_ARG, "flux_kz must be in [1, 256]");
+    if (t->queue_blocks < 1 || t->queue_blocks > 16) return fail(EU3D_ERR_ARG, "queue_blocks must be in [1, 16]");
+    h->flux_kz = t->flux_kz;
+    h->chem_queue = t->chem_queue ? 1 : 0;
+    h->queue_blocks = t->queue_blocks;
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    return EU3D_OK;
+}
+
+int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
+{
+    if (!h || !t) return fail(EU3D_ERR_ARG, "null argument");
+    t->flux_kz = h->flux_kz;
+    t->chem_queue = h->chem_queue;
+    t->queue_blocks = h->queue_blocks;
+    return EU3D_OK;
+}
+
+int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tuning *best, double *best_ms)
+{
+    if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
+    if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
+    CK(cudaSetDevice(h->dev));
+    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks};
+    // the trials advance the state: keep a copy and put it back after each
+    const size_t fs = (size_t)h->L.fs;
+    const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
+    const size_t bytes = (NV + 2) * fs * sizeof(double) + nprim + 2 * sizeof(double) + sizeof(Status);
+    char *bk = nullptr;
+    CK(cudaMalloc(&bk, bytes));
+    struct Piece {
+        void *p;
+        size_t n;
+    } pieces[] = {{h->cs, NV * fs * sizeof(double)}, {h->T, fs * sizeof(double)}, {h->E, fs * sizeof(double)},
+                  {h->prim, nprim},
+                  {h->scal, 2 * sizeof(double)},
+                  {h->status, sizeof(Status)}};
+    auto copy = [&](bool save) {
+        size_t off = 0;
+        for (auto &pc : pieces) {
+            if (save) cudaMemcpyAsync(bk + off, pc.p, pc.n, cudaMemcpyDeviceToDevice, h->st);
+            else cudaMemcpyAsync(pc.p, bk + off, pc.n, cudaMemcpyDeviceToDevice, h->st);
+            off += pc.n;
+        }
+    };
+    copy(true);
+    std::vector<eu3d_tuning> cands;
+    const bool q = s->react == EU3D_REACT_TRAPEZOID && s->type == 1;
+    for (int kz : {4, 8, 16, 32})
+        for (int cq : {0, 1})
+            for (int qb : {2, 3, 4}) {
+                if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
+                if (q && cq == 0 && qb != start.queue_blocks) continue;
+                cands.push_back({kz, cq, qb});
+            }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best_t = 1e300;
+    eu3d_tuning bt = start;
+    int rc = EU3D_OK;
+    for (const auto &c : cands) {
+        if ((rc = eu3d_set_tuning(h, &c))) break;
+        if ((rc = eu3d_step(h, s))) break;  // records the graph, warms up
+        cudaEventRecord(e0, h->st);
+        for (int n = 0; n < steps && !rc; n++) rc = eu3d_step(h, s);
+        cudaEventRecord(e1, h->st);
+        if (rc) break;
+        if (cudaStreamSynchronize(h->st) != cudaSuccess) {
+            rc = fail(EU3D_ERR_CUDA, "autotune trial failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms / steps < best_t) {
+            best_t = ms / steps;
+            bt = c;
+        }
+        copy(false);
+    }
+    copy(false);
+    cudaStreamSynchronize(h->st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(bk);
+    if (rc) {
+        eu3d_set_tuning(h, &start);
+        return rc;
+    }
+    eu3d_set_tuning(h, &bt);
+    if (best) *best = bt;
+    if (best_ms) *best_ms = best_t;
+    return EU3D_OK;
+}
+
 int eu3d_synchronize(eu3d_handle *h)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
@@ -1082,6 +1255,10 @@ int eu3d_get_status(eu3d_handle *h, eu3d_status *o)
     o->substep_capped = s.substep_capped;
     o->surrogate_cells = (long long)s.sur_cells;
     o->surrogate_fallback = (long long)s.sur_fallback;
+    o->surrogate_audited = (long long)s.audit_cells;
+    double mx;
+    memcpy(&mx, &s.audit_max_dT_bits, sizeof(double));
+    o->surrogate_audit_max_dT = mx;
     o->dt = sc[0];
     o->time = sc[1];
     return EU3D_OK;
@@ -1096,3 +1273,5 @@ int eu3d_reset_status(eu3d_handle *h)
 }
 
 }  // extern "C"
+
+#include "sur_host.cuh"

@@ -248,8 +248,18 @@ struct FluxTile {
 // registers (the face below a cell is the face above the previous plane's
 // cell), and each thread then forms its cell's residual in the reference's
 // order ((-dt/dx dF - dt/dy dG) - dt/dz dQ) in FP64.
+// A tile of 32 x TY cells has 33 x TY x faces and 32 x (TY + 1) y faces: the
+// block carries two extra warps, one for the last y-face row (ty == TY) and
+// one for the last x face of each row (ty == TY + 1), so that every warp
+// evaluates at most one face of each direction per plane.
+template <class P>
+constexpr int flux_threads()
+{
+    return FT_X * (FluxTile<P>::TY + 2);
+}
+
 template <class P, int DIFF>
-__global__ void __launch_bounds__(FT_X * FluxTile<P>::TY, 3) k_flux_tile(
+__global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
     Layout L, const P *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
     const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
 {
@@ -264,7 +274,8 @@ __global__ void __launch_bounds__(FT_X * FluxTile<P>::TY, 3) k_flux_tile(
     const int ke = min(kb + kz, L.nk + L.bc);
     const int i = i0 + tx, j = j0 + ty;
     const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
-    const bool act = i <= ilast && j <= jlast;
+    const bool cellw = ty < TY;  // warps that own cells (the other two only add faces)
+    const bool act = cellw && i <= ilast && j <= jlast;
     const int fs = (int)L.fs, sy = L.px, sz = L.px * L.NJ;
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
@@ -273,21 +284,22 @@ __global__ void __launch_bounds__(FT_X * FluxTile<P>::TY, 3) k_flux_tile(
     const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
     if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
     for (int k = kb, it = 0; k < ke; k++, it ^= 1) {
-        // x faces of row j: face f sits between a = i0+f-1 and a+1 and is
-        // needed when a <= ilast; it reads cells a-1 .. a+2
-        if (j <= jlast) {
-            for (int f = tx; f <= FT_X; f += FT_X) {
-                const int a = i0 + f - 1;
-                if (a <= ilast)
-                    face_flux_up<P, 1, DIFF>(q + L.at(a - 1, j, k), fs, 1, species_quirk && a >= L.ni, fx[it][ty][f]);
-            }
+        // x faces of row r: face f sits between a = i0+f-1 and a+1 and is
+        // needed when a <= ilast; it reads cells a-1 .. a+2.  Faces 0..31 by
+        // the cell warps, face 32 of row tx by lane tx of warp TY + 1.
+        {
+            const int r = cellw ? ty : tx;
+            const int f = cellw ? tx : FT_X;
+            const int jr = j0 + r;
+            const int a = i0 + f - 1;
+            if ((cellw || (ty == TY + 1 && tx < TY)) && jr <= jlast && a <= ilast)
+                face_flux_up<P, 1, DIFF>(q + L.at(a - 1, jr, k), fs, 1, species_quirk && a >= L.ni, fx[it][r][f]);
         }
-        // y faces of column i: face g sits between b = j0+g-1 and b+1
-        if (i <= ilast) {
-            for (int g = ty; g <= TY; g += TY) {
-                const int b = j0 + g - 1;
-                if (b <= jlast) face_flux_up<P, 2, DIFF>(q + L.at(i, b - 1, k), fs, sy, zs_cell, fy[it][g][tx]);
-            }
+        // y faces of column i: face g sits between b = j0+g-1 and b+1;
+        // faces 0..TY-1 by the cell warps, face TY by warp TY
+        if (ty <= TY && i <= ilast) {
+            const int b = j0 + ty - 1;
+            if (b <= jlast) face_flux_up<P, 2, DIFF>(q + L.at(i, b - 1, k), fs, sy, species_quirk && i >= L.ni, fy[it][ty][tx]);
         }
         if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, k) - sz, fs, sz, zs_cell, qa);
         __syncthreads();

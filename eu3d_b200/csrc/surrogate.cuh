@@ -1,0 +1,808 @@
+// Learned chemistry surrogate: training-set generation, FP64 labels from the
+// project's own integrators, the fused tensor-core MLP inference kernel and
+// the per-cell apply step (conservation projection, envelope and residual
+// checks, fallback list), plus the persistent fallback queue that runs the
+// FP64 IMEX integrator on the cells the surrogate rejects.
+//
+// Sample record (states, FP64, 12 per sample): T [K], p [Pa], Y_0..Y_8, dt [s].
+// Raw features (FP32, 12): T, ln(p / 1 atm), ln(Y_0 + 1e-12)..ln(Y_8 + 1e-12), ln dt.
+// Raw labels (FP32, 12): dY_0..dY_8 (mass-fraction change over dt of a closed
+// constant-density, constant-energy reactor, projected to element
+// conservation), dT [K], weight (0 = unusable sample), label substeps.
+//
+// Targets: x_k = label_k / (dt A(T)), A(T) = exp(Ta (1/Tr - 1/T)) an
+// Arrhenius activity that vanishes in cold gas; y_k = asinh(x_k / lin_k),
+// standardised with out_mean / out_std.  Inference inverts the chain.
+#pragma once
+
+#include "cell.cuh"
+#include "mlp.cuh"
+
+// offsets into the float normalisation vector (mirrored in include/eu3d_gpu.h)
+#ifndef EU3D_SUR_NORM_LEN
+#define EU3D_SUR_NORM_LEN 80
+#endif
+
+namespace eu3d {
+
+constexpr int SN_IN_MEAN = 0, SN_IN_STD = 12, SN_OUT_MEAN = 24, SN_OUT_STD = 34, SN_LIN = 44, SN_TA = 54, SN_TR = 55,
+              SN_ENV = 56, SN_RATIO = 62, SN_RATIO_TOL = 64, SN_RES_ABS = 65, SN_RES_REL = 66, SN_NEG_TOL = 67,
+              SN_PROJ_EPS = 68, SN_DT_MAX = 69;
+
+struct SurNorm {
+    float v[EU3D_SUR_NORM_LEN];
+};
+
+constexpr int SUR_NELEM = 3;  // H, O, N
+// element matrix: atoms of element e per unit mass of species k (atoms / W_k)
+__constant__ double c_sur_elem[SUR_NELEM][NS];
+
+constexpr double ATM_PA = 101325.0;
+constexpr float SUR_YFLOOR = 1e-12f;  // mass-fraction floor of the log inputs
+
+// ------------------------------------------------------------------ RNG
+__host__ __device__ __forceinline__ unsigned long long smix64(unsigned long long x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// uniform in [0, 1) from (seed, sample, draw)
+__device__ __forceinline__ double urand(unsigned long long seed, unsigned long long idx, int k)
+{
+    return (double)(smix64(seed ^ smix64(idx * 64ull + (unsigned long long)k)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// ------------------------------------------------------ projection, energy
+// Weighted least-change projection of dY onto element conservation:
+// minimise sum_k (dY'_k - dY_k)^2 / w_k subject to sum_k A_ek dY'_k = 0,
+// w_k = Y_k + eps, so that scarce species take small corrections.
+__device__ __forceinline__ void sur_project(const double Y[NS], double dY[NS], double eps)
+{
+    double r[SUR_NELEM], M[SUR_NELEM][SUR_NELEM];
+#pragma unroll
+    for (int e = 0; e < SUR_NELEM; e++) {
+        double a = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; k++) a += c_sur_elem[e][k] * dY[k];
+        r[e] = a;
+#pragma unroll
+        for (int f = 0; f < SUR_NELEM; f++) {
+            double m = 0.0;
+#pragma unroll
+            for (int k = 0; k < NS; k++) m += c_sur_elem[e][k] * (Y[k] + eps) * c_sur_elem[f][k];
+            M[e][f] = m;
+        }
+    }
+    // 3x3 solve by cofactors
+    const double c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+    const double c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+    const double c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+    const double det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+    if (!(fabs(det) > 0.0)) return;
+    const double id = 1.0 / det;
+    const double inv[3][3] = {{c00 * id, (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id,
+                               (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id},
+                              {c01 * id, (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id,
+                               (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id},
+                              {c02 * id, (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id,
+                               (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id}};
+    double lam[SUR_NELEM];
+#pragma unroll
+    for (int e = 0; e < SUR_NELEM; e++) lam[e] = inv[e][0] * r[0] + inv[e][1] * r[1] + inv[e][2] * r[2];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        double a = 0.0;
+#pragma unroll
+        for (int e = 0; e < SUR_NELEM; e++) a += c_sur_elem[e][k] * lam[e];
+        dY[k] -= (Y[k] + eps) * a;
+    }
+}
+
+// internal energy e(T) [J/kg] and cv [J/kg/K] of the mixture Y, with the
+// arithmetic of the decode (mixture polynomial, kJ -> J)
+__device__ __forceinline__ void mix_energy(const double Y[NS], double T, unsigned q, double &e, double &cv)
+{
+    double yr[NS], sYR = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        yr[s] = Y[s] * cM.ri[s];
+        sYR += yr[s];
+    }
+    const TPow p = tpow(T, q);
+    double A[8];
+    mix_coeffs(yr, p.hi, p.rb, A);
+    const double sh = -A[0] * p.tm1 + A[1] * p.lnT + A[2] * p.T + A[3] * p.t2 * 0.5 + A[4] * p.t3 * (1.0 / 3.0) +
+                      A[5] * p.t4 * 0.25 + A[6] * p.t5 * 0.2 + A[7];
+    const double scp = A[0] * p.tm2 + A[1] * p.tm1 + A[2] + A[3] * p.T + A[4] * p.t2 + A[5] * p.t3 + A[6] * p.t4;
+    e = (sh - sYR * T) * 1e3;
+    cv = (scp - sYR) * 1e3;
+}
+
+__device__ __forceinline__ double sur_activity(const SurNorm &n, double T)
+{
+    return exp((double)n.v[SN_TA] * (1.0 / (double)n.v[SN_TR] - 1.0 / T));
+}
+
+// ------------------------------------------------------- sample generation
+struct SurSpecies {
+    int H, O, H2O, OH, O2, H2, H2O2, HO2, N2;
+};
+
+// Random thermochemical states: T uniform, ln p uniform, ln dt uniform and a
+// composition at the fixed element ratios of stoichiometric H2-air, built
+// from the unburnt mixture 2 H2 + O2 + 3.76 N2 by element-preserving steps:
+// progress to H2O, then dissociation into the radical pool.
+__global__ void k_sur_random(double *__restrict__ states, long long base, long long n, unsigned long long seed,
+                             SurSpecies sp, double Tlo, double Thi, double lnplo, double lnphi, double lndtlo,
+                             double lndthi)
+{
+    const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const unsigned long long id = (unsigned long long)(base + m);
+    double nm[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) nm[s] = 0.0;
+    const double lam = urand(seed, id, 0);
+    nm[sp.H2] = 2.0 - 2.0 * lam;
+    nm[sp.O2] = 1.0 - lam;
+    nm[sp.H2O] = 2.0 * lam;
+    nm[sp.N2] = 3.76;
+    double f[5];
+#pragma unroll
+    for (int r = 0; r < 5; r++) {
+        const double u = urand(seed, id, 1 + r), v = urand(seed, id, 6 + r);
+        f[r] = u < 0.15 ? 0.0 : pow(10.0, -7.0 + 6.5 * v);
+    }
+    double e;
+    e = f[0] * nm[sp.H2];  // H2 -> 2 H
+    nm[sp.H2] -= e;
+    nm[sp.H] += 2 * e;
+    e = f[1] * nm[sp.O2];  // O2 -> 2 O
+    nm[sp.O2] -= e;
+    nm[sp.O] += 2 * e;
+    e = f[2] * nm[sp.H2O];  // H2O -> H + OH
+    nm[sp.H2O] -= e;
+    nm[sp.H] += e;
+    nm[sp.OH] += e;
+    e = f[3] * fmin(nm[sp.H], nm[sp.O2]);  // H + O2 -> HO2
+    nm[sp.H] -= e;
+    nm[sp.O2] -= e;
+    nm[sp.HO2] += e;
+    e = f[4] * 0.5 * nm[sp.OH];  // 2 OH -> H2O2
+    nm[sp.OH] -= 2 * e;
+    nm[sp.H2O2] += e;
+    double tot = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        nm[s] = fmax(nm[s], 0.0) * cM.mw[s];
+        tot += nm[s];
+    }
+    double *o = states + (base + m) * 12;
+    o[0] = Tlo + (Thi - Tlo) * urand(seed, id, 11);
+    o[1] = ATM_PA * exp(lnplo + (lnphi - lnplo) * urand(seed, id, 12));
+#pragma unroll
+    for (int s = 0; s < NS; s++) o[2 + s] = nm[s] / tot;
+    o[11] = exp(lndtlo + (lndthi - lndtlo) * urand(seed, id, 13));
+}
+
+// Flowfield snapshot samples: every stride-th interior cell (from offset),
+// its T, p and Y with multiplicative jitter on T and p and ln dt uniform.
+template <class P>
+__global__ void k_sur_snapshot(double *__restrict__ states, long long base, long long n, Layout L,
+                               const double *__restrict__ T, const P *__restrict__ prim, long long stride,
+                               long long offset, unsigned long long seed, double jT, double jP, double lndtlo,
+                               double lndthi)
+{
+    const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const long long idx = offset + m * stride;
+    const int i = (int)(idx % L.ni);
+    const long long r = idx / L.ni;
+    const int j = (int)(r % L.nj), k = (int)(r / L.nj);
+    const long long c = L.at(i + L.bc, j + L.bc, k + L.bc);
+    const unsigned long long id = (unsigned long long)(base + m);
+    double Y[NS], tot = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Y[s] = fmax((double)prim[(PY + s) * L.fs + c], 0.0);
+        tot += Y[s];
+    }
+    double *o = states + (base + m) * 12;
+    o[0] = T[c] * (1.0 + jT * (2.0 * urand(seed, id, 0) - 1.0));
+    o[1] = (double)prim[PP * L.fs + c] * exp(jP * (2.0 * urand(seed, id, 1) - 1.0));
+#pragma unroll
+    for (int s = 0; s < NS; s++) o[2 + s] = Y[s] / tot;
+    o[11] = exp(lndtlo + (lndthi - lndtlo) * urand(seed, id, 2));
+}
+
+// ------------------------------------------------------------------ labels
+enum { SUR_LABEL_IMEX = 1, SUR_LABEL_TRAPEZOID = 0 };
+
+// Closed-reactor chemistry of one sample in FP64 with the project's
+// integrators, then the element projection and the decode at constant
+// density and internal energy.  kind SUR_LABEL_IMEX: one Diagonalized +
+// Update_IMEX step with zero flux residual (the integrator the coupled run
+// falls back to); SUR_LABEL_TRAPEZOID: TrapezoidPrediction substeps of the
+// point-implicit trapezoid (capped at cap substeps).
+template <bool SPEC>
+__global__ void __launch_bounds__(128, 3)
+    k_sur_label(const double *__restrict__ states, long long n, int kind, unsigned q, int cap, double proj_eps,
+                float *__restrict__ X, float *__restrict__ Lb)
+{
+    const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const double *sr = states + m * 12;
+    const double T0 = sr[0], p0 = sr[1], dt = sr[11];
+    double Y0[NS], sdiv = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Y0[s] = sr[2 + s];
+        sdiv += Y0[s] / cM.mw[s];
+    }
+    const double D0 = p0 / (R_GAS * 1000 * sdiv * T0);
+    double E0, cv0;
+    mix_energy(Y0, T0, q, E0, cv0);
+    double cs[NV];
+#pragma unroll
+    for (int s = 0; s < NS; s++) cs[s] = D0 * Y0[s];
+    cs[NS] = cs[NS + 1] = cs[NS + 2] = 0.0;
+    cs[NS + 3] = D0 * E0;
+    Decoded o;
+    int capped = 0, bad = 0, nsub = 1;
+    double Tg = T0;
+    if (kind == SUR_LABEL_IMEX) {
+        double CMS[NS], MD[NS];
+        imex_source<SPEC>(cs, T0, q, CMS, MD);
+#pragma unroll
+        for (int s = 0; s < NS; s++) cs[s] = cs[s] + (CMS[s] * dt) / (1.0 - dt * MD[s]);
+        decode(cs, T0, E0, q, o, capped);
+        Tg = o.T;
+    } else {
+        const int rtb = (q & EU3D_Q_ADAPT_RTB_ZERO) ? 2 : 0;
+        decode(cs, T0, E0, q, o, capped);
+        int nn = predict_nchem<SPEC>(tpow(o.T, q), cs, o.Y, dt, rtb);
+        if (nn > cap) {
+            nn = cap;
+            bad = 1;
+        }
+        nsub = nn;
+        const double dts = dt / nn;
+        for (int st = 0; st < nn; st++) {
+            double dn[NS], Wi[NS];
+            trapezoid<SPEC>(tpow(o.T, q), cs, dts, rtb, dn, Wi);
+            double D = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                cs[s] = dn[s];
+                D += cs[s];
+            }
+            cs[NS + 3] = D * o.E;
+            decode(cs, o.T, o.E, q, o, capped);
+            bad |= capped;
+        }
+        Tg = o.T;
+    }
+    double Dn = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) Dn += cs[s];
+    double dY[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) dY[s] = cs[s] / Dn - Y0[s];
+    sur_project(Y0, dY, proj_eps);
+    // decode of the projected composition at (D0, E0)
+    double cp[NV];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double y = Y0[s] + dY[s];
+        if (y < -1e-7) bad = 1;
+        cp[s] = D0 * fmax(y, 0.0);
+    }
+    cp[NS] = cp[NS + 1] = cp[NS + 2] = 0.0;
+    cp[NS + 3] = D0 * E0;
+    decode(cp, Tg, E0, q, o, capped);
+    bad |= capped;
+    const double dT = o.T - T0;
+    bad |= !isfinite(dT);
+#pragma unroll
+    for (int s = 0; s < NS; s++) bad |= !isfinite(dY[s]);
+    float *x = X + m * 12;
+    x[0] = (float)T0;
+    x[1] = (float)log(p0 / ATM_PA);
+#pragma unroll
+    for (int s = 0; s < NS; s++) x[2 + s] = logf((float)Y0[s] + SUR_YFLOOR);
+    x[11] = (float)log(dt);
+    float *l = Lb + m * 12;
+#pragma unroll
+    for (int s = 0; s < NS; s++) l[s] = bad ? 0.f : (float)dY[s];
+    l[9] = bad ? 0.f : (float)dT;
+    l[10] = bad ? 0.f : 1.f;
+    l[11] = (float)nsub;
+}
+
+// ------------------------------------------------------- training batches
+// Normalised network inputs.  BF16 keeps 8 significant bits, which would
+// resolve T to several kelvin; the spare input columns 12..14 carry the BF16
+// rounding residuals of T, ln p and ln dt scaled by 256, so that the first
+// layer sees those three at about 16 bits.
+__device__ __forceinline__ float bf16_residual(float x) { return (x - __bfloat162float(__float2bfloat16_rn(x))) * 256.f; }
+
+__device__ __forceinline__ void sur_features(const SurNorm &n, const float raw[SUR_NIN], float f[SUR_IN])
+{
+#pragma unroll
+    for (int i = 0; i < SUR_NIN; i++) f[i] = (raw[i] - n.v[SN_IN_MEAN + i]) / n.v[SN_IN_STD + i];
+    f[12] = bf16_residual(f[0]);
+    f[13] = bf16_residual(f[1]);
+    f[14] = bf16_residual(f[11]);
+    f[15] = 0.f;
+}
+
+// Random minibatch (with replacement): normalised features (B x 16) and
+// standardised targets (B x 16, column 15 = sample weight).
+__global__ void k_sur_batch(const float *__restrict__ X, const float *__restrict__ Lb, long long n, SurNorm nrm,
+                            unsigned long long seed, long long step, int B, float *__restrict__ Xb,
+                            float *__restrict__ Yb)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B) return;
+    const long long idx = (long long)(smix64(seed ^ smix64((unsigned long long)step * 0x100000001ull + r)) % n);
+    float raw[SUR_NIN], f[SUR_IN];
+#pragma unroll
+    for (int i = 0; i < SUR_NIN; i++) raw[i] = X[idx * 12 + i];
+    sur_features(nrm, raw, f);
+#pragma unroll
+    for (int i = 0; i < SUR_IN; i++) Xb[(long long)r * SUR_IN + i] = f[i];
+    const double T = raw[0], dt = exp((double)raw[11]);
+    const double sc = dt * sur_activity(nrm, T);
+    const float *l = Lb + idx * 12;
+    float *y = Yb + (long long)r * SUR_OUT;
+#pragma unroll
+    for (int k = 0; k < SUR_NOUT; k++) {
+        const double x = (double)l[k] / sc;
+        const double t = asinh(x / (double)nrm.v[SN_LIN + k]);
+        y[k] = (float)((t - nrm.v[SN_OUT_MEAN + k]) / nrm.v[SN_OUT_STD + k]);
+    }
+    for (int k = SUR_NOUT; k < 15; k++) y[k] = 0.f;
+    y[15] = l[10];
+}
+
+// normalised network output of one output -> raw label (dY_k or dT)
+__device__ __forceinline__ float sur_unscale_f(const SurNorm &n, int k, float t, float sc)
+{
+    const float y = fmaf(t, n.v[SN_OUT_STD + k], n.v[SN_OUT_MEAN + k]);
+    return sc * n.v[SN_LIN + k] * sinhf(y);
+}
+
+// ------------------------------------------------ fused inference kernel
+// 12 -> 128 -> 128 -> 128 -> 10 MLP on the tensor cores.  One CTA holds the
+// four weight matrices in shared memory for its whole life and runs NG tile
+// groups of 128 threads; each group owns 128 TMEM columns and a 32 KB
+// activation tile, and walks 128-cell tiles: features -> bf16 A tile ->
+// tcgen05.mma (FP32 accumulators in TMEM) -> tcgen05.ld, bias, GELU, bf16 ->
+// the next layer's A tile.  While one group runs its epilogue on the CUDA
+// cores, another group's MMAs occupy the tensor pipe.
+constexpr int SUR_NG = 4;
+constexpr int SURK_W1 = 0;                             // 128 x 16
+constexpr int SURK_W2 = SURK_W1 + SUR_H * SUR_IN * 2;  // 128 x 128
+constexpr int SURK_W3 = SURK_W2 + SUR_H * SUR_H * 2;
+constexpr int SURK_W4 = SURK_W3 + SUR_H * SUR_H * 2;   // 16 x 128
+constexpr int SURK_BIAS = SURK_W4 + SUR_OUT * SUR_H * 2;
+constexpr int SURK_A = SURK_BIAS + (3 * SUR_H + SUR_OUT) * 4;
+constexpr int SURK_ATILE = 128 * SUR_H * 2;
+constexpr int SURK_MBAR = SURK_A + SUR_NG * SURK_ATILE;
+constexpr int SURK_SMEM = SURK_MBAR + SUR_NG * 8 + 16;
+
+struct SurWeights {
+    const __nv_bfloat16 *Wt[4];  // out x in, row-major
+    const float *p;              // flat FP32 parameters (biases)
+};
+
+// feature sources / output sinks
+struct SurSrcArray {  // normalised features, n x 16 FP32; outputs n x 16
+    const float *X;
+    float *out;
+    long long n;
+    long long ntiles() const { return (n + 127) / 128; }
+    __device__ __forceinline__ bool load(long long tile, int lane, const SurNorm &, float f[SUR_IN], long long &idx) const
+    {
+        idx = tile * 128 + lane;
+        if (idx >= n) return false;
+        const float4 *p = reinterpret_cast<const float4 *>(X + idx * SUR_IN);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const float4 a = p[v];
+            f[4 * v] = a.x;
+            f[4 * v + 1] = a.y;
+            f[4 * v + 2] = a.z;
+            f[4 * v + 3] = a.w;
+        }
+        return true;
+    }
+    __device__ __forceinline__ void store(long long idx, const float o[SUR_OUT]) const
+    {
+        float4 *p = reinterpret_cast<float4 *>(out + idx * SUR_OUT);
+#pragma unroll
+        for (int v = 0; v < 4; v++) p[v] = make_float4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+    }
+};
+
+// Tiles follow x rows (tpr tiles of 128 cells per row) so that a tile's
+// cells are contiguous in memory and no 64-bit division is needed.
+template <class P>
+struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
+    Layout L;
+    const double *T;
+    const P *prim;
+    const double *scal;
+    float *out;
+    long long n;
+    int tpr;  // tiles per x row
+    long long ntiles() const { return (long long)tpr * L.nj * L.nk; }
+    __device__ __forceinline__ bool load(long long tile, int lane, const SurNorm &nrm, float f[SUR_IN],
+                                         long long &idx) const
+    {
+        const int t = (int)tile;
+        const int r = t / tpr;
+        const int i = (t - r * tpr) * 128 + lane;
+        if (i >= L.ni) return false;
+        const int j = r % L.nj, k = r / L.nj;
+        idx = (long long)r * L.ni + i;
+        const long long c = L.at(i + L.bc, j + L.bc, k + L.bc);
+        float raw[SUR_NIN];
+        raw[0] = (float)T[c];
+        raw[1] = __logf((float)prim[PP * L.fs + c] * (float)(1.0 / ATM_PA));
+#pragma unroll
+        for (int s = 0; s < NS; s++) raw[2 + s] = __logf(fmaxf((float)prim[(PY + s) * L.fs + c], 0.f) + SUR_YFLOOR);
+        raw[11] = __logf((float)scal[0]);
+        sur_features(nrm, raw, f);
+        return true;
+    }
+    __device__ __forceinline__ void store(long long idx, const float o[SUR_OUT]) const
+    {
+#pragma unroll
+        for (int k = 0; k < SUR_NOUT; k++) out[k * n + idx] = o[k];
+    }
+};
+
+// stage a row-major (R x K) bf16 matrix into the canonical K-major operand layout
+__device__ __forceinline__ void sur_stage(unsigned char *dst, const __nv_bfloat16 *src, int R, int K, int tid,
+                                          int nthr)
+{
+    const int vec = K >> 3;
+    for (int v = tid; v < R * vec; v += nthr) {
+        const int r = v / vec, kk = (v % vec) * 8;
+        *reinterpret_cast<uint4 *>(dst + tc::op_off(R, r, kk)) =
+            *reinterpret_cast<const uint4 *>(src + (size_t)r * K + kk);
+    }
+}
+
+__device__ __forceinline__ void named_bar(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b)
+{
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+// hidden-layer epilogue of one row: 128 accumulators + bias -> GELU -> bf16 A tile
+__device__ __forceinline__ void sur_hidden_epilogue(uint32_t tmem_row, const float *bias, unsigned char *A, int row)
+{
+#pragma unroll 1
+    for (int c0 = 0; c0 < SUR_H; c0 += 32) {
+        float v[32];
+        tc::tmem_ld32(tmem_row + c0, v);
+        const float4 *b4 = reinterpret_cast<const float4 *>(bias + c0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float4 ba = b4[2 * q], bb = b4[2 * q + 1];
+            uint4 w;
+            w.x = gelu_bf16x2(v[8 * q + 0] + ba.x, v[8 * q + 1] + ba.y);
+            w.y = gelu_bf16x2(v[8 * q + 2] + ba.z, v[8 * q + 3] + ba.w);
+            w.z = gelu_bf16x2(v[8 * q + 4] + bb.x, v[8 * q + 5] + bb.y);
+            w.w = gelu_bf16x2(v[8 * q + 6] + bb.z, v[8 * q + 7] + bb.w);
+            *reinterpret_cast<uint4 *>(A + tc::op_off(128, row, c0 + 8 * q)) = w;
+        }
+    }
+}
+
+template <class Src>
+__global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const SurNorm *__restrict__ nrm_g, Src src,
+                                                           long long ntiles, int *__restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int g = tid >> 7, t = tid & 127, warp = tid >> 5;
+    float *bias = reinterpret_cast<float *>(sm + SURK_BIAS);
+    __shared__ SurNorm nrm;
+    for (int v = tid; v < EU3D_SUR_NORM_LEN; v += nthr) nrm.v[v] = nrm_g->v[v];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + SURK_MBAR);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(sm + SURK_MBAR + SUR_NG * 8);
+    unsigned char *A = sm + SURK_A + g * SURK_ATILE;
+
+    sur_stage(sm + SURK_W1, W.Wt[0], SUR_H, SUR_IN, tid, nthr);
+    sur_stage(sm + SURK_W2, W.Wt[1], SUR_H, SUR_H, tid, nthr);
+    sur_stage(sm + SURK_W3, W.Wt[2], SUR_H, SUR_H, tid, nthr);
+    sur_stage(sm + SURK_W4, W.Wt[3], SUR_OUT, SUR_H, tid, nthr);
+    for (int v = tid; v < 3 * SUR_H + SUR_OUT; v += nthr) {
+        const int l = v / SUR_H, c = v % SUR_H;
+        const int off = l == 0 ? SUR_OFF_B1 : l == 1 ? SUR_OFF_B2 : l == 2 ? SUR_OFF_B3 : SUR_OFF_B4;
+        bias[v] = W.p[off + c];
+    }
+    if (warp == 0) tc::tmem_alloc(slot, 128 * SUR_NG);
+    if (tid == 0) {
+        for (int q = 0; q < SUR_NG; q++) tc::mbar_init(tc::smem_u32(mbar + q), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *slot + (uint32_t)(g * 128);
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t mb = tc::smem_u32(mbar + g);
+    const uint32_t aS = tc::smem_u32(A);
+    const uint32_t w1 = tc::smem_u32(sm + SURK_W1), w2 = tc::smem_u32(sm + SURK_W2), w3 = tc::smem_u32(sm + SURK_W3),
+                   w4 = tc::smem_u32(sm + SURK_W4);
+    const uint32_t id128 = tc::idesc_bf16(128, SUR_H), id16 = tc::idesc_bf16(128, SUR_OUT);
+    uint32_t phase = 0;
+    bool ok = true;
+
+    for (long long tile = (long long)blockIdx.x * SUR_NG + g; tile < ntiles; tile += (long long)gridDim.x * SUR_NG) {
+        long long idx = 0;
+        float f[SUR_IN];
+        const bool have = src.load(tile, t, nrm, f, idx);
+        if (!have)
+#pragma unroll
+            for (int i = 0; i < SUR_IN; i++) f[i] = 0.f;
+        uint4 w0, w1v;
+        w0.x = pack_bf16(f[0], f[1]);
+        w0.y = pack_bf16(f[2], f[3]);
+        w0.z = pack_bf16(f[4], f[5]);
+        w0.w = pack_bf16(f[6], f[7]);
+        w1v.x = pack_bf16(f[8], f[9]);
+        w1v.y = pack_bf16(f[10], f[11]);
+        w1v.z = pack_bf16(f[12], f[13]);
+        w1v.w = pack_bf16(f[14], f[15]);
+        *reinterpret_cast<uint4 *>(A + tc::op_off(128, t, 0)) = w0;
+        *reinterpret_cast<uint4 *>(A + tc::op_off(128, t, 8)) = w1v;
+#pragma unroll 1
+        for (int layer = 0; layer < 4; layer++) {
+            tc::fence_async_smem();
+            tc::fence_before();
+            named_bar(1 + g, 128);
+            if (t == 0) {
+                tc::fence_after();
+                if (layer == 0) {
+                    tc::mma(tmem, tc::sdesc(aS), tc::sdesc(w1), id128, 0u);
+                } else {
+                    const uint32_t wb = layer == 1 ? w2 : layer == 2 ? w3 : w4;
+                    const int N = layer == 3 ? SUR_OUT : SUR_H;
+                    const uint32_t idd = layer == 3 ? id16 : id128;
+#pragma unroll
+                    for (int s = 0; s < SUR_H / 16; s++)
+                        tc::mma(tmem, tc::sdesc(aS + s * 128 * 32), tc::sdesc(wb + s * N * 32), idd, s > 0 ? 1u : 0u);
+                }
+                tc::commit(mb);
+            }
+            ok = tc::mbar_wait(mb, phase) && ok;
+            phase ^= 1;
+            tc::fence_after();
+            if (layer < 3) {
+                sur_hidden_epilogue(trow, bias + layer * SUR_H, A, t);
+            } else {
+                float o[SUR_OUT];
+                tc::tmem_ld16(trow, o);
+#pragma unroll
+                for (int k = 0; k < SUR_OUT; k++) o[k] += bias[3 * SUR_H + k];
+                if (have) src.store(idx, o);
+            }
+        }
+        tc::fence_before();
+    }
+    if (!ok && err) atomicExch(err, 1);
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) tc::tmem_free(*slot, 128 * SUR_NG);
+}
+
+// ------------------------------------------------------ coupled-step apply
+struct SurQueue {
+    int *list;      // cell indices; bit 31 marks an audited cell
+    int *count;     // [0] list length, [1] work cursor
+    double *audit;  // per list slot: the surrogate's T for audited cells
+    long long cap;
+};
+
+struct SurApplyArgs {
+    CellArgs a;
+    const SurNorm *nrm;  // device copy
+    const float *out;  // 10 x n network outputs (SoA)
+    long long n;       // interior cells
+    SurQueue qu;
+    int audit_stride;  // 0: no audit
+};
+
+__device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int value, double audit_T)
+{
+    const unsigned act = __activemask();
+    const unsigned m = __ballot_sync(act, push);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(qu.count, __popc(m));
+    base = __shfl_sync(act, base, leader);
+    if (push) {
+        const int slot = base + __popc(m & ((1u << lane) - 1u));
+        if (slot < qu.cap) {
+            qu.list[slot] = value;
+            qu.audit[slot] = audit_T;
+        }
+    }
+}
+
+// One thread per interior cell.  The network's chemistry increment over dt is
+// taken for the state of the previous decode (the state the FP64 integrator
+// would evaluate its rates at), projected to element conservation, checked
+// against the training envelope, for negative mass fractions and for the
+// energy balance at the predicted temperature, then added to the
+// flux-updated conserved state, which is decoded in FP64.  Rejected cells
+// (and audited ones) go to the fallback list untouched.
+template <class P>
+__global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
+{
+    const CellArgs &a = s.a;
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    if (solid_cell(a, i, j)) return;
+    const long long c = L.at(i, j, k);
+    const long long fs = L.fs;
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    const unsigned qk = a.quirks;
+    const SurNorm &n = *s.nrm;
+    const double dt = a.scal[0];
+    double cs[NV];
+    load_cs(a.cs, fs, c, cs);
+    const double T = a.T[c], Eold = a.E[c];
+    double D = 0.0, sdiv = 0.0;
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) D += cs[sp];
+    double Y[NS];
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) {
+        Y[sp] = cs[sp] / D;
+        sdiv += Y[sp] / cM.mw[sp];
+    }
+    const double p = D * R_GAS * 1000 * sdiv * T;
+    // envelope and network-output arithmetic in FP32 (the network itself is BF16)
+    const float Tf = (float)T;
+    const float lnp = logf((float)(p * (1.0 / ATM_PA))), lndt = logf((float)dt);
+    bool ok = Tf >= n.v[SN_ENV + 0] && Tf <= n.v[SN_ENV + 1] && lnp >= n.v[SN_ENV + 2] && lnp <= n.v[SN_ENV + 3] &&
+              lndt >= n.v[SN_ENV + 4] && lndt <= n.v[SN_ENV + 5];
+    {
+        double el[SUR_NELEM];
+#pragma unroll
+        for (int e = 0; e < SUR_NELEM; e++) {
+            double x = 0.0;
+#pragma unroll
+            for (int sp = 0; sp < NS; sp++) x += c_sur_elem[e][sp] * Y[sp];
+            el[e] = x;
+        }
+        const double tol = n.v[SN_RATIO_TOL];
+        ok = ok && fabs(el[0] / (el[1] * n.v[SN_RATIO + 0]) - 1.0) <= tol &&
+             fabs(el[2] / (el[1] * n.v[SN_RATIO + 1]) - 1.0) <= tol;
+    }
+    const float sc = (float)dt * expf(n.v[SN_TA] * (1.f / n.v[SN_TR] - 1.f / Tf));
+    double dY[NS];
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) dY[sp] = (double)sur_unscale_f(n, sp, s.out[sp * s.n + idx], sc);
+    const double dTn = (double)sur_unscale_f(n, NS, s.out[NS * s.n + idx], sc);
+    sur_project(Y, dY, n.v[SN_PROJ_EPS]);
+    double Yn[NS];
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) {
+        const double y = Y[sp] + dY[sp];
+        ok = ok && y >= -(double)n.v[SN_NEG_TOL] && isfinite(y);
+        Yn[sp] = fmax(y, 0.0);
+    }
+    ok = ok && isfinite(dTn) && fabs(dTn) <= n.v[SN_DT_MAX];
+    double Tg = T + dTn;
+    if (ok) {
+        // energy balance at the predicted temperature (constant density and energy)
+        double e, cv;
+        mix_energy(Yn, Tg, qk, e, cv);
+        const double res = (e - Eold) / cv;
+        ok = fabs(res) <= n.v[SN_RES_ABS] + n.v[SN_RES_REL] * fabs(dTn);
+    }
+    Decoded o;
+    int capped = 0;
+    if (ok) {
+        // flux residual, then the chemistry increment on the species
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            double r = a.rhs[v * fs + c];
+            if (v < NS) r += D * (Yn[v] - Y[v]);
+            cs[v] = cs[v] + r;
+        }
+        decode(cs, Tg, Eold, qk, o, capped);
+        // a decode that fails or leaves the envelope's temperatures goes back
+        // to the integrator (from the untouched old state)
+        ok = !capped && isfinite(o.T) && isfinite(o.D) && o.T >= 0.8 * n.v[SN_ENV + 0] && o.T <= 1.2 * n.v[SN_ENV + 1];
+    }
+    const bool audit = ok && s.audit_stride > 0 && (idx % s.audit_stride) == 0;
+    if (ok) {
+        if (!audit) {
+            store_cs(a.cs, fs, c, cs);
+            a.T[c] = o.T;
+            a.E[c] = o.E;
+            store_prims<P>(o, q, fs, c);
+        }
+    }
+    sur_push(s.qu, !ok || audit, (int)c | (audit ? (int)0x80000000u : 0), audit ? o.T : 0.0);
+    warp_count(&a.st->sur_cells, ok && !audit);
+    warp_count(&a.st->sur_fallback, !ok);
+}
+
+// Persistent fallback queue: warps pull 32 listed cells at a time from a
+// global cursor and run the FP64 IMEX update of Euler::IMEX on each
+// (Diagonalized + Update_IMEX + decode).  For audited cells the surrogate's
+// temperature is compared with the integrator's and the largest difference
+// recorded.
+template <class P, bool SPEC>
+__global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restrict__ q, SurQueue qu)
+{
+    const int lane = threadIdx.x & 31;
+    const int total = min((long long)*qu.count, qu.cap);
+    const long long fs = a.L.fs;
+    const unsigned qk = a.quirks;
+    const double dt = a.scal[0];
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(qu.count + 1, 32);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        const int slot = base + lane;
+        if (slot < total) {
+            const int ent = qu.list[slot];
+            const bool audit = ent < 0;
+            const long long c = (long long)(ent & 0x7fffffff);
+            double cs[NV];
+            load_cs(a.cs, fs, c, cs);
+            const double T = a.T[c], Eold = a.E[c];
+            double CMS[NS], MD[NS];
+            imex_source<SPEC>(cs, T, qk, CMS, MD);
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                double r = a.rhs[v * fs + c];
+                if (v < NS) {
+                    r = r + CMS[v] * dt;
+                    cs[v] = cs[v] + r / (1.0 - dt * MD[v]);
+                } else {
+                    cs[v] = cs[v] + r;
+                }
+            }
+            Decoded o;
+            int capped = 0;
+            decode(cs, T, Eold, qk, o, capped);
+            store_cs(a.cs, fs, c, cs);
+            a.T[c] = o.T;
+            a.E[c] = o.E;
+            store_prims<P>(o, q, fs, c);
+            if (capped) atomicAdd(&a.st->newton_capped, 1ull);
+            if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
+            if (audit) {
+                const double d = fabs(qu.audit[slot] - o.T);
+                atomicAdd(&a.st->audit_cells, 1ull);
+                if (isfinite(d)) atomicMax(&a.st->audit_max_dT_bits, (unsigned long long)__double_as_longlong(d));
+                else atomicMax(&a.st->audit_max_dT_bits, 0x7ff0000000000000ull);
+            }
+        }
+    }
+}
+
+}  // namespace eu3d

@@ -35,7 +35,14 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_boundary", "eu3d_advection", "eu3d_update_after_adv", "eu3d_update_after_cs", "eu3d_react_imex",
            "eu3d_react_trapezoid", "eu3d_step", "eu3d_run", "eu3d_synchronize", "eu3d_get_status",
            "eu3d_reset_status", "eu3d_stream", "eu3d_profile_enable", "eu3d_profile_read", "eu3d_cfl_noalloc",
-           "eu3d_gemm_bf16"]
+           "eu3d_gemm_bf16", "eu3d_sur_create", "eu3d_sur_destroy", "eu3d_sur_reset_dataset",
+           "eu3d_sur_dataset_size", "eu3d_sur_add_random", "eu3d_sur_add_snapshot", "eu3d_sur_label",
+           "eu3d_sur_get_dataset", "eu3d_sur_set_norm", "eu3d_sur_get_norm", "eu3d_sur_set_params",
+           "eu3d_sur_get_params", "eu3d_sur_train", "eu3d_sur_loss_grad", "eu3d_sur_predict", "eu3d_sur_infer",
+           "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune"]
+
+SUR_NPARAM = 37264
+SUR_NORM_LEN = 80
 
 
 class Eu3dError(RuntimeError):
@@ -58,7 +65,15 @@ class StepDesc(C.Structure):
 class Status(C.Structure):
     _fields_ = [("nonfinite_cells", C.c_longlong), ("newton_capped", C.c_longlong), ("substeps", C.c_longlong),
                 ("nchem_max", C.c_int), ("substep_capped", C.c_int), ("surrogate_cells", C.c_longlong),
-                ("surrogate_fallback", C.c_longlong), ("dt", C.c_double), ("time", C.c_double)]
+                ("surrogate_fallback", C.c_longlong), ("dt", C.c_double), ("time", C.c_double),
+                ("surrogate_audited", C.c_longlong), ("surrogate_audit_max_dT", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(C.Structure):
+    _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -104,6 +119,29 @@ def load_library(path: Optional[str] = None):
         [C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     L.eu3d_gemm_bf16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.c_void_p, C.c_void_p]
+    _fp = C.POINTER(C.c_float)
+    L.eu3d_sur_create.argtypes = h + [C.c_longlong, _dp, C.POINTER(C.c_void_p)]
+    L.eu3d_sur_destroy.argtypes = h
+    L.eu3d_sur_reset_dataset.argtypes = h
+    L.eu3d_sur_dataset_size.argtypes = h + [C.POINTER(C.c_longlong)]
+    L.eu3d_sur_add_random.argtypes = h + [C.c_longlong, _dp, C.POINTER(C.c_int), C.c_ulonglong]
+    L.eu3d_sur_add_snapshot.argtypes = h + [C.c_void_p, C.c_longlong, C.c_longlong, C.c_longlong, C.c_double,
+                                            C.c_double, C.c_double, C.c_double, C.c_ulonglong]
+    L.eu3d_sur_label.argtypes = h + [C.c_int, C.c_int, C.c_double, C.POINTER(C.c_longlong)]
+    L.eu3d_sur_get_dataset.argtypes = h + [C.c_longlong, C.c_longlong, _dp, _fp, _fp]
+    L.eu3d_sur_set_norm.argtypes = h + [_fp]
+    L.eu3d_sur_get_norm.argtypes = h + [_fp]
+    L.eu3d_sur_set_params.argtypes = h + [_fp]
+    L.eu3d_sur_get_params.argtypes = h + [_fp]
+    L.eu3d_sur_train.argtypes = h + [C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_ulonglong, _fp]
+    L.eu3d_sur_loss_grad.argtypes = h + [_fp, _fp, C.c_int, _fp, _fp, _fp]
+    L.eu3d_sur_predict.argtypes = h + [_fp, C.c_longlong, _fp]
+    L.eu3d_sur_infer.argtypes = h + [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
+    L.eu3d_set_surrogate.argtypes = h + [C.c_void_p, C.c_int]
+    L.eu3d_react_surrogate.argtypes = h
+    L.eu3d_set_tuning.argtypes = h + [C.POINTER(Tuning)]
+    L.eu3d_get_tuning.argtypes = h + [C.POINTER(Tuning)]
+    L.eu3d_autotune.argtypes = h + [C.POINTER(StepDesc), C.c_int, C.POINTER(Tuning), _dp]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]
@@ -237,6 +275,14 @@ class DeviceFlowfield:
     def trapezoid(self, type_: int):
         _check(self.L.eu3d_react_trapezoid(self.h, type_))
 
+    def set_surrogate(self, sur, audit_stride: int = 0):
+        """Use a trained DeviceSurrogate (None: none) for REACT_SURROGATE steps."""
+        _check(self.L.eu3d_set_surrogate(self.h, sur.s if sur is not None else None, audit_stride))
+        self._sur = sur  # keeps the surrogate alive while attached
+
+    def react_surrogate(self):
+        _check(self.L.eu3d_react_surrogate(self.h))
+
     def step(self, react=REACT_IMEX, type_=0, timeadv=ADV_EE, diff=DIFF_MUSCL2, bc_kind=BC_RSBI, cfl=0.0,
              final_time=1.0):
         s = StepDesc(react, type_, timeadv, diff, bc_kind, cfl, final_time)
@@ -249,6 +295,31 @@ class DeviceFlowfield:
 
     def synchronize(self):
         _check(self.L.eu3d_synchronize(self.h))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(self.L.eu3d_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None):
+        t = Tuning(**self.tuning())
+        if flux_kz is not None:
+            t.flux_kz = flux_kz
+        if chem_queue is not None:
+            t.chem_queue = int(chem_queue)
+        if queue_blocks is not None:
+            t.queue_blocks = queue_blocks
+        _check(self.L.eu3d_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, steps=3, react=REACT_IMEX, type_=0, timeadv=ADV_EE, diff=DIFF_MUSCL2, bc_kind=BC_RSBI,
+                 cfl=0.0, final_time=1.0):
+        """Time the candidate launch settings on the current state (which is
+        restored) and keep the fastest; returns (setting, ms per step)."""
+        s = StepDesc(react, type_, timeadv, diff, bc_kind, cfl, final_time)
+        t = Tuning()
+        ms = C.c_double()
+        _check(self.L.eu3d_autotune(self.h, C.byref(s), steps, C.byref(t), C.byref(ms)))
+        return t.as_dict(), ms.value
 
     def status(self) -> dict:
         s = Status()
@@ -275,3 +346,121 @@ class DeviceFlowfield:
     @property
     def stream(self) -> int:
         return self.L.eu3d_stream(self.h)
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        raise Eu3dError(f"shape {a.shape} != {shape}")
+    return a
+
+
+class DeviceSurrogate:
+    """The learned chemistry surrogate's device side (training set, labels,
+    parameters, training and inference), bound to a DeviceFlowfield's device,
+    mechanism and quirk policy."""
+
+    def __init__(self, dev: DeviceFlowfield, capacity: int, atoms: np.ndarray):
+        self.L = dev.L
+        self.dev = dev
+        self.NS = dev.NS
+        a = np.ascontiguousarray(atoms, dtype=np.float64)
+        if a.shape != (3, dev.NS):
+            raise Eu3dError("atoms must be (3, NS): H, O, N counts per species")
+        self.s = C.c_void_p()
+        _check(self.L.eu3d_sur_create(dev.h, int(capacity), a.ctypes.data_as(_dp), C.byref(self.s)))
+        self.capacity = int(capacity)
+
+    def close(self):
+        if getattr(self, "s", None):
+            self.L.eu3d_sur_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ dataset
+    def reset_dataset(self):
+        _check(self.L.eu3d_sur_reset_dataset(self.s))
+
+    @property
+    def size(self) -> int:
+        n = C.c_longlong()
+        _check(self.L.eu3d_sur_dataset_size(self.s, C.byref(n)))
+        return n.value
+
+    def add_random(self, n: int, env, species_index, seed: int):
+        e = np.ascontiguousarray(env, dtype=np.float64)
+        sp = (C.c_int * 9)(*[int(x) for x in species_index])
+        _check(self.L.eu3d_sur_add_random(self.s, int(n), e.ctypes.data_as(_dp), sp, int(seed)))
+
+    def add_snapshot(self, src: DeviceFlowfield, n: int, stride: int, offset: int, jitter_T: float,
+                     jitter_lnp: float, lndt_lo: float, lndt_hi: float, seed: int):
+        _check(self.L.eu3d_sur_add_snapshot(self.s, src.h, int(n), int(stride), int(offset), jitter_T, jitter_lnp,
+                                            lndt_lo, lndt_hi, int(seed)))
+
+    def label(self, kind: int = REACT_IMEX, cap: int = 4096, proj_eps: float = 1e-4) -> int:
+        nv = C.c_longlong()
+        _check(self.L.eu3d_sur_label(self.s, kind, cap, proj_eps, C.byref(nv)))
+        return nv.value
+
+    def dataset(self, first: int = 0, count: Optional[int] = None, states: bool = False):
+        count = self.size - first if count is None else count
+        X = np.empty((count, 12), np.float32)
+        Lb = np.empty((count, 12), np.float32)
+        S = np.empty((count, 12), np.float64) if states else None
+        _check(self.L.eu3d_sur_get_dataset(self.s, first, count, S.ctypes.data_as(_dp) if states else None,
+                                           X.ctypes.data_as(C.POINTER(C.c_float)),
+                                           Lb.ctypes.data_as(C.POINTER(C.c_float))))
+        return (X, Lb, S) if states else (X, Lb)
+
+    # ------------------------------------------------------------- model
+    def set_norm(self, norm):
+        a = _f32(norm, (SUR_NORM_LEN,))
+        _check(self.L.eu3d_sur_set_norm(self.s, a.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def get_norm(self) -> np.ndarray:
+        a = np.empty(SUR_NORM_LEN, np.float32)
+        _check(self.L.eu3d_sur_get_norm(self.s, a.ctypes.data_as(C.POINTER(C.c_float))))
+        return a
+
+    def set_params(self, p):
+        a = _f32(p, (SUR_NPARAM,))
+        _check(self.L.eu3d_sur_set_params(self.s, a.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def get_params(self) -> np.ndarray:
+        a = np.empty(SUR_NPARAM, np.float32)
+        _check(self.L.eu3d_sur_get_params(self.s, a.ctypes.data_as(C.POINTER(C.c_float))))
+        return a
+
+    def train(self, steps: int, batch: int, lr_max: float, lr_min: float, warmup: int, seed: int) -> np.ndarray:
+        losses = np.zeros(max(steps, 1), np.float32)
+        _check(self.L.eu3d_sur_train(self.s, steps, batch, lr_max, lr_min, warmup, int(seed),
+                                     losses.ctypes.data_as(C.POINTER(C.c_float))))
+        return losses[:steps]
+
+    def loss_grad(self, X, Y):
+        B = X.shape[0]
+        X = _f32(X, (B, 16))
+        Y = _f32(Y, (B, 16))
+        loss = np.zeros(1, np.float32)
+        grad = np.empty(SUR_NPARAM, np.float32)
+        out = np.empty((B, 16), np.float32)
+        fp = C.POINTER(C.c_float)
+        _check(self.L.eu3d_sur_loss_grad(self.s, X.ctypes.data_as(fp), Y.ctypes.data_as(fp), B,
+                                         loss.ctypes.data_as(fp), grad.ctypes.data_as(fp), out.ctypes.data_as(fp)))
+        return float(loss[0]), grad, out
+
+    def predict(self, X) -> np.ndarray:
+        n = X.shape[0]
+        X = _f32(X, (n, 16))
+        out = np.empty((n, 16), np.float32)
+        fp = C.POINTER(C.c_float)
+        _check(self.L.eu3d_sur_predict(self.s, X.ctypes.data_as(fp), n, out.ctypes.data_as(fp)))
+        return out
+
+    def infer_device(self, x_ptr: int, n: int, out_ptr: int, stream: int = 0):
+        _check(self.L.eu3d_sur_infer(self.s, x_ptr, n, out_ptr, stream or None))

@@ -1,0 +1,359 @@
+"""Host side of the learned chemistry surrogate: training-set recipe,
+normalisation, parameter initialisation, the training driver and the model
+file.  The device work (sampling, FP64 labels, training kernels, fused
+inference, coupled step) is in the CUDA library, reached through
+``gpu.DeviceSurrogate``.
+
+Model: MLP 12 -> 128 -> 128 -> 128 -> 10 with GELU, BF16 weights and FP32
+accumulation.  Inputs: T, ln(p/atm), ln(Y_k + 1e-12), ln dt (standardised;
+three spare input columns carry BF16 rounding residuals of T, ln p, ln dt).
+Outputs: the chemistry increment over dt of a closed constant-density,
+constant-energy reactor, dY_k and dT, as labelled by the project's FP64
+integrator (one Diagonalized + Update_IMEX step of the reference's
+Euler::IMEX, src/Reaction.cpp:736-811 and src/Flowfield.cpp:1215-1234, or the
+TrapezoidPrediction substeps of src/Reaction.cpp:489-670), projected to
+element conservation.  Targets are scaled by dt A(T), A(T) = exp(Ta (1/Tr -
+1/T)), compressed with asinh(x / lin_k) and standardised.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import re
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import gpu
+from .cases import ATM, odw_case, setup_odw, znd_case, upload_primitive_state
+from .readers import stoichiometric_h2_air
+
+NORM_LEN = gpu.SUR_NORM_LEN
+NPARAM = gpu.SUR_NPARAM
+N_IN, N_OUT, IN_PAD, H, OUT_PAD = 12, 10, 16, 128, 16
+OFF = {}
+_o = 0
+for _name, _n in (("W1", IN_PAD * H), ("b1", H), ("W2", H * H), ("b2", H), ("W3", H * H), ("b3", H),
+                  ("W4", H * OUT_PAD), ("b4", OUT_PAD)):
+    OFF[_name] = (_o, _n)
+    _o += _n
+assert _o == NPARAM
+
+# offsets of the normalisation vector (include/eu3d_gpu.h EU3D_SUR_N_*)
+N_IN_MEAN, N_IN_STD, N_OUT_MEAN, N_OUT_STD, N_LIN = 0, 12, 24, 34, 44
+N_TA, N_TR, N_ENV, N_RATIO, N_RATIO_TOL, N_RES_ABS, N_RES_REL, N_NEG_TOL, N_PROJ_EPS, N_DT_MAX = \
+    54, 55, 56, 62, 64, 65, 66, 67, 68, 69
+
+RADICAL_ORDER = ("H", "O", "H2O", "OH", "O2", "H2", "H2O2", "HO2", "N2")
+ELEMENTS = ("H", "O", "N")
+
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+DEFAULT_MODEL = os.path.join(DATA_DIR, "sur_h2_ja919_imex.npz")
+
+
+def atoms_matrix(mech) -> np.ndarray:
+    """(3, NS) counts of H, O, N atoms per species, parsed from the names."""
+    A = np.zeros((3, mech.NS))
+    for k, name in enumerate(mech.species):
+        for el, cnt in re.findall(r"([A-Z][a-z]?)(\d*)", name):
+            if el in ELEMENTS:
+                A[ELEMENTS.index(el), k] += int(cnt) if cnt else 1
+    return A
+
+
+def species_index(mech) -> list:
+    return [mech.species.index(s) for s in RADICAL_ORDER]
+
+
+def element_ratios(mech, Y) -> np.ndarray:
+    """(H/O, N/O) atom ratios of mass fractions Y (..., NS)."""
+    A = atoms_matrix(mech) / mech.mw
+    el = np.asarray(Y) @ A.T
+    return np.stack([el[..., 0] / el[..., 1], el[..., 2] / el[..., 1]], axis=-1)
+
+
+def activity(T, Ta, Tr):
+    return np.exp(Ta * (1.0 / Tr - 1.0 / np.asarray(T, dtype=np.float64)))
+
+
+def bf16_round(x):
+    """Round-to-nearest-even to BF16, returned as float32."""
+    a = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    r = ((a >> 16) & 1) + np.uint32(0x7FFF)
+    return ((a + r) & np.uint32(0xFFFF0000)).view(np.float32)
+
+
+def features(X, norm) -> np.ndarray:
+    """Normalised network inputs (n, 16) of raw features X (n, 12), with the
+    arithmetic of the device (FP32; residual columns 12..14)."""
+    X = np.asarray(X, dtype=np.float32)
+    f = np.zeros((X.shape[0], IN_PAD), np.float32)
+    f[:, :N_IN] = (X - norm[N_IN_MEAN:N_IN_MEAN + N_IN]) / norm[N_IN_STD:N_IN_STD + N_IN]
+    for col, src in ((12, 0), (13, 1), (14, 11)):
+        f[:, col] = (f[:, src] - bf16_round(f[:, src])) * np.float32(256.0)
+    return f
+
+
+def targets(X, Lb, norm) -> np.ndarray:
+    """Standardised targets (n, 16) of raw labels Lb (n, 12); column 15 = weight."""
+    X = np.asarray(X, dtype=np.float64)
+    sc = np.exp(X[:, 11]) * activity(X[:, 0], norm[N_TA], norm[N_TR])
+    x = np.asarray(Lb[:, :N_OUT], dtype=np.float64) / sc[:, None]
+    y = np.arcsinh(x / norm[N_LIN:N_LIN + N_OUT])
+    t = np.zeros((X.shape[0], OUT_PAD), np.float32)
+    t[:, :N_OUT] = (y - norm[N_OUT_MEAN:N_OUT_MEAN + N_OUT]) / norm[N_OUT_STD:N_OUT_STD + N_OUT]
+    t[:, 15] = Lb[:, 10]
+    return t
+
+
+def unscale(out, X, norm) -> np.ndarray:
+    """Raw labels (n, 10) from network outputs (n, >=10)."""
+    X = np.asarray(X, dtype=np.float64)
+    sc = np.exp(X[:, 11]) * activity(X[:, 0], norm[N_TA], norm[N_TR])
+    y = np.asarray(out[:, :N_OUT], np.float64) * norm[N_OUT_STD:N_OUT_STD + N_OUT] + norm[N_OUT_MEAN:N_OUT_MEAN + N_OUT]
+    return sc[:, None] * norm[N_LIN:N_LIN + N_OUT] * np.sinh(y)
+
+
+def make_norm(mech, X, Lb, Ta=8000.0, Tr=1500.0, env=None, ratio_tol=0.02, res_abs=5.0, res_rel=0.05,
+              neg_tol=1e-6, proj_eps=1e-4, lin_quantile=0.01, dT_max=2500.0) -> np.ndarray:
+    """Normalisation and acceptance vector from (a sample of) the raw set."""
+    ok = Lb[:, 10] > 0
+    Xv, Lv = np.asarray(X[ok], np.float64), np.asarray(Lb[ok], np.float64)
+    n = np.zeros(NORM_LEN, np.float32)
+    n[N_IN_MEAN:N_IN_MEAN + N_IN] = Xv.mean(axis=0)
+    n[N_IN_STD:N_IN_STD + N_IN] = np.maximum(Xv.std(axis=0), 1e-6)
+    n[N_TA], n[N_TR] = Ta, Tr
+    sc = np.exp(Xv[:, 11]) * activity(Xv[:, 0], Ta, Tr)
+    x = Lv[:, :N_OUT] / sc[:, None]
+    lin = np.empty(N_OUT)
+    for k in range(N_OUT):
+        a = np.abs(x[:, k])
+        a = a[a > 0]
+        lin[k] = max(np.quantile(a, lin_quantile), 1e-30) if a.size else 1.0
+    n[N_LIN:N_LIN + N_OUT] = lin
+    y = np.arcsinh(x / lin)
+    n[N_OUT_MEAN:N_OUT_MEAN + N_OUT] = y.mean(axis=0)
+    n[N_OUT_STD:N_OUT_STD + N_OUT] = np.maximum(y.std(axis=0), 1e-6)
+    if env is None:
+        env = (Xv[:, 0].min(), Xv[:, 0].max(), Xv[:, 1].min(), Xv[:, 1].max(), Xv[:, 11].min(), Xv[:, 11].max())
+    n[N_ENV:N_ENV + 6] = env
+    n[N_RATIO:N_RATIO + 2] = element_ratios(mech, stoichiometric_h2_air(mech))
+    n[N_RATIO_TOL], n[N_RES_ABS], n[N_RES_REL], n[N_NEG_TOL], n[N_PROJ_EPS], n[N_DT_MAX] = \
+        ratio_tol, res_abs, res_rel, neg_tol, proj_eps, dT_max
+    return n
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """LeCun-normal weights (std 1/sqrt(fan_in) over the used inputs), zero
+    biases; padded input rows and unused output columns are zero."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NPARAM, np.float32)
+
+    def put(name, a):
+        o, m = OFF[name]
+        p[o:o + m] = a.reshape(-1)
+
+    W1 = rng.standard_normal((IN_PAD, H)) / np.sqrt(N_IN + 3)
+    W1[15] = 0.0
+    put("W1", W1)
+    put("W2", rng.standard_normal((H, H)) / np.sqrt(H))
+    put("W3", rng.standard_normal((H, H)) / np.sqrt(H))
+    W4 = rng.standard_normal((H, OUT_PAD)) / np.sqrt(H)
+    W4[:, N_OUT:] = 0.0
+    put("W4", W4)
+    return p
+
+
+@dataclasses.dataclass
+class SurrogateModel:
+    params: np.ndarray
+    norm: np.ndarray
+    meta: dict
+
+    def save(self, path: str):
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez(path, params=self.params.astype(np.float32), norm=self.norm.astype(np.float32),
+                 meta=np.frombuffer(json.dumps(self.meta).encode(), dtype=np.uint8))
+
+    @classmethod
+    def load(cls, path: str) -> "SurrogateModel":
+        z = np.load(path)
+        return cls(z["params"].astype(np.float32), z["norm"].astype(np.float32),
+                   json.loads(bytes(z["meta"]).decode()))
+
+    def attach(self, dev: gpu.DeviceFlowfield, audit_stride: int = 0) -> gpu.DeviceSurrogate:
+        """A device surrogate with these parameters, attached to dev."""
+        s = gpu.DeviceSurrogate(dev, 0, atoms_matrix(dev.mech))
+        s.set_norm(self.norm)
+        s.set_params(self.params)
+        dev.set_surrogate(s, audit_stride)
+        return s
+
+
+# ----------------------------------------------------------- training set
+@dataclasses.dataclass
+class Recipe:
+    """Training-set and optimiser settings.  Defaults: 2^22 states, half from
+    flowfield snapshots (2D ODW at two resolutions and the 1D ZND, run with
+    the FP64 IMEX integrator), half uniform random states; labels from the
+    closed-reactor IMEX step."""
+
+    n_total: int = 1 << 22
+    frac_random: float = 0.3
+    T_range: tuple = (250.0, 3500.0)
+    p_atm_range: tuple = (0.05, 50.0)
+    dt_range: tuple = (1e-9, 1e-7)
+    jitter_T: float = 0.05
+    jitter_lnp: float = 0.1
+    odw_grids: tuple = ((1024, 512), (512, 256))
+    odw_steps: tuple = (4000, 2500)
+    znd_ni: int = 4000
+    znd_steps: int = 1500
+    snapshots_per_run: int = 8
+    label_kind: int = gpu.REACT_IMEX
+    label_cap: int = 4096
+    steps: int = 20000
+    batch: int = 8192
+    lr_max: float = 2e-3
+    lr_min: float = 2e-5
+    warmup: int = 500
+    Ta: float = 8000.0
+    Tr: float = 1500.0
+    seed: int = 1234
+
+
+def _snapshot_runs(mech, recipe: Recipe, sur: gpu.DeviceSurrogate, n_snap: int, log=print):
+    """Run the config-2 style 2D ODW cases and the 1D ZND with the IMEX
+    integrator and sample their interior cells every few steps."""
+    runs = []
+    for (ni, nj), ns in zip(recipe.odw_grids, recipe.odw_steps):
+        runs.append(("odw", ni, nj, ns))
+    if recipe.znd_ni:
+        runs.append(("znd", recipe.znd_ni, 2, recipe.znd_steps))
+    per_run = n_snap // max(len(runs), 1)
+    lndt = (np.log(recipe.dt_range[0]), np.log(recipe.dt_range[1]))
+    seed = recipe.seed
+    for kind, ni, nj, nsteps in runs:
+        if kind == "odw":
+            case = odw_case(mech, ni, nj, 2, seed=seed)
+            dev = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=32)
+            setup_odw(dev, case)
+            bc = gpu.BC_ODM
+        else:
+            g, st = znd_case(mech, ni)
+            dev = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=32)
+            upload_primitive_state(dev, st)
+            dev.update_after_cs()
+            bc = gpu.BC_TRANSMISSIVE
+        # config 1 (ZND) runs its own scheme: SSP-RK2 with the adaptive
+        # trapezoid; the ODW cases use the IMEX integrator
+        # (at CFL 0.5 the scheme itself goes non-finite in its first step at
+        # the driver interface: AUSM moves momentum, not energy, across a
+        # face whose two sides are at rest, so ZND runs at CFL 0.3)
+        scheme = (dict(react=gpu.REACT_IMEX, cfl=0.5) if kind == "odw" else
+                  dict(react=gpu.REACT_TRAPEZOID, type_=1, timeadv=gpu.ADV_SSPRK2, cfl=0.3))
+        ncell = dev.grid.ni * dev.grid.nj * dev.grid.nk
+        k = recipe.snapshots_per_run
+        chunk = nsteps // k
+        n_each = per_run // k
+        t0 = time.time()
+        for s in range(k):
+            dev.run(chunk, bc_kind=bc, final_time=1.0, **scheme)
+            dev.synchronize()
+            st_ = dev.status()
+            if st_["nonfinite_cells"]:
+                log(f"[surrogate] {kind} {ni}x{nj} went non-finite after {(s + 1) * chunk} steps; "
+                    f"its remaining snapshots are skipped")
+                break
+            stride = max(ncell // n_each, 1)
+            take = min(n_each, ncell // stride)
+            seed += 1
+            off = int(np.random.default_rng(seed).integers(0, max(ncell - (take - 1) * stride, 1)))
+            sur.add_snapshot(dev, take, stride, off, recipe.jitter_T, recipe.jitter_lnp, lndt[0], lndt[1], seed)
+        log(f"[surrogate] snapshots of {kind} {ni}x{nj}: {nsteps} steps, {time.time() - t0:.1f} s")
+        dev.close()
+
+
+def build_dataset(mech, dev: gpu.DeviceFlowfield, recipe: Recipe, log=print) -> gpu.DeviceSurrogate:
+    sur = gpu.DeviceSurrogate(dev, recipe.n_total, atoms_matrix(mech))
+    n_rand = int(recipe.n_total * recipe.frac_random)
+    _snapshot_runs(mech, recipe, sur, recipe.n_total - n_rand, log)
+    n_rand = recipe.n_total - sur.size
+    env = (recipe.T_range[0], recipe.T_range[1], np.log(recipe.p_atm_range[0]), np.log(recipe.p_atm_range[1]),
+           np.log(recipe.dt_range[0]), np.log(recipe.dt_range[1]))
+    sur.add_random(n_rand, env, species_index(mech), recipe.seed + 7)
+    t0 = time.time()
+    nv = sur.label(recipe.label_kind, recipe.label_cap)
+    log(f"[surrogate] labelled {sur.size} states ({nv} usable) in {time.time() - t0:.1f} s")
+    return sur
+
+
+def train_model(mech, dev: gpu.DeviceFlowfield, recipe: Optional[Recipe] = None, log=print,
+                sur: Optional[gpu.DeviceSurrogate] = None):
+    """Build the training set, fit the network on the GPU, and return the
+    model with held-out errors in its meta."""
+    recipe = recipe or Recipe()
+    t_start = time.time()
+    if sur is None:
+        sur = build_dataset(mech, dev, recipe, log)
+    n = sur.size
+    rng = np.random.default_rng(recipe.seed)
+    X, Lb = sur.dataset()
+    env = (recipe.T_range[0], recipe.T_range[1], np.log(recipe.p_atm_range[0]), np.log(recipe.p_atm_range[1]),
+           np.log(recipe.dt_range[0]), np.log(recipe.dt_range[1]))
+    pick = rng.choice(n, size=min(n, 1 << 18), replace=False)
+    norm = make_norm(mech, X[pick], Lb[pick], recipe.Ta, recipe.Tr, env)
+    sur.set_norm(norm)
+    sur.set_params(init_params(recipe.seed))
+    t0 = time.time()
+    losses = sur.train(recipe.steps, recipe.batch, recipe.lr_max, recipe.lr_min, recipe.warmup, recipe.seed)
+    t_train = time.time() - t0
+    params = sur.get_params()
+    hold = rng.choice(n, size=min(n, 1 << 16), replace=False)
+    err = evaluate(sur, X[hold], Lb[hold], norm)
+    meta = dict(recipe=dataclasses.asdict(recipe), n_samples=int(n), train_seconds=t_train,
+                total_seconds=time.time() - t_start, final_loss=float(np.mean(losses[-100:])),
+                first_loss=float(np.mean(losses[:10])), heldout=err)
+    log(f"[surrogate] trained {recipe.steps} steps x {recipe.batch} in {t_train:.1f} s; "
+        f"loss {meta['first_loss']:.3g} -> {meta['final_loss']:.3g}; held-out {err}")
+    return SurrogateModel(params, norm, meta), sur, losses
+
+
+def evaluate(sur: gpu.DeviceSurrogate, X, Lb, norm) -> dict:
+    """Held-out errors of the network in target space and on dT."""
+    ok = Lb[:, 10] > 0
+    X, Lb = X[ok], Lb[ok]
+    out = sur.predict(features(X, norm))
+    t = targets(X, Lb, norm)
+    mse = float(np.mean((out[:, :N_OUT] - t[:, :N_OUT]) ** 2))
+    raw = unscale(out, X, norm)
+    dT_err = np.abs(raw[:, 9] - Lb[:, 9])
+    return dict(mse=mse, dT_mae=float(dT_err.mean()), dT_p99=float(np.quantile(dT_err, 0.99)),
+                dT_max=float(dT_err.max()), n=int(X.shape[0]))
+
+
+def main(argv=None):
+    import argparse
+
+    from .readers import load_h2_ja919
+    ap = argparse.ArgumentParser(description="train the chemistry surrogate on the GPU")
+    ap.add_argument("--out", default=DEFAULT_MODEL)
+    ap.add_argument("--samples", type=int, default=Recipe.n_total)
+    ap.add_argument("--steps", type=int, default=Recipe.steps)
+    ap.add_argument("--batch", type=int, default=Recipe.batch)
+    ap.add_argument("--seed", type=int, default=Recipe.seed)
+    a = ap.parse_args(argv)
+    mech = load_h2_ja919()
+    from .readers import make_grid
+    g = make_grid(8, 0.0, 1.0, 4, 0.0, 1.0, 2, 0.0, 1.0, 2, fixed_ghosts=True)
+    dev = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=32)
+    rec = Recipe(n_total=a.samples, steps=a.steps, batch=a.batch, seed=a.seed)
+    model, sur, losses = train_model(mech, dev, rec)
+    model.save(a.out)
+    print(json.dumps(model.meta["heldout"]))
+
+
+if __name__ == "__main__":
+    main()

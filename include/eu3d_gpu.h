@@ -60,6 +60,7 @@ typedef struct {
 } eu3d_desc;
 
 typedef struct eu3d_handle eu3d_handle;
+typedef struct eu3d_surrogate eu3d_surrogate;
 
 /* Field identifiers for upload/download.  Shapes (reference layout):
    3D fields NI*NJ*NK; EU3D_FIELD_YI/MC/DI NI*NJ*NK*NS; CS/RHS NI*NJ*NK*(NS+4). */
@@ -91,6 +92,8 @@ typedef struct {
     long long surrogate_cells;   /* cells advanced by the learned surrogate */
     long long surrogate_fallback;/* cells sent back to the integrator */
     double dt, time;             /* device copies of Flowfield::dt / ::time */
+    long long surrogate_audited; /* surrogate cells re-run by the integrator to judge it */
+    double surrogate_audit_max_dT; /* largest |T_surrogate - T_integrator| over audited cells [K] */
 } eu3d_status;
 
 const char *eu3d_last_error(void);
@@ -148,6 +151,24 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s);
    after each step only when check_time is nonzero). */
 int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time);
 int eu3d_synchronize(eu3d_handle *h);
+/* Launch settings picked per handle (new): z planes walked by one flux block,
+   adaptive trapezoid on the persistent work queue (1) or one thread per cell
+   (0), and resident queue blocks per SM.  Changing them drops the recorded
+   step graphs. */
+typedef struct {
+    int flux_kz;
+    int chem_queue;
+    int queue_blocks;
+} eu3d_tuning;
+int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t);
+int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t);
+/* Autotuner: times `steps` steps of s for each candidate setting (flux_kz in
+   {4, 8, 16, 32}; for the adaptive trapezoid also the queue on/off and 2..4
+   blocks per SM) on the handle's current state, restoring the state after
+   each trial, and keeps the fastest.  best / best_ms may be NULL.  Needs
+   temporary device memory for one copy of the state. */
+int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tuning *best, double *best_ms);
+
 /* Per-kernel timing with CUDA events on the handle's stream (replaces the
    reference's MPI_Wtime phase timers, src/Euler.cpp:256-344).  While enabled,
    eu3d_step launches its kernels directly instead of replaying its graph.
@@ -191,6 +212,92 @@ int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const do
    ran out of its bound.  Queued on `stream`, no synchronisation. */
 int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int accumulate, int *err,
                    void *stream);
+
+/* ---- Learned chemistry surrogate (new; no counterpart in the reference) ----
+   An MLP 12 -> 128 -> 128 -> 128 -> 10 (GELU), BF16 weights, FP32
+   accumulation on the tensor cores, maps a cell's (T, ln p, Y_k, ln dt) to the
+   chemistry increment (dY_k, dT) over dt.  Its training set lives on the
+   device: sampled states (T, p, Y_k, dt in FP64) labelled by the project's
+   own FP64 integrators.  Parameters: flat FP32 vector of EU3D_SUR_NPARAM
+   values, W1[16][128] b1[128] W2[128][128] b2[128] W3[128][128] b3[128]
+   W4[128][16] b4[16] (W[in][out]; rows 12..15 of W1 take the padded inputs,
+   columns 10..15 of W4 are unused).  Normalisation / acceptance vector: float
+   [EU3D_SUR_NORM_LEN] with the offsets below. */
+#define EU3D_SUR_NPARAM 37264
+#define EU3D_SUR_NORM_LEN 80
+#define EU3D_SUR_N_IN_MEAN 0    /* 12 raw-feature means: T, ln(p/atm), Y_0..8, ln dt */
+#define EU3D_SUR_N_IN_STD 12    /* 12 raw-feature scales */
+#define EU3D_SUR_N_OUT_MEAN 24  /* 10 target means (asinh space) */
+#define EU3D_SUR_N_OUT_STD 34   /* 10 target scales */
+#define EU3D_SUR_N_LIN 44       /* 10 asinh linear scales */
+#define EU3D_SUR_N_TA 54        /* activity temperature Ta [K] */
+#define EU3D_SUR_N_TR 55        /* activity reference temperature Tr [K] */
+#define EU3D_SUR_N_ENV 56       /* envelope: T_lo, T_hi, lnp_lo, lnp_hi, lndt_lo, lndt_hi */
+#define EU3D_SUR_N_RATIO 62     /* element ratios H/O, N/O of the training set */
+#define EU3D_SUR_N_RATIO_TOL 64 /* relative tolerance on those ratios */
+#define EU3D_SUR_N_RES_ABS 65   /* energy-residual tolerance [K] ... */
+#define EU3D_SUR_N_RES_REL 66   /* ... plus this fraction of |dT| */
+#define EU3D_SUR_N_NEG_TOL 67   /* most negative mass fraction accepted (then clipped to 0) */
+#define EU3D_SUR_N_PROJ_EPS 68  /* weight floor of the element projection */
+#define EU3D_SUR_N_DT_MAX 69    /* largest |dT| accepted from the network [K] */
+
+/* Surrogate bound to h's device, quirk policy and mechanism; atoms: (3, NS)
+   counts of H, O, N atoms per species; capacity: training samples. */
+int eu3d_sur_create(eu3d_handle *h, long long capacity, const double *atoms, eu3d_surrogate **out);
+int eu3d_sur_destroy(eu3d_surrogate *s);
+int eu3d_sur_reset_dataset(eu3d_surrogate *s);
+int eu3d_sur_dataset_size(eu3d_surrogate *s, long long *n);
+/* n random states: T uniform in [env0, env1] K, ln(p/atm) in [env2, env3],
+   ln dt in [env4, env5], composition at the element ratios of stoichiometric
+   H2-air; species: indices of H, O, H2O, OH, O2, H2, H2O2, HO2, N2. */
+int eu3d_sur_add_random(eu3d_surrogate *s, long long n, const double *env, const int *species,
+                        unsigned long long seed);
+/* n samples of src's interior cells (offset, offset + stride, ...): T, p, Y
+   with T scaled by 1 + jitter_T u, p by exp(jitter_lnp u), u uniform in
+   [-1, 1], and ln dt uniform in [lndt_lo, lndt_hi]. */
+int eu3d_sur_add_snapshot(eu3d_surrogate *s, eu3d_handle *src, long long n, long long stride, long long offset,
+                          double jitter_T, double jitter_lnp, double lndt_lo, double lndt_hi,
+                          unsigned long long seed);
+/* FP64 labels of every sample: kind EU3D_REACT_IMEX (one closed-reactor
+   Diagonalized + Update_IMEX step, src/Reaction.cpp:736-811,
+   src/Flowfield.cpp:1215-1234) or EU3D_REACT_TRAPEZOID (TrapezoidPrediction
+   substeps, src/Reaction.cpp:489-670, at most cap), projected to element
+   conservation (weight floor proj_eps) and decoded at constant density and
+   energy.  n_valid (may be NULL) counts the usable samples. */
+int eu3d_sur_label(eu3d_surrogate *s, int kind, int cap, double proj_eps, long long *n_valid);
+/* rows [first, first + count) of the states (12 doubles), raw features and
+   raw labels (12 floats each); any output may be NULL */
+int eu3d_sur_get_dataset(eu3d_surrogate *s, long long first, long long count, double *states, float *X, float *L);
+int eu3d_sur_set_norm(eu3d_surrogate *s, const float *norm);
+int eu3d_sur_get_norm(eu3d_surrogate *s, float *norm);
+/* parameters in and out; setting them also clears the Adam moments */
+int eu3d_sur_set_params(eu3d_surrogate *s, const float *params);
+int eu3d_sur_get_params(eu3d_surrogate *s, float *params);
+/* steps Adam steps (beta 0.9, 0.999) on random minibatches of `batch` samples
+   (a multiple of 256): linear warm-up to lr_max over `warmup` steps, then a
+   cosine decay to lr_min.  losses (may be NULL): per-step MSE. */
+int eu3d_sur_train(eu3d_surrogate *s, int steps, int batch, float lr_max, float lr_min, int warmup,
+                   unsigned long long seed, float *losses);
+/* loss and gradient (EU3D_SUR_NPARAM) for one host batch: X (batch x 16
+   normalised inputs), Y (batch x 16 standardised targets, column 15 = sample
+   weight); out (batch x 16, may be NULL): network outputs.  No update. */
+int eu3d_sur_loss_grad(eu3d_surrogate *s, const float *X, const float *Y, int batch, float *loss, float *grad,
+                       float *out);
+/* inference with the fused tensor-core kernel: X (n x 16 normalised inputs)
+   -> out (n x 16 outputs); host buffers (predict, synchronous) or device
+   buffers on `stream` (infer, NULL = the surrogate's stream, asynchronous). */
+int eu3d_sur_predict(eu3d_surrogate *s, const float *X, long long n, float *out);
+int eu3d_sur_infer(eu3d_surrogate *s, const float *X_dev, long long n, float *out_dev, void *stream);
+/* Use s (NULL: none) for EU3D_REACT_SURROGATE steps of h.  Every
+   audit_stride-th accepted cell (0: none) also runs the FP64 integrator,
+   which keeps its result and records the surrogate's temperature error. */
+int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride);
+/* Learned chemistry step of h after the flux residual is in RHS: network
+   increment for the previous decode's state, element projection, envelope /
+   negativity / energy-residual checks, EE update + FP64 decode; rejected
+   cells run the FP64 IMEX step (Euler::IMEX, src/Euler.cpp:748-760) on the
+   device work queue. */
+int eu3d_react_surrogate(eu3d_handle *h);
 
 /* Pointer to the handle's CUDA stream (cudaStream_t), for callers that
    interleave their own work. */
