@@ -311,8 +311,11 @@ __device__ __forceinline__ void warp_sum(unsigned long long *ctr, unsigned long 
 // Reaction::Diagonalized for the state of the previous decode (the stored CS
 // and T), with GetPartial_T (src/Flowfield.cpp:1578-1595) for its Jacobian:
 // source CMS (kg/m^3/s) and diagonal MD of the partial densities.
+// tcouple = false drops the temperature coupling of the Jacobian (PT = 0),
+// leaving its composition part (the adaptive integrator below).
 template <bool SPEC>
-__device__ __forceinline__ void imex_source(const double cs[NV], double T, unsigned qk, double CMS[NS], double MD[NS])
+__device__ __forceinline__ void imex_source(const double cs[NV], double T, unsigned qk, double CMS[NS], double MD[NS],
+                                            bool tcouple = true)
 {
     // state of the previous decode, recomputed from the stored CS and T
     double D = 0.0;
@@ -345,7 +348,7 @@ __device__ __forceinline__ void imex_source(const double cs[NV], double T, unsig
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         const double hs = (qk & EU3D_Q_PARTIAL_T_UNITS) ? cM.ri[s] * hr[s] : (cM.ri[s] * hr[s]) * 1e3;
-        PT[s] = (ke - hs + cM.ri[s] * 1e3 * T) / (CV * D);
+        PT[s] = tcouple ? (ke - hs + cM.ri[s] * 1e3 * T) / (CV * D) : 0.0;
         G[s] = R_GAS * hr[s] - (R_GAS * sr[s]) * T;
         Di[s] = cs[s] * 1e-3;
         Mc[s] = (cs[s] / cM.mw[s] * 1000) * 1e-6;
@@ -354,6 +357,135 @@ __device__ __forceinline__ void imex_source(const double cs[NV], double T, unsig
         h2ja919::diagonalized_spec(p, G, Mc, Di, PT, CMS, MD);
     else
         diagonalized(p, G, Mc, Di, PT, CMS, MD);
+}
+
+// FP64 adaptive closed-reactor chemistry (new; the reference's one-step IMEX
+// and adaptive trapezoid both diverge through H2-air ignition at the step
+// sizes of its detonation cases).  Substeps of the species-diagonal implicit
+// update rho_s += h CMS_s / (1 - h MD_s), with CMS and the composition part of
+// the diagonal Jacobian MD from Reaction::Diagonalized at the current state,
+// and a decode at constant density and energy after each.  The substep is the
+// largest h <= the time left with h |CMS_s| <= rel (rho_s + 1e-9 rho) for
+// every species and h MD_s <= amp where MD_s > 0 (growth stays bounded and
+// consumed species stay positive), but at least dt / nmax; the last allowed
+// substep takes the time left.
+struct AdaptCfg {
+    double rel, amp;
+    int nmax;
+};
+
+template <bool SPEC>
+__device__ __forceinline__ int chem_adaptive(double cs[NV], double &T, double Eold, unsigned qk, double dt,
+                                             const AdaptCfg &cfg, int &capped_any)
+{
+    double trem = dt;
+    int k = 0;
+    const double hmin = dt / cfg.nmax;
+    Decoded o;
+    while (trem > 0.0 && k < cfg.nmax) {
+        double CMS[NS], MD[NS];
+        imex_source<SPEC>(cs, T, qk, CMS, MD, false);
+        double D = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) D += cs[s];
+        double h = trem;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const double w = fabs(CMS[s]);
+            if (w > 0.0) h = fmin(h, cfg.rel * (cs[s] + 1e-9 * D) / w);
+            if (MD[s] > 0.0) h = fmin(h, cfg.amp / MD[s]);
+        }
+        h = fmin(fmax(h, hmin), trem);
+        if (k == cfg.nmax - 1) h = trem;
+#pragma unroll
+        for (int s = 0; s < NS; s++) cs[s] = fmax(cs[s] + h * CMS[s] / (1.0 - h * MD[s]), 0.0);
+        int cp = 0;
+        decode(cs, T, Eold, qk, o, cp);
+        capped_any |= cp;
+        T = o.T;
+        trem -= h;
+        k++;
+    }
+    return k;
+}
+
+// Element projection of a composition change: the least change in the
+// metric sum_k dY_k^2 / (Y_k + eps) that conserves the atoms of each element.
+constexpr int SUR_NELEM = 3;  // H, O, N
+// atoms of element e per unit mass of species k (atoms / W_k)
+__constant__ double c_sur_elem[SUR_NELEM][NS];
+
+__device__ __forceinline__ void elem_project(const double Y[NS], double dY[NS], double eps)
+{
+    double r[SUR_NELEM], M[SUR_NELEM][SUR_NELEM];
+#pragma unroll
+    for (int e = 0; e < SUR_NELEM; e++) {
+        double a = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; k++) a += c_sur_elem[e][k] * dY[k];
+        r[e] = a;
+#pragma unroll
+        for (int f = 0; f < SUR_NELEM; f++) {
+            double m = 0.0;
+#pragma unroll
+            for (int k = 0; k < NS; k++) m += c_sur_elem[e][k] * (Y[k] + eps) * c_sur_elem[f][k];
+            M[e][f] = m;
+        }
+    }
+    // 3x3 solve by cofactors
+    const double c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+    const double c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+    const double c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+    const double det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
+    if (!(fabs(det) > 0.0)) return;
+    const double id = 1.0 / det;
+    const double inv[3][3] = {{c00 * id, (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id,
+                               (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id},
+                              {c01 * id, (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id,
+                               (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id},
+                              {c02 * id, (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id,
+                               (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id}};
+    double lam[SUR_NELEM];
+#pragma unroll
+    for (int e = 0; e < SUR_NELEM; e++) lam[e] = inv[e][0] * r[0] + inv[e][1] * r[1] + inv[e][2] * r[2];
+#pragma unroll
+    for (int k = 0; k < NS; k++) {
+        double a = 0.0;
+#pragma unroll
+        for (int e = 0; e < SUR_NELEM; e++) a += c_sur_elem[e][k] * lam[e];
+        dY[k] -= (Y[k] + eps) * a;
+    }
+}
+
+// Chemistry increment of one cell over dt with the adaptive integrator: the
+// closed reactor at the cell's density, momentum and energy, then the
+// mass-fraction change projected to element conservation.  Tchem: the
+// temperature the integrator reached (a Newton start for the next decode).
+template <bool SPEC>
+__device__ __forceinline__ int chem_increment(const double cs0[NV], double T0, double Eold, unsigned qk, double dt,
+                                              const AdaptCfg &cfg, double proj_eps, double dY[NS], double &Tchem,
+                                              int &capped_any)
+{
+    double cs[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) cs[v] = cs0[v];
+    double T = T0;
+    const int n = chem_adaptive<SPEC>(cs, T, Eold, qk, dt, cfg, capped_any);
+    double D0 = 0.0, Dn = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        D0 += cs0[s];
+        Dn += cs[s];
+    }
+    double Y0[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Y0[s] = cs0[s] / D0;
+        dY[s] = cs[s] / Dn - Y0[s];
+    }
+    elem_project(Y0, dY, proj_eps);
+    Tchem = T;
+    return n;
 }
 
 enum CellMode {
@@ -365,7 +497,8 @@ enum CellMode {
     M_RK_STAGE1 = 5,
     M_RK_STAGE2 = 6,
     M_NOCHEM = 7,
-    M_TRAP1_PREDICT = 8
+    M_TRAP1_PREDICT = 8,
+    M_ADAPT = 9
 };
 
 // Work queue of the adaptive trapezoid: cells binned by floor(log2 Nchem),
@@ -389,7 +522,9 @@ struct CellArgs {
     const double *xn, *yn;
     double wedge[3];
     int wedge_on;
-    int *qbins;  // work-queue bin counts (M_TRAP1_PREDICT)
+    int *qbins;       // work-queue bin counts (M_TRAP1_PREDICT)
+    AdaptCfg acfg;    // adaptive chemistry (M_ADAPT)
+    double proj_eps;  // weight floor of its element projection
 };
 
 __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
@@ -442,6 +577,24 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         }
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
+    } else if (MODE == M_ADAPT) {
+        // chemistry increment of the closed reactor at the previous decode's
+        // state (adaptive integrator, element-projected), added with the
+        // flux residual
+        double dY[NS], Tc;
+        const int nsub = chem_increment<SPEC>(cs, T, Eold, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped_any);
+        double D0 = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) D0 += cs[s];
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+            double r = a.rhs[v * fs + c];
+            if (v < NS) r += D0 * dY[v];
+            cs[v] = cs[v] + r;
+        }
+        decode(cs, Tc, Eold, qk, o, capped);
+        capped_any |= capped;
+        warp_sum(&a.st->substeps, (unsigned long long)nsub);
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;

@@ -77,6 +77,9 @@ struct eu3d_handle {
     int flux_kz = 16;   // z planes walked by one flux block
     int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
     int queue_blocks = 3;  // resident queue blocks per SM
+    AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
+    double proj_eps = 1e-4;
+    bool elements = false;  // element matrix loaded (eu3d_set_elements)
     int *qlist = nullptr, *qbins = nullptr;
     std::map<StepKey, cudaGraphExec_t> graphs;
     // per-kernel CUDA-event timing (eu3d_profile_enable)
@@ -156,6 +159,8 @@ CellArgs cell_args(eu3d_handle *h)
     a.wedge[2] = h->wedge[2];
     a.wedge_on = h->wedge_on;
     a.qbins = h->qbins;
+    a.acfg = h->acfg;
+    a.proj_eps = h->proj_eps;
     return a;
 }
 
@@ -167,8 +172,9 @@ void launch_cell_t(eu3d_handle *h, int mode)
     CellArgs a = cell_args(h);
     P *q = (P *)h->prim;
     dim3 g = cell_grid(h->L, 128);
-    static const char *names[] = {"cell_decode", "cell_adv", "cell_imex", "cell_trap0", "cell_trap1", "cell_rk1",
-                                  "cell_rk2", "cell_nochem"};
+    static const char *names[] = {"cell_decode", "cell_adv",   "cell_imex",          "cell_trap0", "cell_trap1",
+                                  "cell_rk1",    "cell_rk2",   "cell_nochem",        "cell_trap1_predict",
+                                  "cell_adapt"};
     ProfScope ps(h, names[mode]);
     switch (mode) {
     case M_DECODE: k_cell<P, M_DECODE, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
@@ -179,6 +185,7 @@ void launch_cell_t(eu3d_handle *h, int mode)
     case M_RK_STAGE1: k_cell<P, M_RK_STAGE1, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     case M_RK_STAGE2: k_cell<P, M_RK_STAGE2, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     case M_NOCHEM: k_cell<P, M_NOCHEM, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_ADAPT: k_cell<P, M_ADAPT, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     }
 }
 
@@ -588,6 +595,7 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
         // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
         return cell_op(h, M_NOCHEM);
     case EU3D_REACT_SURROGATE: return sur_chem_op(h);
+    case EU3D_REACT_ADAPTIVE: return cell_op(h, M_ADAPT);
     default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
     }
 }
@@ -994,8 +1002,10 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
     if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "unknown time scheme");
     if (s->diff != EU3D_DIFF_MUSCL1 && s->diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
     if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE &&
-        s->react != EU3D_REACT_SURROGATE)
+        s->react != EU3D_REACT_SURROGATE && s->react != EU3D_REACT_ADAPTIVE)
         return fail(EU3D_ERR_ARG, "unsupported reaction scheme");
+    if (s->react == EU3D_REACT_ADAPTIVE && !h->elements)
+        return fail(EU3D_ERR_STATE, "element composition not set (eu3d_set_elements)");
     if (s->react == EU3D_REACT_SURROGATE && !h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached");
     if (s->react == EU3D_REACT_SURROGATE && s->timeadv == EU3D_ADV_SSPRK2)
         return fail(EU3D_ERR_ARG, "the surrogate step follows the EE update");
@@ -1134,6 +1144,39 @@ int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, 
     return EU3D_OK;
 }
 
+int eu3d_set_elements(eu3d_handle *h, const double *atoms)
+{
+    if (!h || !atoms) return fail(EU3D_ERR_ARG, "null argument");
+    CK(cudaSetDevice(h->dev));
+    double A[SUR_NELEM][NS];
+    for (int e = 0; e < SUR_NELEM; e++)
+        for (int k = 0; k < NS; k++) {
+            if (!(atoms[e * NS + k] >= 0)) return fail(EU3D_ERR_ARG, "atom counts must be >= 0");
+            A[e][k] = atoms[e * NS + k] / g_mech_loaded[0].mw[k];
+        }
+    CK(cudaMemcpyToSymbol(c_sur_elem, A, sizeof(A)));
+    h->elements = true;
+    return EU3D_OK;
+}
+
+int eu3d_set_adaptive(eu3d_handle *h, double rel, double amp, int nmax)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (!(rel > 0 && rel <= 1) || !(amp > 0 && amp < 1) || nmax < 1 || nmax > NCHEM_CAP)
+        return fail(EU3D_ERR_ARG, "adaptive chemistry: 0 < rel <= 1, 0 < amp < 1, 1 <= nmax <= 2^20");
+    h->acfg = AdaptCfg{rel, amp, nmax};
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    return EU3D_OK;
+}
+
+int eu3d_react_adaptive(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (!h->elements) return fail(EU3D_ERR_STATE, "element composition not set (eu3d_set_elements)");
+    return cell_op(h, M_ADAPT);
+}
+
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
 {
     if (!h || !t) return fail(EU3D_ERR_ARG, "null argument");
@@ -1259,6 +1302,7 @@ int eu3d_get_status(eu3d_handle *h, eu3d_status *o)
     double mx;
     memcpy(&mx, &s.audit_max_dT_bits, sizeof(double));
     o->surrogate_audit_max_dT = mx;
+    for (int r = 0; r < 4; r++) o->surrogate_rejects[r] = (long long)s.sur_reject[r];
     o->dt = sc[0];
     o->time = sc[1];
     return EU3D_OK;

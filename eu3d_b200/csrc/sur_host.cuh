@@ -12,6 +12,7 @@ struct eu3d_surrogate {
     cudaStream_t st = nullptr;
     unsigned quirks = 0;
     bool spec = false;
+    AdaptCfg acfg{0.02, 0.5, 4096};  // adaptive labels (nmax: the label call's cap)
     long long cap = 0, n = 0;
     double *states = nullptr;
     float *X = nullptr, *Lb = nullptr;
@@ -272,14 +273,9 @@ int eu3d_sur_create(eu3d_handle *h, long long capacity, const double *atoms, eu3
     CK(cudaSetDevice(h->dev));
     int rc;
     if ((rc = sur_set_attrs())) return rc;
-    double A[SUR_NELEM][NS];
-    for (int e = 0; e < SUR_NELEM; e++)
-        for (int k = 0; k < NS; k++) {
-            if (!(atoms[e * NS + k] >= 0)) return fail(EU3D_ERR_ARG, "atom counts must be >= 0");
-            A[e][k] = atoms[e * NS + k] / g_mech_loaded[0].mw[k];
-        }
-    CK(cudaMemcpyToSymbol(c_sur_elem, A, sizeof(A)));
+    if ((rc = eu3d_set_elements(h, atoms))) return rc;
     eu3d_surrogate *s = new eu3d_surrogate();
+    s->acfg = h->acfg;
     s->dev = h->dev;
     s->quirks = h->quirks;
     s->spec = h->spec;
@@ -382,18 +378,22 @@ int eu3d_sur_add_snapshot(eu3d_surrogate *s, eu3d_handle *src, long long n, long
 int eu3d_sur_label(eu3d_surrogate *s, int kind, int cap, double proj_eps, long long *n_valid)
 {
     if (!s) return fail(EU3D_ERR_ARG, "null surrogate");
-    if (kind != EU3D_REACT_IMEX && kind != EU3D_REACT_TRAPEZOID)
-        return fail(EU3D_ERR_ARG, "label integrator must be EU3D_REACT_IMEX or EU3D_REACT_TRAPEZOID");
+    if (kind != EU3D_REACT_IMEX && kind != EU3D_REACT_TRAPEZOID && kind != EU3D_REACT_ADAPTIVE)
+        return fail(EU3D_ERR_ARG, "label integrator must be EU3D_REACT_ADAPTIVE, _IMEX or _TRAPEZOID");
     if (cap < 1 || cap > NCHEM_CAP) return fail(EU3D_ERR_ARG, "substep cap out of range");
     if (!(proj_eps > 0)) return fail(EU3D_ERR_ARG, "projection weight floor must be > 0");
     CK(cudaSetDevice(s->dev));
-    const int k = kind == EU3D_REACT_IMEX ? SUR_LABEL_IMEX : SUR_LABEL_TRAPEZOID;
+    const int k = kind == EU3D_REACT_IMEX       ? SUR_LABEL_IMEX
+                  : kind == EU3D_REACT_ADAPTIVE ? SUR_LABEL_ADAPTIVE
+                                                : SUR_LABEL_TRAPEZOID;
     if (s->n > 0) {
         const unsigned nb = (unsigned)((s->n + 127) / 128);
         if (s->spec)
-            k_sur_label<true><<<nb, 128, 0, s->st>>>(s->states, s->n, k, s->quirks, cap, proj_eps, s->X, s->Lb);
+            k_sur_label<true><<<nb, 128, 0, s->st>>>(s->states, s->n, k, s->quirks, cap, proj_eps, s->acfg, s->X,
+                                                     s->Lb);
         else
-            k_sur_label<false><<<nb, 128, 0, s->st>>>(s->states, s->n, k, s->quirks, cap, proj_eps, s->X, s->Lb);
+            k_sur_label<false><<<nb, 128, 0, s->st>>>(s->states, s->n, k, s->quirks, cap, proj_eps, s->acfg, s->X,
+                                                      s->Lb);
     }
     CK(cudaGetLastError());
     if (n_valid) {
@@ -601,6 +601,7 @@ int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride)
     }
     h->sur = s;
     h->sur_audit_stride = audit_stride;
+    if (s) h->elements = true;  // eu3d_sur_create loaded the element matrix on this device
     // recorded step graphs hold the previous surrogate's buffers and settings
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();

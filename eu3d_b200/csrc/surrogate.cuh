@@ -2,7 +2,8 @@
 // project's own integrators, the fused tensor-core MLP inference kernel and
 // the per-cell apply step (conservation projection, envelope and residual
 // checks, fallback list), plus the persistent fallback queue that runs the
-// FP64 IMEX integrator on the cells the surrogate rejects.
+// FP64 adaptive integrator (the network's teacher) on the cells the surrogate
+// rejects.
 //
 // Sample record (states, FP64, 12 per sample): T [K], p [Pa], Y_0..Y_8, dt [s].
 // Raw features (FP32, 12): T, ln(p / 1 atm), ln(Y_0 + 1e-12)..ln(Y_8 + 1e-12), ln dt.
@@ -10,9 +11,11 @@
 // constant-density, constant-energy reactor, projected to element
 // conservation), dT [K], weight (0 = unusable sample), label substeps.
 //
-// Targets: x_k = label_k / (dt A(T)), A(T) = exp(Ta (1/Tr - 1/T)) an
-// Arrhenius activity that vanishes in cold gas; y_k = asinh(x_k / lin_k),
-// standardised with out_mean / out_std.  Inference inverts the chain.
+// Targets: x_k = label_k / s_k with s_k = dt A(T) (Y_k + delta) for species
+// and dt A(T) T for dT (relative rates; with delta = 0 the plain dt A(T)),
+// A(T) = exp(Ta (1/Tr - 1/T)) an optional Arrhenius activity (Ta = 0: 1);
+// y_k = asinh(x_k / lin_k), standardised with out_mean / out_std.  Inference
+// inverts the chain.
 #pragma once
 
 #include "cell.cuh"
@@ -27,15 +30,11 @@ namespace eu3d {
 
 constexpr int SN_IN_MEAN = 0, SN_IN_STD = 12, SN_OUT_MEAN = 24, SN_OUT_STD = 34, SN_LIN = 44, SN_TA = 54, SN_TR = 55,
               SN_ENV = 56, SN_RATIO = 62, SN_RATIO_TOL = 64, SN_RES_ABS = 65, SN_RES_REL = 66, SN_NEG_TOL = 67,
-              SN_PROJ_EPS = 68, SN_DT_MAX = 69;
+              SN_PROJ_EPS = 68, SN_DT_MAX = 69, SN_DELTA = 70;
 
 struct SurNorm {
     float v[EU3D_SUR_NORM_LEN];
 };
-
-constexpr int SUR_NELEM = 3;  // H, O, N
-// element matrix: atoms of element e per unit mass of species k (atoms / W_k)
-__constant__ double c_sur_elem[SUR_NELEM][NS];
 
 constexpr double ATM_PA = 101325.0;
 constexpr float SUR_YFLOOR = 1e-12f;  // mass-fraction floor of the log inputs
@@ -56,50 +55,7 @@ __device__ __forceinline__ double urand(unsigned long long seed, unsigned long l
 }
 
 // ------------------------------------------------------ projection, energy
-// Weighted least-change projection of dY onto element conservation:
-// minimise sum_k (dY'_k - dY_k)^2 / w_k subject to sum_k A_ek dY'_k = 0,
-// w_k = Y_k + eps, so that scarce species take small corrections.
-__device__ __forceinline__ void sur_project(const double Y[NS], double dY[NS], double eps)
-{
-    double r[SUR_NELEM], M[SUR_NELEM][SUR_NELEM];
-#pragma unroll
-    for (int e = 0; e < SUR_NELEM; e++) {
-        double a = 0.0;
-#pragma unroll
-        for (int k = 0; k < NS; k++) a += c_sur_elem[e][k] * dY[k];
-        r[e] = a;
-#pragma unroll
-        for (int f = 0; f < SUR_NELEM; f++) {
-            double m = 0.0;
-#pragma unroll
-            for (int k = 0; k < NS; k++) m += c_sur_elem[e][k] * (Y[k] + eps) * c_sur_elem[f][k];
-            M[e][f] = m;
-        }
-    }
-    // 3x3 solve by cofactors
-    const double c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
-    const double c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
-    const double c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
-    const double det = M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02;
-    if (!(fabs(det) > 0.0)) return;
-    const double id = 1.0 / det;
-    const double inv[3][3] = {{c00 * id, (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id,
-                               (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id},
-                              {c01 * id, (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id,
-                               (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id},
-                              {c02 * id, (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id,
-                               (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id}};
-    double lam[SUR_NELEM];
-#pragma unroll
-    for (int e = 0; e < SUR_NELEM; e++) lam[e] = inv[e][0] * r[0] + inv[e][1] * r[1] + inv[e][2] * r[2];
-#pragma unroll
-    for (int k = 0; k < NS; k++) {
-        double a = 0.0;
-#pragma unroll
-        for (int e = 0; e < SUR_NELEM; e++) a += c_sur_elem[e][k] * lam[e];
-        dY[k] -= (Y[k] + eps) * a;
-    }
-}
+__device__ __forceinline__ void sur_project(const double Y[NS], double dY[NS], double eps) { elem_project(Y, dY, eps); }
 
 // internal energy e(T) [J/kg] and cv [J/kg/K] of the mixture Y, with the
 // arithmetic of the decode (mixture polynomial, kJ -> J)
@@ -219,18 +175,19 @@ __global__ void k_sur_snapshot(double *__restrict__ states, long long base, long
 }
 
 // ------------------------------------------------------------------ labels
-enum { SUR_LABEL_IMEX = 1, SUR_LABEL_TRAPEZOID = 0 };
+enum { SUR_LABEL_IMEX = 1, SUR_LABEL_TRAPEZOID = 0, SUR_LABEL_ADAPTIVE = 4 };
 
 // Closed-reactor chemistry of one sample in FP64 with the project's
 // integrators, then the element projection and the decode at constant
 // density and internal energy.  kind SUR_LABEL_IMEX: one Diagonalized +
 // Update_IMEX step with zero flux residual (the integrator the coupled run
 // falls back to); SUR_LABEL_TRAPEZOID: TrapezoidPrediction substeps of the
-// point-implicit trapezoid (capped at cap substeps).
+// point-implicit trapezoid (capped at cap substeps); SUR_LABEL_ADAPTIVE: the
+// adaptive species-implicit integrator (chem_adaptive, at most cap substeps).
 template <bool SPEC>
 __global__ void __launch_bounds__(128, 3)
     k_sur_label(const double *__restrict__ states, long long n, int kind, unsigned q, int cap, double proj_eps,
-                float *__restrict__ X, float *__restrict__ Lb)
+                AdaptCfg acfg, float *__restrict__ X, float *__restrict__ Lb)
 {
     const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (m >= n) return;
@@ -253,7 +210,15 @@ __global__ void __launch_bounds__(128, 3)
     Decoded o;
     int capped = 0, bad = 0, nsub = 1;
     double Tg = T0;
-    if (kind == SUR_LABEL_IMEX) {
+    double dY[NS];
+    bool projected = false;
+    if (kind == SUR_LABEL_ADAPTIVE) {
+        int cp = 0;
+        acfg.nmax = cap;
+        nsub = chem_increment<SPEC>(cs, T0, E0, q, dt, acfg, proj_eps, dY, Tg, cp);
+        bad |= cp;
+        projected = true;
+    } else if (kind == SUR_LABEL_IMEX) {
         double CMS[NS], MD[NS];
         imex_source<SPEC>(cs, T0, q, CMS, MD);
 #pragma unroll
@@ -285,13 +250,14 @@ __global__ void __launch_bounds__(128, 3)
         }
         Tg = o.T;
     }
-    double Dn = 0.0;
+    if (!projected) {
+        double Dn = 0.0;
 #pragma unroll
-    for (int s = 0; s < NS; s++) Dn += cs[s];
-    double dY[NS];
+        for (int s = 0; s < NS; s++) Dn += cs[s];
 #pragma unroll
-    for (int s = 0; s < NS; s++) dY[s] = cs[s] / Dn - Y0[s];
-    sur_project(Y0, dY, proj_eps);
+        for (int s = 0; s < NS; s++) dY[s] = cs[s] / Dn - Y0[s];
+        sur_project(Y0, dY, proj_eps);
+    }
     // decode of the projected composition at (D0, E0)
     double cp[NV];
 #pragma unroll
@@ -356,11 +322,13 @@ __global__ void k_sur_batch(const float *__restrict__ X, const float *__restrict
     for (int i = 0; i < SUR_IN; i++) Xb[(long long)r * SUR_IN + i] = f[i];
     const double T = raw[0], dt = exp((double)raw[11]);
     const double sc = dt * sur_activity(nrm, T);
+    const double delta = nrm.v[SN_DELTA];
     const float *l = Lb + idx * 12;
     float *y = Yb + (long long)r * SUR_OUT;
 #pragma unroll
     for (int k = 0; k < SUR_NOUT; k++) {
-        const double x = (double)l[k] / sc;
+        const double rel = delta > 0 ? (k < NS ? exp((double)raw[2 + k]) - (double)SUR_YFLOOR + delta : T) : 1.0;
+        const double x = (double)l[k] / (sc * rel);
         const double t = asinh(x / (double)nrm.v[SN_LIN + k]);
         y[k] = (float)((t - nrm.v[SN_OUT_MEAN + k]) / nrm.v[SN_OUT_STD + k]);
     }
@@ -684,6 +652,7 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
     const float lnp = logf((float)(p * (1.0 / ATM_PA))), lndt = logf((float)dt);
     bool ok = Tf >= n.v[SN_ENV + 0] && Tf <= n.v[SN_ENV + 1] && lnp >= n.v[SN_ENV + 2] && lnp <= n.v[SN_ENV + 3] &&
               lndt >= n.v[SN_ENV + 4] && lndt <= n.v[SN_ENV + 5];
+    bool ok_env;
     {
         double el[SUR_NELEM];
 #pragma unroll
@@ -696,12 +665,15 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
         const double tol = n.v[SN_RATIO_TOL];
         ok = ok && fabs(el[0] / (el[1] * n.v[SN_RATIO + 0]) - 1.0) <= tol &&
              fabs(el[2] / (el[1] * n.v[SN_RATIO + 1]) - 1.0) <= tol;
+        ok_env = ok;
     }
     const float sc = (float)dt * expf(n.v[SN_TA] * (1.f / n.v[SN_TR] - 1.f / Tf));
+    const float delta = n.v[SN_DELTA];
     double dY[NS];
 #pragma unroll
-    for (int sp = 0; sp < NS; sp++) dY[sp] = (double)sur_unscale_f(n, sp, s.out[sp * s.n + idx], sc);
-    const double dTn = (double)sur_unscale_f(n, NS, s.out[NS * s.n + idx], sc);
+    for (int sp = 0; sp < NS; sp++)
+        dY[sp] = (double)sur_unscale_f(n, sp, s.out[sp * s.n + idx], delta > 0.f ? sc * ((float)Y[sp] + delta) : sc);
+    const double dTn = (double)sur_unscale_f(n, NS, s.out[NS * s.n + idx], delta > 0.f ? sc * Tf : sc);
     sur_project(Y, dY, n.v[SN_PROJ_EPS]);
     double Yn[NS];
 #pragma unroll
@@ -711,6 +683,7 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
         Yn[sp] = fmax(y, 0.0);
     }
     ok = ok && isfinite(dTn) && fabs(dTn) <= n.v[SN_DT_MAX];
+    const bool ok_out = ok;
     double Tg = T + dTn;
     if (ok) {
         // energy balance at the predicted temperature (constant density and energy)
@@ -719,6 +692,7 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
         const double res = (e - Eold) / cv;
         ok = fabs(res) <= n.v[SN_RES_ABS] + n.v[SN_RES_REL] * fabs(dTn);
     }
+    const bool ok_res = ok;
     Decoded o;
     int capped = 0;
     if (ok) {
@@ -746,13 +720,17 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
     sur_push(s.qu, !ok || audit, (int)c | (audit ? (int)0x80000000u : 0), audit ? o.T : 0.0);
     warp_count(&a.st->sur_cells, ok && !audit);
     warp_count(&a.st->sur_fallback, !ok);
+    warp_count(&a.st->sur_reject[0], !ok_env);
+    warp_count(&a.st->sur_reject[1], ok_env && !ok_out);
+    warp_count(&a.st->sur_reject[2], ok_out && !ok_res);
+    warp_count(&a.st->sur_reject[3], ok_res && !ok);
 }
 
 // Persistent fallback queue: warps pull 32 listed cells at a time from a
-// global cursor and run the FP64 IMEX update of Euler::IMEX on each
-// (Diagonalized + Update_IMEX + decode).  For audited cells the surrogate's
-// temperature is compared with the integrator's and the largest difference
-// recorded.
+// global cursor and run the FP64 adaptive integrator the network was trained
+// on (chem_increment, the M_ADAPT cell update) on each.  For audited cells the
+// surrogate's temperature is compared with the integrator's and the largest
+// difference recorded.
 template <class P, bool SPEC>
 __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restrict__ q, SurQueue qu)
 {
@@ -774,21 +752,21 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
             double cs[NV];
             load_cs(a.cs, fs, c, cs);
             const double T = a.T[c], Eold = a.E[c];
-            double CMS[NS], MD[NS];
-            imex_source<SPEC>(cs, T, qk, CMS, MD);
+            double dY[NS], Tc;
+            int capped = 0;
+            const int nsub = chem_increment<SPEC>(cs, T, Eold, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped);
+            double D0 = 0.0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) D0 += cs[s];
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 double r = a.rhs[v * fs + c];
-                if (v < NS) {
-                    r = r + CMS[v] * dt;
-                    cs[v] = cs[v] + r / (1.0 - dt * MD[v]);
-                } else {
-                    cs[v] = cs[v] + r;
-                }
+                if (v < NS) r += D0 * dY[v];
+                cs[v] = cs[v] + r;
             }
             Decoded o;
-            int capped = 0;
-            decode(cs, T, Eold, qk, o, capped);
+            decode(cs, Tc, Eold, qk, o, capped);
+            atomicAdd(&a.st->substeps, (unsigned long long)nsub);
             store_cs(a.cs, fs, c, cs);
             a.T[c] = o.T;
             a.E[c] = o.E;

@@ -22,7 +22,7 @@ _dp = C.POINTER(C.c_double)
 QUIRKS_REF = 0x1FF
 QUIRKS_FIXED = 0x000
 BC_RSBI, BC_ODM, BC_TRANSMISSIVE, BC_NONE = 0, 1, 2, 3
-REACT_TRAPEZOID, REACT_IMEX, REACT_NONE, REACT_SURROGATE = 0, 1, 2, 3
+REACT_TRAPEZOID, REACT_IMEX, REACT_NONE, REACT_SURROGATE, REACT_ADAPTIVE = 0, 1, 2, 3, 4
 DIFF_MUSCL1, DIFF_MUSCL2 = 0, 1
 ADV_EE, ADV_TVD_RK3, ADV_SSPRK2 = 0, 1, 2
 
@@ -39,7 +39,8 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_sur_dataset_size", "eu3d_sur_add_random", "eu3d_sur_add_snapshot", "eu3d_sur_label",
            "eu3d_sur_get_dataset", "eu3d_sur_set_norm", "eu3d_sur_get_norm", "eu3d_sur_set_params",
            "eu3d_sur_get_params", "eu3d_sur_train", "eu3d_sur_loss_grad", "eu3d_sur_predict", "eu3d_sur_infer",
-           "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune"]
+           "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune",
+           "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive"]
 
 SUR_NPARAM = 37264
 SUR_NORM_LEN = 80
@@ -66,10 +67,13 @@ class Status(C.Structure):
     _fields_ = [("nonfinite_cells", C.c_longlong), ("newton_capped", C.c_longlong), ("substeps", C.c_longlong),
                 ("nchem_max", C.c_int), ("substep_capped", C.c_int), ("surrogate_cells", C.c_longlong),
                 ("surrogate_fallback", C.c_longlong), ("dt", C.c_double), ("time", C.c_double),
-                ("surrogate_audited", C.c_longlong), ("surrogate_audit_max_dT", C.c_double)]
+                ("surrogate_audited", C.c_longlong), ("surrogate_audit_max_dT", C.c_double),
+                ("surrogate_rejects", C.c_longlong * 4)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["surrogate_rejects"] = list(d["surrogate_rejects"])
+        return d
 
 
 class Tuning(C.Structure):
@@ -139,6 +143,9 @@ def load_library(path: Optional[str] = None):
     L.eu3d_sur_infer.argtypes = h + [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
     L.eu3d_set_surrogate.argtypes = h + [C.c_void_p, C.c_int]
     L.eu3d_react_surrogate.argtypes = h
+    L.eu3d_set_elements.argtypes = h + [_dp]
+    L.eu3d_set_adaptive.argtypes = h + [C.c_double, C.c_double, C.c_int]
+    L.eu3d_react_adaptive.argtypes = h
     L.eu3d_set_tuning.argtypes = h + [C.POINTER(Tuning)]
     L.eu3d_get_tuning.argtypes = h + [C.POINTER(Tuning)]
     L.eu3d_autotune.argtypes = h + [C.POINTER(StepDesc), C.c_int, C.POINTER(Tuning), _dp]
@@ -274,6 +281,19 @@ class DeviceFlowfield:
 
     def trapezoid(self, type_: int):
         _check(self.L.eu3d_react_trapezoid(self.h, type_))
+
+    def set_elements(self, atoms):
+        """(3, NS) H, O, N atom counts per species (adaptive chemistry, surrogate)."""
+        a = np.ascontiguousarray(atoms, dtype=np.float64)
+        if a.shape != (3, self.NS):
+            raise Eu3dError("atoms must be (3, NS)")
+        _check(self.L.eu3d_set_elements(self.h, a.ctypes.data_as(_dp)))
+
+    def set_adaptive(self, rel: float = 0.02, amp: float = 0.5, nmax: int = 1024):
+        _check(self.L.eu3d_set_adaptive(self.h, rel, amp, nmax))
+
+    def react_adaptive(self):
+        _check(self.L.eu3d_react_adaptive(self.h))
 
     def set_surrogate(self, sur, audit_stride: int = 0):
         """Use a trained DeviceSurrogate (None: none) for REACT_SURROGATE steps."""

@@ -9,11 +9,13 @@ accumulation.  Inputs: T, ln(p/atm), ln(Y_k + 1e-12), ln dt (standardised;
 three spare input columns carry BF16 rounding residuals of T, ln p, ln dt).
 Outputs: the chemistry increment over dt of a closed constant-density,
 constant-energy reactor, dY_k and dT, as labelled by the project's FP64
-integrator (one Diagonalized + Update_IMEX step of the reference's
-Euler::IMEX, src/Reaction.cpp:736-811 and src/Flowfield.cpp:1215-1234, or the
-TrapezoidPrediction substeps of src/Reaction.cpp:489-670), projected to
-element conservation.  Targets are scaled by dt A(T), A(T) = exp(Ta (1/Tr -
-1/T)), compressed with asinh(x / lin_k) and standardised.
+adaptive integrator (substeps of the species-diagonal implicit update built
+on Reaction::Diagonalized, src/Reaction.cpp:736-811; the reference's one-step
+IMEX, src/Flowfield.cpp:1215-1234, and the TrapezoidPrediction substeps,
+src/Reaction.cpp:489-670, are also available as labels), projected to element
+conservation.  Targets are relative rates dY_k / ((Y_k + delta) dt) and
+dT / (T dt) (optionally times an Arrhenius activity A(T) = exp(Ta (1/Tr -
+1/T))), compressed with asinh(x / lin_k) and standardised.
 """
 from __future__ import annotations
 
@@ -43,8 +45,9 @@ assert _o == NPARAM
 
 # offsets of the normalisation vector (include/eu3d_gpu.h EU3D_SUR_N_*)
 N_IN_MEAN, N_IN_STD, N_OUT_MEAN, N_OUT_STD, N_LIN = 0, 12, 24, 34, 44
-N_TA, N_TR, N_ENV, N_RATIO, N_RATIO_TOL, N_RES_ABS, N_RES_REL, N_NEG_TOL, N_PROJ_EPS, N_DT_MAX = \
-    54, 55, 56, 62, 64, 65, 66, 67, 68, 69
+N_TA, N_TR, N_ENV, N_RATIO, N_RATIO_TOL, N_RES_ABS, N_RES_REL, N_NEG_TOL, N_PROJ_EPS, N_DT_MAX, N_DELTA = \
+    54, 55, 56, 62, 64, 65, 66, 67, 68, 69, 70
+Y_FLOOR = 1e-12  # mass-fraction floor of the log inputs
 
 RADICAL_ORDER = ("H", "O", "H2O", "OH", "O2", "H2", "H2O2", "HO2", "N2")
 ELEMENTS = ("H", "O", "N")
@@ -75,7 +78,7 @@ def element_ratios(mech, Y) -> np.ndarray:
 
 
 def activity(T, Ta, Tr):
-    return np.exp(Ta * (1.0 / Tr - 1.0 / np.asarray(T, dtype=np.float64)))
+    return np.exp(float(Ta) * (1.0 / float(Tr) - 1.0 / np.asarray(T, dtype=np.float64)))
 
 
 def bf16_round(x):
@@ -96,11 +99,23 @@ def features(X, norm) -> np.ndarray:
     return f
 
 
+def label_scale(X, norm) -> np.ndarray:
+    """Per-output scale s_k (n, 10) of the raw labels: dt A(T) (Y_k + delta)
+    for species and dt A(T) T for dT (delta > 0), else dt A(T)."""
+    X = np.asarray(X, dtype=np.float64)
+    sc = np.exp(X[:, 11]) * activity(X[:, 0], norm[N_TA], norm[N_TR])
+    s = np.repeat(sc[:, None], N_OUT, axis=1)
+    delta = float(norm[N_DELTA])
+    if delta > 0:
+        s[:, :9] *= np.exp(X[:, 2:11]) - Y_FLOOR + delta
+        s[:, 9] *= X[:, 0]
+    return s
+
+
 def targets(X, Lb, norm) -> np.ndarray:
     """Standardised targets (n, 16) of raw labels Lb (n, 12); column 15 = weight."""
     X = np.asarray(X, dtype=np.float64)
-    sc = np.exp(X[:, 11]) * activity(X[:, 0], norm[N_TA], norm[N_TR])
-    x = np.asarray(Lb[:, :N_OUT], dtype=np.float64) / sc[:, None]
+    x = np.asarray(Lb[:, :N_OUT], dtype=np.float64) / label_scale(X, norm)
     y = np.arcsinh(x / norm[N_LIN:N_LIN + N_OUT])
     t = np.zeros((X.shape[0], OUT_PAD), np.float32)
     t[:, :N_OUT] = (y - norm[N_OUT_MEAN:N_OUT_MEAN + N_OUT]) / norm[N_OUT_STD:N_OUT_STD + N_OUT]
@@ -110,23 +125,22 @@ def targets(X, Lb, norm) -> np.ndarray:
 
 def unscale(out, X, norm) -> np.ndarray:
     """Raw labels (n, 10) from network outputs (n, >=10)."""
-    X = np.asarray(X, dtype=np.float64)
-    sc = np.exp(X[:, 11]) * activity(X[:, 0], norm[N_TA], norm[N_TR])
     y = np.asarray(out[:, :N_OUT], np.float64) * norm[N_OUT_STD:N_OUT_STD + N_OUT] + norm[N_OUT_MEAN:N_OUT_MEAN + N_OUT]
-    return sc[:, None] * norm[N_LIN:N_LIN + N_OUT] * np.sinh(y)
+    return label_scale(X, norm) * norm[N_LIN:N_LIN + N_OUT] * np.sinh(y)
 
 
-def make_norm(mech, X, Lb, Ta=8000.0, Tr=1500.0, env=None, ratio_tol=0.02, res_abs=5.0, res_rel=0.05,
-              neg_tol=1e-6, proj_eps=1e-4, lin_quantile=0.01, dT_max=2500.0) -> np.ndarray:
+def make_norm(mech, X, Lb, Ta=0.0, Tr=1500.0, env=None, ratio_tol=0.02, res_abs=5.0, res_rel=0.05,
+              neg_tol=1e-6, proj_eps=1e-4, lin_quantile=0.5, dT_max=2500.0, delta=1e-10) -> np.ndarray:
     """Normalisation and acceptance vector from (a sample of) the raw set."""
     ok = Lb[:, 10] > 0
     Xv, Lv = np.asarray(X[ok], np.float64), np.asarray(Lb[ok], np.float64)
     n = np.zeros(NORM_LEN, np.float32)
     n[N_IN_MEAN:N_IN_MEAN + N_IN] = Xv.mean(axis=0)
-    n[N_IN_STD:N_IN_STD + N_IN] = np.maximum(Xv.std(axis=0), 1e-6)
-    n[N_TA], n[N_TR] = Ta, Tr
-    sc = np.exp(Xv[:, 11]) * activity(Xv[:, 0], Ta, Tr)
-    x = Lv[:, :N_OUT] / sc[:, None]
+    # a floor keeps a feature that is constant in the set from amplifying
+    # small deviations into huge network inputs
+    n[N_IN_STD:N_IN_STD + N_IN] = np.maximum(Xv.std(axis=0), 0.01)
+    n[N_TA], n[N_TR], n[N_DELTA] = Ta, Tr, delta
+    x = Lv[:, :N_OUT] / label_scale(Xv, n)
     lin = np.empty(N_OUT)
     for k in range(N_OUT):
         a = np.abs(x[:, k])
@@ -195,10 +209,10 @@ class SurrogateModel:
 # ----------------------------------------------------------- training set
 @dataclasses.dataclass
 class Recipe:
-    """Training-set and optimiser settings.  Defaults: 2^22 states, half from
+    """Training-set and optimiser settings.  Defaults: 2^22 states, 70 % from
     flowfield snapshots (2D ODW at two resolutions and the 1D ZND, run with
-    the FP64 IMEX integrator), half uniform random states; labels from the
-    closed-reactor IMEX step."""
+    the FP64 adaptive integrator) with jitter on T, p and dt, 30 % uniform
+    random states; labels from the adaptive integrator."""
 
     n_total: int = 1 << 22
     frac_random: float = 0.3
@@ -212,20 +226,21 @@ class Recipe:
     znd_ni: int = 4000
     znd_steps: int = 1500
     snapshots_per_run: int = 8
-    label_kind: int = gpu.REACT_IMEX
+    label_kind: int = gpu.REACT_ADAPTIVE
     label_cap: int = 4096
     steps: int = 20000
     batch: int = 8192
     lr_max: float = 2e-3
     lr_min: float = 2e-5
     warmup: int = 500
-    Ta: float = 8000.0
+    Ta: float = 0.0
     Tr: float = 1500.0
+    delta: float = 1e-10
     seed: int = 1234
 
 
 def _snapshot_runs(mech, recipe: Recipe, sur: gpu.DeviceSurrogate, n_snap: int, log=print):
-    """Run the config-2 style 2D ODW cases and the 1D ZND with the IMEX
+    """Run the config-2 style 2D ODW cases and the 1D ZND with the adaptive
     integrator and sample their interior cells every few steps."""
     runs = []
     for (ni, nj), ns in zip(recipe.odw_grids, recipe.odw_steps):
@@ -240,20 +255,22 @@ def _snapshot_runs(mech, recipe: Recipe, sur: gpu.DeviceSurrogate, n_snap: int, 
             case = odw_case(mech, ni, nj, 2, seed=seed)
             dev = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=32)
             setup_odw(dev, case)
+            dev.set_elements(atoms_matrix(mech))
             bc = gpu.BC_ODM
         else:
             g, st = znd_case(mech, ni)
             dev = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=32)
             upload_primitive_state(dev, st)
             dev.update_after_cs()
+            dev.set_elements(atoms_matrix(mech))
             bc = gpu.BC_TRANSMISSIVE
-        # config 1 (ZND) runs its own scheme: SSP-RK2 with the adaptive
-        # trapezoid; the ODW cases use the IMEX integrator
-        # (at CFL 0.5 the scheme itself goes non-finite in its first step at
-        # the driver interface: AUSM moves momentum, not energy, across a
-        # face whose two sides are at rest, so ZND runs at CFL 0.3)
-        scheme = (dict(react=gpu.REACT_IMEX, cfl=0.5) if kind == "odw" else
-                  dict(react=gpu.REACT_TRAPEZOID, type_=1, timeadv=gpu.ADV_SSPRK2, cfl=0.3))
+        # the reference's own integrators diverge through ignition, so every
+        # run uses the adaptive one; ZND keeps its SSP-RK2 time scheme and
+        # runs at CFL 0.3 (at 0.5 the scheme goes non-finite in its first
+        # step at the driver interface: AUSM moves momentum, not energy,
+        # across a face whose two sides are at rest)
+        scheme = (dict(react=gpu.REACT_ADAPTIVE, cfl=0.5) if kind == "odw" else
+                  dict(react=gpu.REACT_ADAPTIVE, timeadv=gpu.ADV_SSPRK2, cfl=0.3))
         ncell = dev.grid.ni * dev.grid.nj * dev.grid.nk
         k = recipe.snapshots_per_run
         chunk = nsteps // k
@@ -304,7 +321,7 @@ def train_model(mech, dev: gpu.DeviceFlowfield, recipe: Optional[Recipe] = None,
     env = (recipe.T_range[0], recipe.T_range[1], np.log(recipe.p_atm_range[0]), np.log(recipe.p_atm_range[1]),
            np.log(recipe.dt_range[0]), np.log(recipe.dt_range[1]))
     pick = rng.choice(n, size=min(n, 1 << 18), replace=False)
-    norm = make_norm(mech, X[pick], Lb[pick], recipe.Ta, recipe.Tr, env)
+    norm = make_norm(mech, X[pick], Lb[pick], recipe.Ta, recipe.Tr, env, delta=recipe.delta)
     sur.set_norm(norm)
     sur.set_params(init_params(recipe.seed))
     t0 = time.time()

@@ -94,6 +94,9 @@ typedef struct {
     double dt, time;             /* device copies of Flowfield::dt / ::time */
     long long surrogate_audited; /* surrogate cells re-run by the integrator to judge it */
     double surrogate_audit_max_dT; /* largest |T_surrogate - T_integrator| over audited cells [K] */
+    long long surrogate_rejects[4]; /* why cells fell back: outside the envelope, network output
+                                       (non-finite, |dT| too large, negative fraction), energy
+                                       residual, failed decode */
 } eu3d_status;
 
 const char *eu3d_last_error(void);
@@ -144,6 +147,20 @@ int eu3d_react_imex(eu3d_handle *h);
    or TrapezoidPrediction + per-cell substeps (type 1, :489-670) on the device
    work queue */
 int eu3d_react_trapezoid(eu3d_handle *h, int type);
+/* FP64 adaptive chemistry (new): the closed-reactor chemistry increment of
+   each cell over dt, integrated with species-diagonal implicit substeps (the
+   composition part of Reaction::Diagonalized's Jacobian, src/Reaction.cpp:
+   736-811) and a decode after each, projected to element conservation and
+   added with the flux residual.  Substep h: largest with h |CMS_s| <= rel
+   (rho_s + 1e-9 rho) for all s and h MD_s <= amp where MD_s > 0, at least
+   dt / nmax (defaults rel 0.02, amp 0.5, nmax 1024).  The reference's
+   one-step IMEX and adaptive trapezoid diverge through H2-air ignition at the
+   time steps of its detonation cases; this integrator does not, and it is
+   the learned surrogate's teacher and fallback.  Needs the element
+   composition: atoms (3, NS) = H, O, N atoms per species. */
+int eu3d_set_elements(eu3d_handle *h, const double *atoms);
+int eu3d_set_adaptive(eu3d_handle *h, double rel, double amp, int nmax);
+int eu3d_react_adaptive(eu3d_handle *h);
 /* One pass of Euler::Computing's loop body, src/Euler.cpp:266-333 (CFL, ghost
    fill, advection, chemistry), recorded once and replayed as a CUDA graph. */
 int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s);
@@ -230,7 +247,7 @@ int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, 
 #define EU3D_SUR_N_OUT_MEAN 24  /* 10 target means (asinh space) */
 #define EU3D_SUR_N_OUT_STD 34   /* 10 target scales */
 #define EU3D_SUR_N_LIN 44       /* 10 asinh linear scales */
-#define EU3D_SUR_N_TA 54        /* activity temperature Ta [K] */
+#define EU3D_SUR_N_TA 54        /* activity temperature Ta [K] (0: no activity scaling) */
 #define EU3D_SUR_N_TR 55        /* activity reference temperature Tr [K] */
 #define EU3D_SUR_N_ENV 56       /* envelope: T_lo, T_hi, lnp_lo, lnp_hi, lndt_lo, lndt_hi */
 #define EU3D_SUR_N_RATIO 62     /* element ratios H/O, N/O of the training set */
@@ -240,6 +257,7 @@ int eu3d_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, 
 #define EU3D_SUR_N_NEG_TOL 67   /* most negative mass fraction accepted (then clipped to 0) */
 #define EU3D_SUR_N_PROJ_EPS 68  /* weight floor of the element projection */
 #define EU3D_SUR_N_DT_MAX 69    /* largest |dT| accepted from the network [K] */
+#define EU3D_SUR_N_DELTA 70     /* > 0: relative targets dY_k / (Y_k + delta), dT / T; 0: absolute */
 
 /* Surrogate bound to h's device, quirk policy and mechanism; atoms: (3, NS)
    counts of H, O, N atoms per species; capacity: training samples. */

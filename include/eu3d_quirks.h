@@ -52,6 +52,7 @@
 #define EU3D_REACT_IMEX 1
 #define EU3D_REACT_NONE 2      /* "DNN"/"Cantera" in the reference: no chemistry */
 #define EU3D_REACT_SURROGATE 3 /* learned MLP substep with integrator fallback (new) */
+#define EU3D_REACT_ADAPTIVE 4  /* FP64 adaptive species-implicit substeps (new; the surrogate's teacher) */
 
 /* Spatial schemes (include/Global.hpp DIFF) */
 #define EU3D_DIFF_MUSCL1 0
