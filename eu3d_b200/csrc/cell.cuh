@@ -534,6 +534,49 @@ __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
     return x > a.wedge[0] && (y - a.wedge[1]) < (x - a.wedge[0]) * a.wedge[2];
 }
 
+// Split adaptive step of one cell: the flux residual (CS += RHS, then a
+// decode; skipped with with_rhs = false when it was applied already), the
+// closed-reactor chemistry over dt at that state with the adaptive
+// integrator, applied as CS_s = rho (Y_s + dY_s) with negatives clipped, and
+// a decode (o).  Returns the substeps taken.
+template <bool SPEC>
+__device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, double cs[NV], double T, double Eold,
+                                                bool with_rhs, Decoded &o, int &capped_any)
+{
+    const long long fs = a.L.fs;
+    const unsigned qk = a.quirks;
+    const double dt = a.scal[0];
+    int cp = 0;
+    if (with_rhs) {
+#pragma unroll
+        for (int v = 0; v < NV; v++) cs[v] = cs[v] + a.rhs[v * fs + c];
+        decode(cs, T, Eold, qk, o, cp);
+        capped_any |= cp;
+    } else {
+        // the state is decoded already: re-derive it from CS and T
+        double D = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) D += cs[s];
+#pragma unroll
+        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
+        o.U = cs[NS] / D;
+        o.V = cs[NS + 1] / D;
+        o.W = cs[NS + 2] / D;
+        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) / D;
+        o.T = T;
+        o.D = D;
+    }
+    double dY[NS], Tc;
+    const int n = chem_increment<SPEC>(cs, o.T, o.E, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped_any);
+    const double D = o.D;
+#pragma unroll
+    for (int s = 0; s < NS; s++) cs[s] = fmax(D * (o.Y[s] + dY[s]), 0.0);
+    const double E1 = o.E;
+    decode(cs, Tc, E1, qk, o, cp);
+    capped_any |= cp;
+    return n;
+}
+
 // One thread per interior cell.  MODE selects the reference sequence:
 //  M_DECODE  Update_after_CS
 //  M_ADV     Update_after_Adv (+ decode)
@@ -578,22 +621,10 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
     } else if (MODE == M_ADAPT) {
-        // chemistry increment of the closed reactor at the previous decode's
-        // state (adaptive integrator, element-projected), added with the
-        // flux residual
-        double dY[NS], Tc;
-        const int nsub = chem_increment<SPEC>(cs, T, Eold, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped_any);
-        double D0 = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; s++) D0 += cs[s];
-#pragma unroll
-        for (int v = 0; v < NV; v++) {
-            double r = a.rhs[v * fs + c];
-            if (v < NS) r += D0 * dY[v];
-            cs[v] = cs[v] + r;
-        }
-        decode(cs, Tc, Eold, qk, o, capped);
-        capped_any |= capped;
+        // split step: the flux residual first (Update_after_Adv + decode),
+        // then the chemistry of the closed reactor at that state over dt
+        // (adaptive integrator, element-projected), then a decode
+        const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, true, o, capped_any);
         warp_sum(&a.st->substeps, (unsigned long long)nsub);
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);

@@ -227,6 +227,8 @@ void sur_chem_t(eu3d_handle *h)
     const long long n = L.interior_cells();
     P *q = (P *)h->prim;
     cudaMemsetAsync(h->sur_count, 0, 2 * sizeof(int), h->st);
+    // split step: the flux update and its decode first (Update_after_Adv)
+    launch_cell_t<P, SPEC>(h, M_ADV);
     {
         ProfScope ps(h, "sur_mlp");
         SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};

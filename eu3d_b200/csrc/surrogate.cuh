@@ -611,13 +611,13 @@ __device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int valu
     }
 }
 
-// One thread per interior cell.  The network's chemistry increment over dt is
-// taken for the state of the previous decode (the state the FP64 integrator
-// would evaluate its rates at), projected to element conservation, checked
+// One thread per interior cell, after the flux update and its decode (a split
+// step, as the adaptive integrator's).  The network's chemistry increment
+// over dt for the cell's state is projected to element conservation, checked
 // against the training envelope, for negative mass fractions and for the
-// energy balance at the predicted temperature, then added to the
-// flux-updated conserved state, which is decoded in FP64.  Rejected cells
-// (and audited ones) go to the fallback list untouched.
+// energy balance at the predicted temperature, then applied to the species
+// and decoded in FP64.  Rejected cells (and audited ones) go to the fallback
+// list untouched.
 template <class P>
 __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
 {
@@ -696,13 +696,9 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
     Decoded o;
     int capped = 0;
     if (ok) {
-        // flux residual, then the chemistry increment on the species
+        // the chemistry increment on the species (the flux residual is in already)
 #pragma unroll
-        for (int v = 0; v < NV; v++) {
-            double r = a.rhs[v * fs + c];
-            if (v < NS) r += D * (Yn[v] - Y[v]);
-            cs[v] = cs[v] + r;
-        }
+        for (int v = 0; v < NS; v++) cs[v] = D * Yn[v];
         decode(cs, Tg, Eold, qk, o, capped);
         // a decode that fails or leaves the envelope's temperatures goes back
         // to the integrator (from the untouched old state)
@@ -752,20 +748,9 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
             double cs[NV];
             load_cs(a.cs, fs, c, cs);
             const double T = a.T[c], Eold = a.E[c];
-            double dY[NS], Tc;
-            int capped = 0;
-            const int nsub = chem_increment<SPEC>(cs, T, Eold, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped);
-            double D0 = 0.0;
-#pragma unroll
-            for (int s = 0; s < NS; s++) D0 += cs[s];
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                double r = a.rhs[v * fs + c];
-                if (v < NS) r += D0 * dY[v];
-                cs[v] = cs[v] + r;
-            }
             Decoded o;
-            decode(cs, Tc, Eold, qk, o, capped);
+            int capped = 0;
+            const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, false, o, capped);
             atomicAdd(&a.st->substeps, (unsigned long long)nsub);
             store_cs(a.cs, fs, c, cs);
             a.T[c] = o.T;

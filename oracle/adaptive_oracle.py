@@ -91,14 +91,16 @@ def increment(o, dt, atoms, rel=0.02, amp=0.5, nmax=1024, proj_eps=1e-4):
 
 
 def adaptive_step(o, dt, atoms, **kw):
-    """The coupled cell update: CS += RHS + rho_0 dY (species), decode from Tchem."""
+    """The split cell update: CS += RHS and decode (Update_after_Adv,
+    src/Flowfield.cpp:1140-1157), the increment at that state, CS_s = rho
+    max(Y_s + dY_s, 0), decode from Tchem."""
     NS = o.NS
+    o.update_after_adv()
     dY, Tchem, nsub = increment(o, dt, atoms, **kw)
     c = _interior(o, "CS")
-    D0 = c[..., :NS].sum(-1)
-    rhs = _interior(o, "RHS")
-    c[...] = c + rhs
-    c[..., :NS] += D0[..., None] * dY
+    D = c[..., :NS].sum(-1)
+    Y = c[..., :NS] / D[..., None]
+    c[..., :NS] = np.maximum(D[..., None] * (Y + dY), 0.0)
     _interior(o, "T")[...] = Tchem
     o.update_after_cs()
     return nsub
