@@ -1007,8 +1007,6 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
     if (s->react == EU3D_REACT_ADAPTIVE && !h->elements)
         return fail(EU3D_ERR_STATE, "element composition not set (eu3d_set_elements)");
     if (s->react == EU3D_REACT_SURROGATE && !h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached");
-    if (s->react == EU3D_REACT_SURROGATE && s->timeadv == EU3D_ADV_SSPRK2)
-        return fail(EU3D_ERR_ARG, "the surrogate step follows the EE update");
     if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
     if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
     if (s->react == EU3D_REACT_TRAPEZOID && s->type == 1 && h->chem_queue) {
