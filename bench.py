@@ -4,13 +4,19 @@
 Workload (one GPU): 3D oblique detonation, 512 x 256 x 256 interior cells
 (33.5 M), stoichiometric H2-air at Mach 7, 0.1 atm, 300 K with a seeded 1 %
 inflow density perturbation, 25 degree wedge from x = 0.1 L, L = 0.2 m.
-MUSCL_2/minmod + AUSM with FP32 reconstruction and FP64 state, EE time
-advance, CFL 0.5, FP64 IMEX chemistry (9 species, 19 reactions), every step
-one CUDA-graph replay of CFL -> ghost fill -> flux sweeps -> chemistry+decode.
-Inputs (~11 GB of state) are far larger than L2 (126 MB), so no flush is
-needed between steps.
+MUSCL_2/minmod + AUSM with FP32 reconstruction and FP64 state, SSP-RK2 time
+advance, CFL 0.5, every step one CUDA-graph replay of CFL -> ghost fill ->
+flux sweeps -> chemistry + decode.  The timed state is a developed flow: the
+2D case with the same cells advanced with the FP64 adaptive integrator and
+extruded along z.  Inputs (~12 GB of state) are far larger than L2 (126 MB),
+so no flush is needed between steps.
 
-Metric: Mcell-steps/s = interior cells x steps / device time.
+Metric: Mcell-steps/s = interior cells x steps / device time, with the
+learned chemistry surrogate (value); the same steps with the plain FP64 IMEX
+integrator and with the FP64 adaptive integrator (the surrogate's teacher)
+are timed on the same GPU and state and reported beside it, with the
+coupled accuracy of a 2D run (peak T, detonation front) against the FP64
+runs.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -37,7 +43,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s, 3D ODW: NN chemistry vs FP64 integrator, same GPU, ≤1% T err"
 UNIT = "Mcell-steps/s"
-BYTES_PER_CELL_STEP = 224  # algorithmic HBM bytes per cell-step of the fused step (13 FP64 in/out + T in/out)
 CFL = 0.5
 
 
@@ -51,6 +56,10 @@ def parse():
     ap.add_argument("--flux-bits", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--develop", type=int, default=1500, help="2D steps that develop the timed state")
+    ap.add_argument("--model", default=os.path.join(ROOT, "eu3d_b200", "data", "sur_h2_ja919.npz"))
     return ap.parse_args()
 
 
@@ -188,8 +197,158 @@ def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return d.get("hbm_gbs", 6650.0), "measured"
-    return 6650.0, "fallback"
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+# algorithmic work per cell and launch of the kernels a roofline may be quoted for
+KERNEL_WORK = {
+    # flux + residual: 16 FP32 primitives in, 13 FP64 residuals out
+    "advection": ("hbm", 16 * 4 + 13 * 8),
+    # decode after the flux update: 13 FP64 state + RHS in, state + T, E + 16 FP32 primitives out
+    "cell_adv": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
+    # surrogate apply: state + T, E + 10 FP32 outputs in; 9 species + T, E + 16 primitives out
+    "sur_apply": ("hbm", 13 * 8 + 16 + 40 + 9 * 8 + 16 + 16 * 4),
+    # MLP 12 -> 3 x 128 -> 10 forward: 2 (16 128 + 2 128 128 + 128 16) FLOP
+    "sur_mlp": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
+    "cell_imex": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
+    "cell_rk1": ("hbm", 13 * 8 * 4 + 2 * 8 * 2 + 16 * 4),
+    "cell_rk2": ("hbm", 13 * 8 * 4 + 2 * 8 * 2 + 16 * 4),
+}
+
+
+def timed_steps(dev, step, K, W, torch, world, dist, clocks=False, local=0):
+    for _ in range(W):
+        dev.step(**step)
+    dev.synchronize()
+    stream = torch.cuda.ExternalStream(dev.stream)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    ev0.record(stream)
+    for _ in range(K):
+        dev.step(**step)
+    ev1.record(stream)
+    dev.synchronize()
+    if clk:
+        clk.__exit__(None, None, None)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, (clk.summary() if clk else None)
+
+
+def profiled(dev, step, K):
+    """Per-kernel CUDA-event durations over K steps (no graph)."""
+    dev.profile(True)
+    for _ in range(K):
+        dev.step(**step)
+    prof = dev.profile_read()
+    dev.profile(False)
+    return prof
+
+
+def roofline(prof, cells, hbm, tflops, src):
+    """Roofline of the kernel with the largest share of the step among those
+    with a stated algorithmic work."""
+    cand = [(k, v) for k, v in prof.items() if k in KERNEL_WORK]
+    k, v = max(cand, key=lambda kv: kv[1][0])
+    avg_ms = v[0] / v[1]
+    bound, work = KERNEL_WORK[k]
+    if bound == "hbm":
+        ach = work * cells / (avg_ms * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": k, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": TRAFFIC.get(k), "per_cell": f"{work} B", "avg_ms": avg_ms,
+                "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; peak {src} "
+                        f"(MEASURED_PEAKS.json hbm_gbs)"}
+    ach = work * cells / (avg_ms * 1e-3) / 1e12
+    return {"bound": "tensor", "kernel": k, "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops,
+            "traffic": TRAFFIC.get(k), "per_cell": f"{work} FLOP", "avg_ms": avg_ms,
+            "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; peak {src} "
+                    f"(MEASURED_PEAKS.json bf16_tflops)"}
+
+
+# DRAM bytes per launch of the full-size workload (ncu dram__bytes_read + _write,
+# summarised under profiles/; scaled from the captured case by cells)
+TRAFFIC = {}
+
+
+def developed_state(mech, ni, nj, nk, steps2d, seed):
+    """A developed 3D ODW state: the 2D case (same cells) advanced steps2d
+    SSP-RK2 steps with the FP64 adaptive integrator, extruded along z, with
+    the 3D case's seeded inflow perturbation."""
+    from eu3d_b200 import gpu
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.cases import extrude_state, odw_case, setup_odw
+    c2 = odw_case(mech, ni, nj, 2, seed=seed)
+    d2 = gpu.DeviceFlowfield(mech, c2.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=32)
+    setup_odw(d2, c2)
+    d2.set_elements(S.atoms_matrix(mech))
+    d2.run(steps2d, react=gpu.REACT_ADAPTIVE, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
+    d2.synchronize()
+    c3 = odw_case(mech, ni, nj, nk, seed=seed)
+    return d2, c3
+
+
+def accuracy_2d(mech, model, steps, ni=512, nj=256):
+    """Coupled 2D ODW (the 3D case's cells) with the surrogate, the FP64
+    adaptive integrator (its teacher) and the plain FP64 IMEX integrator:
+    peak T and detonation-front position (first x where T > 1800 K, per row)."""
+    from eu3d_b200 import gpu
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.cases import odw_case, setup_odw
+    res, stats = {}, {}
+    for name, react in (("adaptive", gpu.REACT_ADAPTIVE), ("surrogate", gpu.REACT_SURROGATE), ("imex", gpu.REACT_IMEX)):
+        c = odw_case(mech, ni, nj, 2)
+        d = gpu.DeviceFlowfield(mech, c.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=32)
+        setup_odw(d, c)
+        d.set_elements(S.atoms_matrix(mech))
+        if react == gpu.REACT_SURROGATE:
+            model.attach(d, 97)
+        d.run(steps, react=react, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
+        d.synchronize()
+        res[name] = d.download("T")[2:-2, 2:-2, 2].copy()
+        stats[name] = d.status()
+        d.close()
+
+    def fronts(T, thr=1800.0):
+        f = np.full(T.shape[1], np.nan)
+        for j in range(T.shape[1]):
+            r = T[:, j]
+            k = int(np.argmax(r > thr))
+            if r[k] > thr and k > 0:
+                f[j] = k - 1 + (thr - r[k - 1]) / (r[k] - r[k - 1])
+        return f
+
+    fa = fronts(res["adaptive"])
+    out = {"case": f"2D ODW {ni}x{nj} (the 3D case's cells), SSP-RK2, CFL {CFL}, {steps} steps",
+           "peak_T_adaptive": float(np.nanmax(res["adaptive"]))}
+    for name in ("surrogate", "imex"):
+        fx = fronts(res[name])
+        both = np.isfinite(fa) & np.isfinite(fx)
+        d = np.abs(fa - fx)[both]
+        st = stats[name]
+        out[name] = {"peak_T": float(np.nanmax(res[name])),
+                     "peak_T_rel_err_vs_adaptive": float(abs(np.nanmax(res[name]) / np.nanmax(res["adaptive"]) - 1)),
+                     "mean_abs_dT_K": float(np.nanmean(np.abs(res[name] - res["adaptive"]))),
+                     "front_rows_both": int(both.sum()), "front_rows_one_only": int((np.isfinite(fa) ^ np.isfinite(fx)).sum()),
+                     "front_abs_diff_cells_median": float(np.median(d)) if d.size else None,
+                     "front_abs_diff_cells_max": float(d.max()) if d.size else None,
+                     "nonfinite_cells": st["nonfinite_cells"]}
+        if name == "surrogate":
+            tot = st["surrogate_cells"] + st["surrogate_fallback"]
+            out[name]["fallback_frac"] = st["surrogate_fallback"] / max(tot, 1)
+            out[name]["audit_max_dT_K"] = st["surrogate_audit_max_dT"]
+    return out
 
 
 def run_ours(a, rank, world, local):
@@ -197,91 +356,88 @@ def run_ours(a, rank, world, local):
     import torch.distributed as dist
 
     from eu3d_b200 import gpu
-    from eu3d_b200.cases import odw_case, setup_odw
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.cases import extrude_state, setup_odw
     from eu3d_b200.readers import load_h2_ja919
 
     torch.cuda.set_device(local)
     ni, nj, nk = (int(x) for x in a.grid.split(","))
     mech = load_h2_ja919()
-    case = odw_case(mech, ni, nj, nk, seed=rank)
     cells = ni * nj * nk
+    model = S.SurrogateModel.load(a.model)
+    d2, case = developed_state(mech, ni, nj, nk, a.develop, seed=rank)
     dev = gpu.DeviceFlowfield(mech, case.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=a.flux_bits, device=local)
     setup_odw(dev, case)
-    step = dict(react=gpu.REACT_IMEX, type_=0, timeadv=gpu.ADV_EE, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_ODM,
-                cfl=CFL, final_time=1.0)
-    stream = torch.cuda.ExternalStream(dev.stream)
+    dev.set_elements(S.atoms_matrix(mech))
+    model.attach(dev, 4099)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    def reset():
+        extrude_state(d2, dev)
+        dev.set_time(0.0)
+        dev.reset_status()
 
-    for _ in range(max(a.warmup, 3)):
-        dev.step(**step)
-    dev.synchronize()
-
-    # timed region: K graph replays, CUDA events on the handle's stream
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        for _ in range(a.steps):
-            dev.step(**step)
-        ev1.record(stream)
-        dev.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    clocks = clk.summary()
-
-    # per-kernel CUDA-event durations over K more steps (no graph)
-    dev.profile(True)
-    for _ in range(a.steps):
-        dev.step(**step)
-    prof = dev.profile_read()
-    dev.profile(False)
+    base = dict(type_=0, timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
+    forms = {"surrogate": gpu.REACT_SURROGATE, "imex": gpu.REACT_IMEX, "adaptive": gpu.REACT_ADAPTIVE}
+    W = max(a.warmup, 3)
+    timing, profs, statuses, clocks = {}, {}, {}, None
+    for name, react in forms.items():
+        reset()
+        step = dict(base, react=react)
+        ms, clk = timed_steps(dev, step, a.steps, W, torch, world, dist, clocks=(name == "surrogate"), local=local)
+        if clk:
+            clocks = clk
+        statuses[name] = dev.status()
+        timing[name] = ms
+        profs[name] = profiled(dev, step, a.steps)
+    hbm, tfl, src = peaks()
+    prof = profs["surrogate"]
     prof_total = sum(v[0] for v in prof.values())
-    launches = sum(v[1] for v in prof.values())
-    top = max(prof.items(), key=lambda kv: kv[1][0])
-    top_avg_ms = top[1][0] / top[1][1]
-    hbm, src = peaks()
-    achieved = BYTES_PER_CELL_STEP * cells / (top_avg_ms * 1e-3) / 1e9
-    st = dev.status()
-
-    e2e = None
-    if not a.no_e2e:
-        e2e = run_e2e(dev, step, a.steps, cells, torch)
-
+    launches = sum(v[1] for v in prof.values()) * a.steps // max(a.steps, 1)
+    rf = roofline(prof, cells, hbm, tfl, src)
+    ms = timing["surrogate"]
     value = cells * a.steps * world / (ms * 1e-3) / 1e6
+    integ = {k: cells * a.steps * world / (timing[k] * 1e-3) / 1e6 for k in ("imex", "adaptive")}
+    st = statuses["surrogate"]
+    tot = st["surrogate_cells"] + st["surrogate_fallback"]
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": W,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge)",
-                   "cells_per_gpu": cells, "chemistry": "FP64 IMEX integrator (surrogate path not in this line)",
-                   "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state", "time": "EE, CFL 0.5",
+        "dtype": "bf16 (network) + f64 (state, decode, fallback integrator)", "data": "synthetic",
+        "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge, "
+                               f"1 % seeded inflow density perturbation)",
+                   "cells_per_gpu": cells, "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback",
+                   "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state",
+                   "time": f"SSP-RK2, CFL {CFL}",
+                   "state": f"developed: 2D case advanced {a.develop} steps with the FP64 adaptive integrator, "
+                            f"extruded along z",
                    "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
-                   "l2": "state ~11 GB per GPU >> 126 MB L2 (no flush needed)", "graph": "one CUDA graph per step"},
-        "gpu_launches": int(launches),
-        "kernels": {k: {"ms_avg": v[0] / v[1], "share": v[0] / prof_total, "launches": v[1]} for k, v in
-                    sorted(prof.items(), key=lambda kv: -kv[1][0])},
-        "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "note": f"achieved = {BYTES_PER_CELL_STEP} B/cell-step x {cells} cells / avg launch of {top[0]}; "
-                             f"peak {src} (MEASURED_PEAKS.json hbm_gbs)"},
+                   "l2": "state ~12 GB per GPU >> 126 MB L2 (no flush needed)", "graph": "one CUDA graph per step"},
+        "integrator": {"imex_value": integ["imex"], "adaptive_value": integ["adaptive"],
+                       "ratio_vs_imex": value / integ["imex"], "ratio_vs_adaptive": value / integ["adaptive"],
+                       "ms_per_step": {k: timing[k] / a.steps for k in timing},
+                       "note": "same GPU, same state and step; imex = the reference's one-step FP64 IMEX, "
+                               "adaptive = FP64 adaptive integrator (the surrogate's teacher and fallback)"},
+        "surrogate": {"fallback_frac": st["surrogate_fallback"] / max(tot, 1), "rejects": st["surrogate_rejects"],
+                      "audited": st["surrogate_audited"], "audit_max_dT_K": st["surrogate_audit_max_dT"],
+                      "model": os.path.relpath(a.model, ROOT)},
+        "gpu_launches": int(sum(v[1] for v in prof.values())),
+        "kernels": {f: {k: {"ms_avg": v[0] / v[1], "share": v[0] / sum(x[0] for x in profs[f].values()),
+                            "launches": v[1]} for k, v in sorted(profs[f].items(), key=lambda kv: -kv[1][0])}
+                    for f in profs},
+        "roofline": rf,
         "status": {k: st[k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")},
     }
     if clocks:
         out["clocks"] = clocks
-    if e2e:
-        out["e2e"] = e2e
+    if not a.no_accuracy and rank == 0:
+        out["accuracy"] = accuracy_2d(mech, model, a.accuracy_steps)
+    if not a.no_e2e:
+        reset()
+        out["e2e"] = run_e2e(dev, dict(base, react=gpu.REACT_SURROGATE), a.steps, cells, torch)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     dev.close()
+    d2.close()
     return out
 
 
@@ -309,10 +465,11 @@ def run_e2e(dev, step, K, cells, torch):
     dev.synchronize()
     ms = ev0.elapsed_time(ev1)
     h2d = sum(host[n].nbytes for n in ("CS", "T", "E"))
-    d2h = host["CS"].nbytes + host["T"].nbytes + K * 72
+    d2h = host["CS"].nbytes + host["T"].nbytes + K * 96
     return {"value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
             "d2h_bytes_per_step": d2h // K, "ms": ms,
-            "protocol": "upload CS,T,E (pinned) + decode, K eu3d_step calls each with a status read, download CS,T"}
+            "protocol": "upload CS,T,E (pinned) + decode, K eu3d_step calls (surrogate chemistry) each with a status "
+                        "read, download CS,T"}
 
 
 def run_reference(a, rank, world):

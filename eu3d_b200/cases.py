@@ -127,5 +127,22 @@ def upload_primitive_state(dev, st: dict) -> None:
         dev.upload(n, st[n])
 
 
-__all__ = ["complete_state", "species_thermo", "odw_case", "setup_odw", "znd_case", "upload_primitive_state",
+STATE_FIELDS = ("U", "V", "W", "P", "D", "T", "H", "Gamma", "E", "Yi", "CS")
+
+
+def extrude_state(src, dst, k_src: int = None) -> None:
+    """Copy the state of one z plane of handle `src` (default: its first
+    interior plane) into every plane of handle `dst` (same NI, NJ): a
+    spanwise-uniform 3D state from a 2D solution."""
+    if (src.NI, src.NJ) != (dst.NI, dst.NJ):
+        raise ValueError("extrude_state: x-y extents differ")
+    k = src.grid.bc if k_src is None else k_src
+    for n in STATE_FIELDS:
+        a = src.download(n)[:, :, k]
+        b = np.ascontiguousarray(np.broadcast_to(a[:, :, None], (dst.NI, dst.NJ, dst.NK) + a.shape[2:]))
+        dst.upload(n, b)
+        del b
+
+
+__all__ = ["extrude_state", "STATE_FIELDS", "complete_state", "species_thermo", "odw_case", "setup_odw", "znd_case", "upload_primitive_state",
            "OdwCase", "ATM"]

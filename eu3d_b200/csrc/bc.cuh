@@ -158,30 +158,20 @@ __global__ void k_ghost_z(GhostArgs a, P *q)
 
 // Wedge immersed boundary (new): solid cells take the state of the fluid
 // cell nearest to their mirror image across the wedge surface, with the
-// velocity reflected about the surface.  Only solid cells are written and
-// only fluid cells are read.
+// velocity reflected about the surface.  Only the band of solid cells that
+// flux stencils reach is filled (fluid within two cells along x or y);
+// band[n] = (i, j, si, sj): the solid column and its mirror source, the same
+// for every k, listed on the host when the wedge is set.
 template <class P>
-__global__ void k_wedge(GhostArgs a, P *q, const double *xn, const double *yn, double x0, double y0, double tn)
+__global__ void k_wedge_band(GhostArgs a, P *q, const int4 *__restrict__ band, int nband, double nx, double ny)
 {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (n >= nband) return;
+    const int4 b = band[n];
     const Layout &L = a.L;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    const int k = blockIdx.z;
-    if (i >= L.NI) return;
-    const double x = xn[i], y = yn[j];
-    if (!(x > x0 && (y - y0) < (x - x0) * tn)) return;
-    const double cs = 1.0 / sqrt(1.0 + tn * tn), sn = tn * cs;
-    const double nx = -sn, ny = cs;
-    const double dx = xn[L.bc + 1] - xn[L.bc], dy = yn[L.bc + 1] - yn[L.bc];
-    const double dist = (x - x0) * sn - (y - y0) * cs;
-    const double xi = x + 2.0 * dist * nx, yi = y + 2.0 * dist * ny;
-    int si = (int)floor((xi - xn[0]) / dx + 0.5);
-    int sj = (int)floor((yi - yn[0]) / dy + 0.5);
-    si = si < 0 ? 0 : (si > L.NI - 1 ? L.NI - 1 : si);
-    sj = sj < 0 ? 0 : (sj > L.NJ - 1 ? L.NJ - 1 : sj);
-    while (sj < L.NJ - 1 && xn[si] > x0 && (yn[sj] - y0) < (xn[si] - x0) * tn) sj++;
     const long long fs = L.fs;
-    const long long d = L.at(i, j, k), s = L.at(si, sj, k);
+    const long long d = L.at(b.x, b.y, k), s = L.at(b.z, b.w, k);
     ghost_copy(a, q, d, s);
     const double u = (double)q[PU * fs + s], v = (double)q[PV * fs + s];
     const double un = u * nx + v * ny;

@@ -525,6 +525,7 @@ struct CellArgs {
     int *qbins;       // work-queue bin counts (M_TRAP1_PREDICT)
     AdaptCfg acfg;    // adaptive chemistry (M_ADAPT)
     double proj_eps;  // weight floor of its element projection
+    int rhs_applied;  // M_ADAPT: the flux update is in the state and decoded already
 };
 
 __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         // split step: the flux residual first (Update_after_Adv + decode),
         // then the chemistry of the closed reactor at that state over dt
         // (adaptive integrator, element-projected), then a decode
-        const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, true, o, capped_any);
+        const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, !a.rhs_applied, o, capped_any);
         warp_sum(&a.st->substeps, (unsigned long long)nsub);
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);

@@ -73,13 +73,17 @@ struct eu3d_handle {
     size_t stage_bytes = 0;
     double wedge[3] = {0, 0, 0};
     int wedge_on = 0;
+    int4 *wedge_band = nullptr;  // solid cells the stencils reach, with their mirror sources
+    int wedge_nband = 0;
     bool spec = false;  // mechanism equals the compiled-in H2_JA919 tables
     int flux_kz = 16;   // z planes walked by one flux block
+    int flux_stage = 1; // FP32 flux: primitives staged through shared memory (0: read through L1)
     int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
     int queue_blocks = 3;  // resident queue blocks per SM
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
+    bool rhs_applied = false;  // the next M_ADAPT launch finds the flux update decoded already
     int *qlist = nullptr, *qbins = nullptr;
     std::map<StepKey, cudaGraphExec_t> graphs;
     // per-kernel CUDA-event timing (eu3d_profile_enable)
@@ -161,6 +165,7 @@ CellArgs cell_args(eu3d_handle *h)
     a.qbins = h->qbins;
     a.acfg = h->acfg;
     a.proj_eps = h->proj_eps;
+    a.rhs_applied = h->rhs_applied ? 1 : 0;
     return a;
 }
 
@@ -266,6 +271,18 @@ void launch_adv(eu3d_handle *h, int diff)
     dim3 b(FT_X, TY + 2);
     constexpr size_t smem = FluxTile<P>::SMEM;
     ProfScope ps(h, "advection");
+    if (sizeof(P) == 4 && h->flux_stage) {
+        dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
+        dim3 bs(FT_X, FS_TY + 2);
+        const float *qf = (const float *)h->prim;
+        if (diff == EU3D_DIFF_MUSCL1)
+            k_flux_stage<EU3D_DIFF_MUSCL1><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal,
+                                                                              h->rhs, sq, kz);
+        else
+            k_flux_stage<EU3D_DIFF_MUSCL2><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal,
+                                                                              h->rhs, sq, kz);
+        return;
+    }
     if (diff == EU3D_DIFF_MUSCL1)
         k_flux_tile<P, EU3D_DIFF_MUSCL1><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
                                                                  h->rhs, sq, kz);
@@ -315,10 +332,12 @@ void launch_ghost(eu3d_handle *h, int kind)
             k_ghost_z<P><<<(n + 255) / 256, 256, 0, h->st>>>(a, q);
         }
     }
-    if (h->wedge_on) {
-        dim3 gw((L.NI + 127) / 128, L.NJ, L.NK);
+    if (h->wedge_on && h->wedge_nband > 0) {
+        const double tn = h->wedge[2];
+        const double cs = 1.0 / sqrt(1.0 + tn * tn), sn = tn * cs;
+        dim3 gw((h->wedge_nband + 127) / 128, L.NK);
         ProfScope ps(h, "wedge");
-        k_wedge<P><<<gw, 128, 0, h->st>>>(a, q, h->xn, h->yn, h->wedge[0], h->wedge[1], h->wedge[2]);
+        k_wedge_band<P><<<gw, 128, 0, h->st>>>(a, q, h->wedge_band, h->wedge_nband, -sn, cs);
     }
 }
 
@@ -553,7 +572,7 @@ void free_handle(eu3d_handle *h)
     void *ptrs[] = {h->cs,      h->rhs,    h->cs0,    h->T,       h->E,         h->prim,
                     h->nchem,   h->xn,     h->yn,     h->zn,      h->scal,      h->partial,
                     h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
-                    h->sur_audit, h->qlist,   h->qbins};
+                    h->sur_audit, h->qlist,   h->qbins,  h->wedge_band};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
@@ -571,7 +590,7 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
     return EU3D_OK;
 }
 
-int sur_chem_op(eu3d_handle *h);  // learned chemistry step, sur_host.cuh
+int sur_chem_op(eu3d_handle *h, bool decoded);  // learned chemistry step, sur_host.cuh
 
 int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
 {
@@ -594,8 +613,14 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
     case EU3D_REACT_NONE:
         // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
         return cell_op(h, M_NOCHEM);
-    case EU3D_REACT_SURROGATE: return sur_chem_op(h);
-    case EU3D_REACT_ADAPTIVE: return cell_op(h, M_ADAPT);
+    // after SSP-RK2 the state is decoded and RHS holds zeros already
+    case EU3D_REACT_SURROGATE: return sur_chem_op(h, s->timeadv == EU3D_ADV_SSPRK2);
+    case EU3D_REACT_ADAPTIVE: {
+        h->rhs_applied = s->timeadv == EU3D_ADV_SSPRK2;
+        const int rc = cell_op(h, M_ADAPT);
+        h->rhs_applied = false;
+        return rc;
+    }
     default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
     }
 }
@@ -776,6 +801,10 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     cudaMemcpyAsync(h->zn, d->znode, L.NK * sizeof(double), cudaMemcpyHostToDevice, h->st);
     {
         // dynamic shared memory of the tiled flux kernels (above the 48 KB default)
+        cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxStage::SMEM);
+        cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxStage::SMEM);
         cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)FluxTile<float>::SMEM);
         cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -933,6 +962,48 @@ int eu3d_set_wedge(eu3d_handle *h, double x0, double y0, double tan_angle, int e
     h->wedge[1] = y0;
     h->wedge[2] = tan_angle;
     h->wedge_on = enabled ? 1 : 0;
+    if (h->wedge_band) cudaFree(h->wedge_band);
+    h->wedge_band = nullptr;
+    h->wedge_nband = 0;
+    if (h->wedge_on) {
+        // the band of solid cells within two cells (along x or y) of the
+        // fluid and the mirror source of each, on the host in the order of
+        // operations of the wedge fill
+        const Layout &L = h->L;
+        std::vector<double> xn(L.NI), yn(L.NJ);
+        CK(cudaMemcpy(xn.data(), h->xn, L.NI * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(yn.data(), h->yn, L.NJ * sizeof(double), cudaMemcpyDeviceToHost));
+        auto solid = [&](double x, double y) { return x > x0 && (y - y0) < (x - x0) * tan_angle; };
+        const double cs = 1.0 / sqrt(1.0 + tan_angle * tan_angle), sn = tan_angle * cs;
+        const double nx = -sn, ny = cs;
+        const double dx = xn[L.bc + 1] - xn[L.bc], dy = yn[L.bc + 1] - yn[L.bc];
+        std::vector<int4> band;
+        for (int i = 0; i < L.NI; i++)
+            for (int j = 0; j < L.NJ; j++) {
+                const double x = xn[i], y = yn[j];
+                if (!solid(x, y)) continue;
+                bool near = false;
+                for (int o = -2; o <= 2 && !near; o++) {
+                    if (o == 0) continue;
+                    if (i + o >= 0 && i + o < L.NI && !solid(xn[i + o], y)) near = true;
+                    if (j + o >= 0 && j + o < L.NJ && !solid(x, yn[j + o])) near = true;
+                }
+                if (!near) continue;
+                const double dist = (x - x0) * sn - (y - y0) * cs;
+                const double xi = x + 2.0 * dist * nx, yi = y + 2.0 * dist * ny;
+                int si = (int)floor((xi - xn[0]) / dx + 0.5);
+                int sj = (int)floor((yi - yn[0]) / dy + 0.5);
+                si = si < 0 ? 0 : (si > L.NI - 1 ? L.NI - 1 : si);
+                sj = sj < 0 ? 0 : (sj > L.NJ - 1 ? L.NJ - 1 : sj);
+                while (sj < L.NJ - 1 && solid(xn[si], yn[sj])) sj++;
+                band.push_back(make_int4(i, j, si, sj));
+            }
+        if (!band.empty()) {
+            CK(cudaMalloc(&h->wedge_band, band.size() * sizeof(int4)));
+            CK(cudaMemcpy(h->wedge_band, band.data(), band.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        }
+        h->wedge_nband = (int)band.size();
+    }
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;
@@ -1183,6 +1254,7 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     h->flux_kz = t->flux_kz;
     h->chem_queue = t->chem_queue ? 1 : 0;
     h->queue_blocks = t->queue_blocks;
+    h->flux_stage = t->flux_stage ? 1 : 0;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;
@@ -1194,6 +1266,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
     t->flux_kz = h->flux_kz;
     t->chem_queue = h->chem_queue;
     t->queue_blocks = h->queue_blocks;
+    t->flux_stage = h->flux_stage;
     return EU3D_OK;
 }
 
@@ -1202,7 +1275,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
     CK(cudaSetDevice(h->dev));
-    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks};
+    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage};
     // the trials advance the state: keep a copy and put it back after each
     const size_t fs = (size_t)h->L.fs;
     const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
@@ -1227,13 +1300,15 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     copy(true);
     std::vector<eu3d_tuning> cands;
     const bool q = s->react == EU3D_REACT_TRAPEZOID && s->type == 1;
-    for (int kz : {4, 8, 16, 32})
-        for (int cq : {0, 1})
-            for (int qb : {2, 3, 4}) {
-                if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
-                if (q && cq == 0 && qb != start.queue_blocks) continue;
-                cands.push_back({kz, cq, qb});
-            }
+    for (int fst : {0, 1})
+        for (int kz : {4, 8, 16, 32})
+            for (int cq : {0, 1})
+                for (int qb : {2, 3, 4}) {
+                    if (h->flux_bits == 64 && fst != start.flux_stage) continue;
+                    if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
+                    if (q && cq == 0 && qb != start.queue_blocks) continue;
+                    cands.push_back({kz, cq, qb, fst});
+                }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

@@ -171,11 +171,12 @@ __device__ __forceinline__ void face_flux_g(const P *__restrict__ q, long long f
 // are reconstructed: both sides of P, D, gamma and the normal velocity (they
 // set the interface Mach number), then only the upwind side of the
 // tangential velocities, H and the species.  Same values as face_flux_g.
-template <class P, int DIR, int DIFF>
+template <class P, int DIR, int DIFF, bool LDG = true>
 __device__ __forceinline__ void face_flux_up(const P *__restrict__ qc, int fs, int st, bool zspec, P out[NV])
 {
     // qc points at cell a-1 of field 0; field f of cell a-1+n is qc[f * fs + n * st]
-    auto ld = [&](int f, int n) -> P { return __ldg(qc + f * fs + n * st); };
+    // (global memory through the read-only path, or shared memory with LDG = false)
+    auto ld = [&](int f, int n) -> P { return LDG ? __ldg(qc + f * fs + n * st) : qc[f * fs + n * st]; };
     auto both = [&](int f, P &L, P &R) {
         const P v0 = ld(f, 0), v1 = ld(f, 1), v2 = ld(f, 2), v3 = ld(f, 3);
         L = recon_left<P, DIFF>(v0, v1, v2);
@@ -310,6 +311,88 @@ __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
             for (int v = 0; v < NV; v++) {
                 double r = ax * ((double)fx[it][ty][tx + 1][v] - (double)fx[it][ty][tx][v]);
                 r = r - by * ((double)fy[it][ty + 1][tx][v] - (double)fy[it][ty][tx][v]);
+                rhs[v * L.fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
+                qb[v] = qa[v];
+            }
+        }
+    }
+}
+
+// FP32 flux kernel with the primitives staged through shared memory.  Same
+// tile, thread roles and residual order as k_flux_tile, but at each z plane
+// the block first copies the plane's 36 x (TY + 4) cells (the tile and a
+// two-cell halo) of all 16 primitives into shared memory with coalesced
+// loads, then evaluates the x and y faces from there; z faces read their
+// column from global memory as before.
+constexpr int FS_TY = 8, FS_HX = FT_X + 4, FS_HY = FS_TY + 4;
+struct FluxStage {
+    static constexpr int PLANE = NPRIM * FS_HY * FS_HX;  // floats of one staged plane
+    static constexpr int FX = FS_TY * (FT_X + 1) * NV;
+    static constexpr int FY = (FS_TY + 1) * FT_X * NV;
+    static constexpr size_t SMEM = sizeof(float) * (PLANE + FX + FY);
+};
+
+template <int DIFF>
+__global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
+    Layout L, const float *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
+    const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
+{
+    constexpr int TY = FS_TY, HX = FS_HX, HY = FS_HY, PL = HX * HY;
+    extern __shared__ __align__(16) unsigned char flux_smem[];
+    float *S = reinterpret_cast<float *>(flux_smem);
+    auto fx = reinterpret_cast<float(*)[FT_X + 1][NV]>(S + FluxStage::PLANE);
+    auto fy = reinterpret_cast<float(*)[FT_X][NV]>(S + FluxStage::PLANE + FluxStage::FX);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * FT_X + tx, nthr = FT_X * (TY + 2);
+    const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
+    const int kb = L.bc + blockIdx.z * kz;
+    const int ke = min(kb + kz, L.nk + L.bc);
+    const int i = i0 + tx, j = j0 + ty;
+    const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
+    const bool cellw = ty < TY;
+    const bool act = cellw && i <= ilast && j <= jlast;
+    const int fs = (int)L.fs, sz = L.px * L.NJ;
+    const double dt = *dtp;
+    const bool zs_cell = species_quirk && i >= L.ni;
+    float qb[NV], qa[NV];
+    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
+    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
+    for (int k = kb; k < ke; k++) {
+        // stage cells x in [i0 - 2, i0 + 34), y in [j0 - 2, j0 + TY + 2) of plane k
+        // (indices past the array, never needed by a face, are clamped)
+        for (int e = tid; e < FluxStage::PLANE; e += nthr) {
+            const int f = e / PL, r = e - f * PL;
+            const int yy = r / HX, xx = r - yy * HX;
+            const int gi = min(i0 - 2 + xx, L.NI - 1), gj = min(j0 - 2 + yy, L.NJ - 1);
+            S[e] = __ldg(q + (long long)f * fs + L.at(gi, gj, k));
+        }
+        __syncthreads();
+        // x face f of row r: between a = i0+f-1 and a+1, cells a-1 .. a+2 at
+        // staged columns f .. f+3 of staged row r+2
+        {
+            const int r = cellw ? ty : tx;
+            const int f = cellw ? tx : FT_X;
+            const int jr = j0 + r;
+            const int a = i0 + f - 1;
+            if ((cellw || (ty == TY + 1 && tx < TY)) && jr <= jlast && a <= ilast)
+                face_flux_up<float, 1, DIFF, false>(S + (r + 2) * HX + f, PL, 1, species_quirk && a >= L.ni, fx[r][f]);
+        }
+        // y face g of column i: between b = j0+g-1 and b+1, staged rows g .. g+3
+        if (ty <= TY && i <= ilast) {
+            const int b = j0 + ty - 1;
+            if (b <= jlast)
+                face_flux_up<float, 2, DIFF, false>(S + ty * HX + tx + 2, PL, HX, species_quirk && i >= L.ni, fy[ty][tx]);
+        }
+        if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, k) - sz, fs, sz, zs_cell, qa);
+        __syncthreads();
+        if (act) {
+            const double cz = dt / (zn[k] - zn[k - 1]);
+            const long long c = L.at(i, j, k);
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                double r = ax * ((double)fx[ty][tx + 1][v] - (double)fx[ty][tx][v]);
+                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
                 rhs[v * L.fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
                 qb[v] = qa[v];
             }

@@ -220,15 +220,16 @@ int sur_set_attrs()
 
 // ---------------------------------------------------------- coupled step
 template <class P, bool SPEC>
-void sur_chem_t(eu3d_handle *h)
+void sur_chem_t(eu3d_handle *h, bool decoded)
 {
     eu3d_surrogate *s = h->sur;
     const Layout &L = h->L;
     const long long n = L.interior_cells();
     P *q = (P *)h->prim;
     cudaMemsetAsync(h->sur_count, 0, 2 * sizeof(int), h->st);
-    // split step: the flux update and its decode first (Update_after_Adv)
-    launch_cell_t<P, SPEC>(h, M_ADV);
+    // split step: the flux update and its decode first (Update_after_Adv),
+    // unless the time scheme left the state decoded with the update in
+    if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
     {
         ProfScope ps(h, "sur_mlp");
         SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
@@ -248,15 +249,15 @@ void sur_chem_t(eu3d_handle *h)
     }
 }
 
-int sur_chem_op(eu3d_handle *h)
+int sur_chem_op(eu3d_handle *h, bool decoded)
 {
     if (!h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached (eu3d_set_surrogate)");
     if (h->flux_bits == 64) {
-        if (h->spec) sur_chem_t<double, true>(h);
-        else sur_chem_t<double, false>(h);
+        if (h->spec) sur_chem_t<double, true>(h, decoded);
+        else sur_chem_t<double, false>(h, decoded);
     } else {
-        if (h->spec) sur_chem_t<float, true>(h);
-        else sur_chem_t<float, false>(h);
+        if (h->spec) sur_chem_t<float, true>(h, decoded);
+        else sur_chem_t<float, false>(h, decoded);
     }
     CK(cudaGetLastError());
     return EU3D_OK;
@@ -613,7 +614,7 @@ int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride)
 int eu3d_react_surrogate(eu3d_handle *h)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
-    return sur_chem_op(h);
+    return sur_chem_op(h, false);
 }
 
 }  // extern "C"

@@ -619,7 +619,7 @@ __device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int valu
 // and decoded in FP64.  Rejected cells (and audited ones) go to the fallback
 // list untouched.
 template <class P>
-__global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
+__global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
 {
     const CellArgs &a = s.a;
     const Layout &L = a.L;
@@ -684,30 +684,31 @@ __global__ void __launch_bounds__(128, 3) k_sur_apply(SurApplyArgs s, P *__restr
     }
     ok = ok && isfinite(dTn) && fabs(dTn) <= n.v[SN_DT_MAX];
     const bool ok_out = ok;
-    double Tg = T + dTn;
-    if (ok) {
-        // energy balance at the predicted temperature (constant density and energy)
-        double e, cv;
-        mix_energy(Yn, Tg, qk, e, cv);
-        const double res = (e - Eold) / cv;
-        ok = fabs(res) <= n.v[SN_RES_ABS] + n.v[SN_RES_REL] * fabs(dTn);
-    }
-    const bool ok_res = ok;
+    const double Tg = T + dTn;
     Decoded o;
     int capped = 0;
+    bool ok_res = ok;
     if (ok) {
-        // the chemistry increment on the species (the flux residual is in already)
+        // the chemistry increment on the species (the flux update is in
+        // already), decoded from the predicted temperature.  The decode's
+        // first Newton correction is the energy residual of the prediction
+        // at constant density and energy, (e(Y + dY, T + dT) - E) / cv; its
+        // converged result stands in for it: the prediction is kept when
+        // |T_decoded - (T + dT)| <= res_abs + res_rel |dT|.
 #pragma unroll
         for (int v = 0; v < NS; v++) cs[v] = D * Yn[v];
         decode(cs, Tg, Eold, qk, o, capped);
+        ok_res = fabs(o.T - Tg) <= n.v[SN_RES_ABS] + n.v[SN_RES_REL] * fabs(dTn);
         // a decode that fails or leaves the envelope's temperatures goes back
         // to the integrator (from the untouched old state)
-        ok = !capped && isfinite(o.T) && isfinite(o.D) && o.T >= 0.8 * n.v[SN_ENV + 0] && o.T <= 1.2 * n.v[SN_ENV + 1];
+        ok = ok_res && !capped && isfinite(o.T) && isfinite(o.D) && o.T >= 0.8 * n.v[SN_ENV + 0] &&
+             o.T <= 1.2 * n.v[SN_ENV + 1];
     }
     const bool audit = ok && s.audit_stride > 0 && (idx % s.audit_stride) == 0;
     if (ok) {
         if (!audit) {
-            store_cs(a.cs, fs, c, cs);
+#pragma unroll
+            for (int v = 0; v < NS; v++) a.cs[v * fs + c] = cs[v];  // momenta and energy are unchanged
             a.T[c] = o.T;
             a.E[c] = o.E;
             store_prims<P>(o, q, fs, c);

@@ -79,14 +79,28 @@ __device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity)
     return ok != 0;
 }
 
-// bounded wait on an mbarrier phase (about half a second at most): false
-// when the bound ran out, so that no caller can spin forever
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t max_tries = (1u << 22))
+// potentially blocking test: the thread is suspended until the phase
+// completes or about hint_ns pass (then false)
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity, uint32_t hint_ns)
 {
-    for (uint32_t t = 0; t < max_tries; t++) {
-        if (mbar_test(mbar, parity)) return true;
-        if (t > 32) __nanosleep(64);
-    }
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait on an mbarrier phase (under a second): false when the bound
+// ran out, so that no caller can spin forever.  Waiting threads sleep in
+// the barrier instead of issuing test instructions.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t max_tries = (1u << 19))
+{
+    for (uint32_t t = 0; t < max_tries; t++)
+        if (mbar_try(mbar, parity, 1000u)) return true;
     return false;
 }
 

@@ -170,18 +170,21 @@ int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time
 int eu3d_synchronize(eu3d_handle *h);
 /* Launch settings picked per handle (new): z planes walked by one flux block,
    adaptive trapezoid on the persistent work queue (1) or one thread per cell
-   (0), and resident queue blocks per SM.  Changing them drops the recorded
-   step graphs. */
+   (0), resident queue blocks per SM, and (FP32 flux) primitives staged
+   through shared memory (1) or read through L1 (0).  Changing them drops the
+   recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
     int queue_blocks;
+    int flux_stage;
 } eu3d_tuning;
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t);
 int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t);
 /* Autotuner: times `steps` steps of s for each candidate setting (flux_kz in
-   {4, 8, 16, 32}; for the adaptive trapezoid also the queue on/off and 2..4
-   blocks per SM) on the handle's current state, restoring the state after
+   {4, 8, 16, 32}, FP32 flux staged or not; for the adaptive trapezoid also
+   the queue on/off and 2..4 blocks per SM) on the handle's current state,
+   restoring the state after
    each trial, and keeps the fastest.  best / best_ms may be NULL.  Needs
    temporary device memory for one copy of the state. */
 int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tuning *best, double *best_ms);

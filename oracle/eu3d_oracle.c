@@ -710,6 +710,15 @@ static void wedge_fill(orc_field *f, const orc_mech *m, const double *w)
         for (int j = 0; j < f->NJ; j++) {
             double x = f->xnode[i], y = f->ynode[j];
             if (!orc_wedge_solid(w, x, y)) continue;
+            /* only the band the flux stencils reach: a fluid cell within two
+               cells along x or y */
+            int band = 0;
+            for (int o = -2; o <= 2 && !band; o++) {
+                if (o == 0) continue;
+                if (i + o >= 0 && i + o < f->NI && !orc_wedge_solid(w, f->xnode[i + o], y)) band = 1;
+                if (j + o >= 0 && j + o < f->NJ && !orc_wedge_solid(w, x, f->ynode[j + o])) band = 1;
+            }
+            if (!band) continue;
             double dist = ((x - x0) * sn - (y - y0) * cs); /* depth below the surface, >= 0 */
             double xi = x + 2.0 * dist * nx, yi = y + 2.0 * dist * ny;
             int si = (int)floor((xi - f->xnode[0]) / dx + 0.5);
