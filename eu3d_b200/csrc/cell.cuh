@@ -46,16 +46,18 @@ __device__ __forceinline__ void decode(const double cs[NV], double T0, double Eo
     double D = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) D += cs[s];
+    // one reciprocal of the density serves every quotient (within an ulp of dividing)
+    const double iD = 1.0 / D;
     double yr[NS], sYR = 0.0, sdiv = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        o.Y[s] = cs[s] / D;
+        o.Y[s] = cs[s] * iD;
         yr[s] = o.Y[s] * cM.ri[s];
         sYR += yr[s];
-        sdiv += o.Y[s] / cM.mw[s];
+        sdiv += o.Y[s] * cM.imw[s];
     }
-    const double U = cs[NS] / D, V = cs[NS + 1] / D, W = cs[NS + 2] / D;
-    const double Enew = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) / D;
+    const double U = cs[NS] * iD, V = cs[NS + 1] * iD, W = cs[NS + 2] * iD;
+    const double Enew = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) * iD;
     const double Et = (q & EU3D_Q_STALE_E) ? Eold : Enew;
     double A[8];
     int cur = -1;
@@ -558,12 +560,13 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
         double D = 0.0;
 #pragma unroll
         for (int s = 0; s < NS; s++) D += cs[s];
+        const double iD = 1.0 / D;
 #pragma unroll
-        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
-        o.U = cs[NS] / D;
-        o.V = cs[NS + 1] / D;
-        o.W = cs[NS + 2] / D;
-        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) / D;
+        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] * iD;
+        o.U = cs[NS] * iD;
+        o.V = cs[NS + 1] * iD;
+        o.W = cs[NS + 2] * iD;
+        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) * iD;
         o.T = T;
         o.D = D;
     }
@@ -780,12 +783,13 @@ __device__ __forceinline__ void trap1_cell(const CellArgs &a, P *__restrict__ q,
         double D = 0.0;
 #pragma unroll
         for (int s = 0; s < NS; s++) D += cs[s];
+        const double iD = 1.0 / D;
 #pragma unroll
-        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] / D;
-        o.U = cs[NS] / D;
-        o.V = cs[NS + 1] / D;
-        o.W = cs[NS + 2] / D;
-        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) / D;
+        for (int s = 0; s < NS; s++) o.Y[s] = cs[s] * iD;
+        o.U = cs[NS] * iD;
+        o.V = cs[NS + 1] * iD;
+        o.W = cs[NS + 2] * iD;
+        o.E = (cs[NS + 3] - 0.5 * D * (o.U * o.U + o.V * o.V + o.W * o.W)) * iD;
         o.T = a.T[c];
         o.D = D;
         const int n = a.nchem[c];

@@ -37,6 +37,7 @@ struct Layout {
 struct MechConst {
     double c[2][9][NS];  // NASA-9 coefficients [range][a1..a7,b1,b2][species]
     double mw[NS], ri[NS];
+    double imw[NS];      // 1 / mw
     double af[NR], bf[NR], eaf[NR];
     double sf[NS][NR], sb[NS][NR], tb[NS][NR];
     double nu[NS][NR];   // sb - sf

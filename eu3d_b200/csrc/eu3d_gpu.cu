@@ -534,6 +534,7 @@ int validate_mech(const eu3d_desc *d, MechConst &m)
         if (!(d->mw[s] > 0)) return fail(EU3D_ERR_ARG, "molar masses must be positive");
         m.mw[s] = d->mw[s];
         m.ri[s] = R_GAS / d->mw[s];
+        m.imw[s] = 1.0 / d->mw[s];
     }
     for (int r = 0; r < NR; r++) {
         m.af[r] = d->af[r];

@@ -340,7 +340,9 @@ __global__ void k_sur_batch(const float *__restrict__ X, const float *__restrict
 __device__ __forceinline__ float sur_unscale_f(const SurNorm &n, int k, float t, float sc)
 {
     const float y = fmaf(t, n.v[SN_OUT_STD + k], n.v[SN_OUT_MEAN + k]);
-    return sc * n.v[SN_LIN + k] * sinhf(y);
+    // sinh from one fast exponential (the network's output is BF16-accurate)
+    const float e = __expf(fminf(fmaxf(y, -80.f), 80.f));
+    return sc * n.v[SN_LIN + k] * (0.5f * (e - __frcp_rn(e)));
 }
 
 // ------------------------------------------------ fused inference kernel
@@ -348,16 +350,22 @@ __device__ __forceinline__ float sur_unscale_f(const SurNorm &n, int k, float t,
 // four weight matrices in shared memory for its whole life and runs NG tile
 // groups of 128 threads; each group owns 128 TMEM columns and a 32 KB
 // activation tile, and walks 128-cell tiles: features -> bf16 A tile ->
-// tcgen05.mma (FP32 accumulators in TMEM) -> tcgen05.ld, bias, GELU, bf16 ->
-// the next layer's A tile.  While one group runs its epilogue on the CUDA
-// cores, another group's MMAs occupy the tensor pipe.
+// tcgen05.mma (FP32 accumulators in TMEM) -> tcgen05.ld, GELU, bf16 -> the
+// next layer's A tile.  While one group runs its epilogue on the CUDA cores,
+// another group's MMAs occupy the tensor pipe.  The biases ride on the tensor
+// cores too, in BF16: layer 1 through its spare input column 15 (held at 1,
+// with the bias in W1's row 15), layers 2..4 through one more K = 16 MMA of
+// a shared all-ones column against a bias column.
 constexpr int SUR_NG = 4;
 constexpr int SURK_W1 = 0;                             // 128 x 16
 constexpr int SURK_W2 = SURK_W1 + SUR_H * SUR_IN * 2;  // 128 x 128
 constexpr int SURK_W3 = SURK_W2 + SUR_H * SUR_H * 2;
 constexpr int SURK_W4 = SURK_W3 + SUR_H * SUR_H * 2;   // 16 x 128
-constexpr int SURK_BIAS = SURK_W4 + SUR_OUT * SUR_H * 2;
-constexpr int SURK_A = SURK_BIAS + (3 * SUR_H + SUR_OUT) * 4;
+constexpr int SURK_ONES = SURK_W4 + SUR_OUT * SUR_H * 2;   // 128 x 16, column 0 = 1
+constexpr int SURK_BB2 = SURK_ONES + 128 * 16 * 2;           // 128 x 16, column 0 = b2
+constexpr int SURK_BB3 = SURK_BB2 + SUR_H * 16 * 2;          // 128 x 16, column 0 = b3
+constexpr int SURK_BB4 = SURK_BB3 + SUR_H * 16 * 2;          // 16 x 16, column 0 = b4
+constexpr int SURK_A = SURK_BB4 + SUR_OUT * 16 * 2;
 constexpr int SURK_ATILE = 128 * SUR_H * 2;
 constexpr int SURK_MBAR = SURK_A + SUR_NG * SURK_ATILE;
 constexpr int SURK_SMEM = SURK_MBAR + SUR_NG * 8 + 16;
@@ -454,24 +462,38 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-// hidden-layer epilogue of one row: 128 accumulators + bias -> GELU -> bf16 A tile
-__device__ __forceinline__ void sur_hidden_epilogue(uint32_t tmem_row, const float *bias, unsigned char *A, int row)
+// hidden-layer epilogue of one row: 128 accumulators (bias included) -> GELU
+// -> bf16 A tile
+__device__ __forceinline__ void sur_hidden_epilogue(uint32_t tmem_row, unsigned char *A, int row)
 {
-#pragma unroll 1
+#pragma unroll
     for (int c0 = 0; c0 < SUR_H; c0 += 32) {
         float v[32];
         tc::tmem_ld32(tmem_row + c0, v);
-        const float4 *b4 = reinterpret_cast<const float4 *>(bias + c0);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const float4 ba = b4[2 * q], bb = b4[2 * q + 1];
             uint4 w;
-            w.x = gelu_bf16x2(v[8 * q + 0] + ba.x, v[8 * q + 1] + ba.y);
-            w.y = gelu_bf16x2(v[8 * q + 2] + ba.z, v[8 * q + 3] + ba.w);
-            w.z = gelu_bf16x2(v[8 * q + 4] + bb.x, v[8 * q + 5] + bb.y);
-            w.w = gelu_bf16x2(v[8 * q + 6] + bb.z, v[8 * q + 7] + bb.w);
+            w.x = gelu_bf16x2(v[8 * q + 0], v[8 * q + 1]);
+            w.y = gelu_bf16x2(v[8 * q + 2], v[8 * q + 3]);
+            w.z = gelu_bf16x2(v[8 * q + 4], v[8 * q + 5]);
+            w.w = gelu_bf16x2(v[8 * q + 6], v[8 * q + 7]);
             *reinterpret_cast<uint4 *>(A + tc::op_off(128, row, c0 + 8 * q)) = w;
         }
+    }
+}
+
+// a K = 16 operand tile of R rows whose column 0 holds bf16(src[r] * scale) (or
+// 1 when src is null) and whose other columns are zero
+__device__ __forceinline__ void sur_stage_col(unsigned char *dst, const float *src, int R, int tid, int nthr)
+{
+    for (int v = tid; v < R * 2; v += nthr) {
+        const int r = v >> 1, half = v & 1;
+        uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        if (half == 0) {
+            const __nv_bfloat16 b = __float2bfloat16_rn(src ? src[r] : 1.0f);
+            z.x = (uint32_t)__bfloat16_as_ushort(b);
+        }
+        *reinterpret_cast<uint4 *>(dst + tc::op_off(R, r, 8 * half)) = z;
     }
 }
 
@@ -482,7 +504,6 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, nthr = blockDim.x;
     const int g = tid >> 7, t = tid & 127, warp = tid >> 5;
-    float *bias = reinterpret_cast<float *>(sm + SURK_BIAS);
     __shared__ SurNorm nrm;
     for (int v = tid; v < EU3D_SUR_NORM_LEN; v += nthr) nrm.v[v] = nrm_g->v[v];
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + SURK_MBAR);
@@ -493,11 +514,15 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
     sur_stage(sm + SURK_W2, W.Wt[1], SUR_H, SUR_H, tid, nthr);
     sur_stage(sm + SURK_W3, W.Wt[2], SUR_H, SUR_H, tid, nthr);
     sur_stage(sm + SURK_W4, W.Wt[3], SUR_OUT, SUR_H, tid, nthr);
-    for (int v = tid; v < 3 * SUR_H + SUR_OUT; v += nthr) {
-        const int l = v / SUR_H, c = v % SUR_H;
-        const int off = l == 0 ? SUR_OFF_B1 : l == 1 ? SUR_OFF_B2 : l == 2 ? SUR_OFF_B3 : SUR_OFF_B4;
-        bias[v] = W.p[off + c];
-    }
+    sur_stage_col(sm + SURK_ONES, nullptr, 128, tid, nthr);
+    sur_stage_col(sm + SURK_BB2, W.p + SUR_OFF_B2, SUR_H, tid, nthr);
+    sur_stage_col(sm + SURK_BB3, W.p + SUR_OFF_B3, SUR_H, tid, nthr);
+    sur_stage_col(sm + SURK_BB4, W.p + SUR_OFF_B4, SUR_OUT, tid, nthr);
+    __syncthreads();
+    // layer 1's bias takes the place of W1's row 15 (input column 15 is held at 1)
+    for (int n = tid; n < SUR_H; n += nthr)
+        *reinterpret_cast<__nv_bfloat16 *>(sm + SURK_W1 + tc::op_off(SUR_H, n, 15)) =
+            __float2bfloat16_rn(W.p[SUR_OFF_B1 + n]);
     if (warp == 0) tc::tmem_alloc(slot, 128 * SUR_NG);
     if (tid == 0) {
         for (int q = 0; q < SUR_NG; q++) tc::mbar_init(tc::smem_u32(mbar + q), 1);
@@ -514,6 +539,8 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
     const uint32_t w1 = tc::smem_u32(sm + SURK_W1), w2 = tc::smem_u32(sm + SURK_W2), w3 = tc::smem_u32(sm + SURK_W3),
                    w4 = tc::smem_u32(sm + SURK_W4);
     const uint32_t id128 = tc::idesc_bf16(128, SUR_H), id16 = tc::idesc_bf16(128, SUR_OUT);
+    const uint32_t ones = tc::smem_u32(sm + SURK_ONES), bb2 = tc::smem_u32(sm + SURK_BB2),
+                   bb3 = tc::smem_u32(sm + SURK_BB3), bb4 = tc::smem_u32(sm + SURK_BB4);
     uint32_t phase = 0;
     bool ok = true;
 
@@ -524,6 +551,7 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
         if (!have)
 #pragma unroll
             for (int i = 0; i < SUR_IN; i++) f[i] = 0.f;
+        f[15] = 1.0f;  // carries layer 1's bias
         uint4 w0, w1v;
         w0.x = pack_bf16(f[0], f[1]);
         w0.y = pack_bf16(f[2], f[3]);
@@ -535,7 +563,7 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
         w1v.w = pack_bf16(f[14], f[15]);
         *reinterpret_cast<uint4 *>(A + tc::op_off(128, t, 0)) = w0;
         *reinterpret_cast<uint4 *>(A + tc::op_off(128, t, 8)) = w1v;
-#pragma unroll 1
+#pragma unroll
         for (int layer = 0; layer < 4; layer++) {
             tc::fence_async_smem();
             tc::fence_before();
@@ -551,6 +579,8 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
 #pragma unroll
                     for (int s = 0; s < SUR_H / 16; s++)
                         tc::mma(tmem, tc::sdesc(aS + s * 128 * 32), tc::sdesc(wb + s * N * 32), idd, s > 0 ? 1u : 0u);
+                    const uint32_t bb = layer == 1 ? bb2 : layer == 2 ? bb3 : bb4;
+                    tc::mma(tmem, tc::sdesc(ones), tc::sdesc(bb), idd, 1u);  // + bias
                 }
                 tc::commit(mb);
             }
@@ -558,12 +588,10 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
             phase ^= 1;
             tc::fence_after();
             if (layer < 3) {
-                sur_hidden_epilogue(trow, bias + layer * SUR_H, A, t);
+                sur_hidden_epilogue(trow, A, t);
             } else {
                 float o[SUR_OUT];
                 tc::tmem_ld16(trow, o);
-#pragma unroll
-                for (int k = 0; k < SUR_OUT; k++) o[k] += bias[3 * SUR_H + k];
                 if (have) src.store(idx, o);
             }
         }
@@ -640,11 +668,12 @@ __global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restr
     double D = 0.0, sdiv = 0.0;
 #pragma unroll
     for (int sp = 0; sp < NS; sp++) D += cs[sp];
+    const double iD = 1.0 / D;
     double Y[NS];
 #pragma unroll
     for (int sp = 0; sp < NS; sp++) {
-        Y[sp] = cs[sp] / D;
-        sdiv += Y[sp] / cM.mw[sp];
+        Y[sp] = cs[sp] * iD;
+        sdiv += Y[sp] * cM.imw[sp];
     }
     const double p = D * R_GAS * 1000 * sdiv * T;
     // envelope and network-output arithmetic in FP32 (the network itself is BF16)
