@@ -60,6 +60,7 @@ struct Status {
     unsigned long long audit_cells;        // surrogate cells also run through the integrator
     unsigned long long audit_max_dT_bits;  // largest |T_surrogate - T_integrator| (double bits)
     unsigned long long sur_reject[4];      // rejections: envelope, network output, energy residual, decode
+    unsigned long long wait_timeouts;      // kernels that gave up a bounded wait (shared-memory ring, TMA)
 };
 
 // Powers of T shared by every species' polynomial at one temperature.

@@ -1,6 +1,7 @@
 // EU3D B200 hot path: handle, memory, launches and the C ABI declared in
 // include/eu3d_gpu.h.  One translation unit so that the mechanism lives in a
 // single __constant__ object shared by every kernel.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -77,7 +78,9 @@ struct eu3d_handle {
     int wedge_nband = 0;
     bool spec = false;  // mechanism equals the compiled-in H2_JA919 tables
     int flux_kz = 16;   // z planes walked by one flux block
-    int flux_stage = 1; // FP32 flux: primitives staged through shared memory (0: read through L1)
+    int flux_stage = 2; // FP32 flux: 2 TMA ring (k_flux_ring), 1 staged by loads (k_flux_stage), 0 through L1
+    CUtensorMap tq{};   // TMA map of the FP32 primitive array (k_flux_ring)
+    bool tq_ok = false;
     int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
     int queue_blocks = 3;  // resident queue blocks per SM
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
@@ -260,6 +263,45 @@ int cell_op(eu3d_handle *h, int mode)
     return EU3D_OK;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &qr) == cudaSuccess &&
+            qr == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)f;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// TMA map of the FP32 primitives as a 4-D tensor {x: px, y: NJ, z: NK,
+// field: NPRIM}, box {36, 12, 1, 16}: one tile plane with its halo.
+bool make_prim_map(eu3d_handle *h)
+{
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc || h->flux_bits != 32 || h->L.bc != 2) return false;
+    const Layout &L = h->L;
+    const cuuint64_t dims[4] = {(cuuint64_t)L.px, (cuuint64_t)L.NJ, (cuuint64_t)L.NK, (cuuint64_t)NPRIM};
+    const cuuint64_t strides[3] = {(cuuint64_t)L.px * 4, (cuuint64_t)L.px * L.NJ * 4, (cuuint64_t)L.fs * 4};
+    const cuuint32_t box[4] = {FluxRing::BOX[0], FluxRing::BOX[1], FluxRing::BOX[2], FluxRing::BOX[3]};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(&h->tq, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, h->prim, dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <class P>
 void launch_adv(eu3d_handle *h, int diff)
 {
@@ -271,6 +313,18 @@ void launch_adv(eu3d_handle *h, int diff)
     dim3 b(FT_X, TY + 2);
     constexpr size_t smem = FluxTile<P>::SMEM;
     ProfScope ps(h, "advection");
+    if (sizeof(P) == 4 && h->flux_stage == 2 && h->tq_ok) {
+        dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
+        dim3 bs(FT_X, FR_TY + 2);
+        const float *qf = (const float *)h->prim;
+        if (diff == EU3D_DIFF_MUSCL1)
+            k_flux_ring<EU3D_DIFF_MUSCL1><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn,
+                                                                            h->scal, h->rhs, sq, kz, h->status);
+        else
+            k_flux_ring<EU3D_DIFF_MUSCL2><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn,
+                                                                            h->scal, h->rhs, sq, kz, h->status);
+        return;
+    }
     if (sizeof(P) == 4 && h->flux_stage) {
         dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
         dim3 bs(FT_X, FS_TY + 2);
@@ -801,7 +855,18 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     cudaMemcpyAsync(h->yn, d->ynode, L.NJ * sizeof(double), cudaMemcpyHostToDevice, h->st);
     cudaMemcpyAsync(h->zn, d->znode, L.NK * sizeof(double), cudaMemcpyHostToDevice, h->st);
     {
-        // dynamic shared memory of the tiled flux kernels (above the 48 KB default)
+        // dynamic shared memory of the tiled flux kernels (above the 48 KB default);
+        // the TMA ring kernel runs two blocks per SM
+        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxRing::SMEM);
+        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)FluxRing::SMEM);
+        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        h->tq_ok = make_prim_map(h);
+        if (!h->tq_ok) h->flux_stage = 1;
         cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)FluxStage::SMEM);
         cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1255,7 +1320,9 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     h->flux_kz = t->flux_kz;
     h->chem_queue = t->chem_queue ? 1 : 0;
     h->queue_blocks = t->queue_blocks;
-    h->flux_stage = t->flux_stage ? 1 : 0;
+    if (t->flux_stage < 0 || t->flux_stage > 2) return fail(EU3D_ERR_ARG, "flux_stage must be 0, 1 or 2");
+    // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
+    h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;
@@ -1301,7 +1368,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     copy(true);
     std::vector<eu3d_tuning> cands;
     const bool q = s->react == EU3D_REACT_TRAPEZOID && s->type == 1;
-    for (int fst : {0, 1})
+    for (int fst : {0, 1, 2})
         for (int kz : {4, 8, 16, 32})
             for (int cq : {0, 1})
                 for (int qb : {2, 3, 4}) {
@@ -1377,6 +1444,7 @@ int eu3d_get_status(eu3d_handle *h, eu3d_status *o)
     memcpy(&mx, &s.audit_max_dT_bits, sizeof(double));
     o->surrogate_audit_max_dT = mx;
     for (int r = 0; r < 4; r++) o->surrogate_rejects[r] = (long long)s.sur_reject[r];
+    o->wait_timeouts = (long long)s.wait_timeouts;
     o->dt = sc[0];
     o->time = sc[1];
     return EU3D_OK;

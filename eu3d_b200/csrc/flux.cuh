@@ -17,7 +17,10 @@
 // straightforward form, kept for cross-checking the tiled kernel.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace eu3d {
 
@@ -82,16 +85,16 @@ template <>
 __device__ __forceinline__ float recon_left<float, EU3D_DIFF_MUSCL2>(float a, float b, float c)
 {
     const float A0 = b - a, A1 = c - b, d = A0 + 1e-12f;
-    if (!(A1 * d > 0.f)) return b;
-    return b + 0.5f * (fabsf(A1) >= fabsf(d) ? A0 : A1);
+    const float r = __fmaf_rn(0.5f, fabsf(A1) >= fabsf(d) ? A0 : A1, b);
+    return __fmul_rn(A1, d) > 0.f ? r : b;
 }
 
 template <>
 __device__ __forceinline__ float recon_right<float, EU3D_DIFF_MUSCL2>(float b, float c, float d)
 {
     const float A1 = c - b, A2 = d - c, e = A2 + 1e-12f;
-    if (!(A1 * e > 0.f)) return c;
-    return c - 0.5f * (fabsf(A1) >= fabsf(e) ? A2 : A1);
+    const float r = __fmaf_rn(-0.5f, fabsf(A1) >= fabsf(e) ? A2 : A1, c);
+    return __fmul_rn(A1, e) > 0.f ? r : c;
 }
 
 // a / b: IEEE in FP64 (parity path), the fast approximate form in FP32
@@ -166,16 +169,129 @@ __device__ __forceinline__ void face_flux_g(const P *__restrict__ q, long long f
     ausm<P, DIR>(ql, qr, yl, yr, out);
 }
 
+// Upwind-side MUSCL_2 state in one formula for both sides, FP32.  For the
+// left state pass (far, ctr, oth) = f(a-1), f(a), f(a+1) and seps = +1e-12;
+// for the right state f(a+2), f(a+1), f(a) and seps = -1e-12.  Negating both
+// differences and the epsilon turns recon_right's arithmetic into
+// recon_left's with every rounding mirrored, so the result equals
+// recon_left / recon_right bit for bit and no branch picks the side.
+__device__ __forceinline__ float up_muscl2(float far, float ctr, float oth, float seps)
+{
+    const float A0 = ctr - far, A1 = oth - ctr, d = A0 + seps;
+    const float h = fabsf(A1) >= fabsf(d) ? A0 : A1;
+    return (__fmul_rn(A1, d) > 0.f) ? __fmaf_rn(0.5f, h, ctr) : ctr;
+}
+
+// AUSM face flux from the four cells a-1 .. a+2 around the face (a, a+1).
+// Only the states AUSM reads are reconstructed: both sides of P, D, gamma
+// and the normal velocity (they set the interface Mach number), then only
+// the upwind side of the tangential velocities, H and the species.  The
+// source gives field f of cell a-1+n as v(f, n) and the upwind triple of a
+// field as up3(f, left, far, ctr, oth) (cells a-1, a, a+1 when left, else
+// a+2, a+1, a); both are plain loads, from global or shared memory.
+// src/Flowfield.cpp:1395-1500 (AUSM), include/Differ.hpp:149-238 (MUSCL_2).
+template <int DIR, int DIFF, class Src>
+__device__ __forceinline__ void face_flux_src(const Src &src, bool zspec, float out[NV])
+{
+    // Every sum of products is written out with explicit rounding
+    // (__fmaf_rn / __fmul_rn), so that the compiler cannot contract it
+    // differently in different kernels: all FP32 flux kernels give the same
+    // bits for the same face.
+    auto both = [&](int f, float &L, float &R) {
+        const float v0 = src.v(f, 0), v1 = src.v(f, 1), v2 = src.v(f, 2), v3 = src.v(f, 3);
+        L = recon_left<float, DIFF>(v0, v1, v2);
+        R = recon_right<float, DIFF>(v1, v2, v3);
+    };
+    constexpr int FN = DIR == 1 ? PU : DIR == 2 ? PV : PW;
+    float DL, DR, PL, PR, GL, GR, NL, NR;
+    both(PD, DL, DR);
+    both(PP, PL, PR);
+    both(PG, GL, GR);
+    both(FN, NL, NR);
+    const float CL = sqrtf(__fdividef(__fmul_rn(GL, PL), DL));
+    const float CR = sqrtf(__fdividef(__fmul_rn(GR, PR), DR));
+    const float CI = __fmul_rn(0.5f, CL + CR);
+    const float MaL = __fdividef(NL, CI), MaR = __fdividef(NR, CI);
+    // both branches of the split Mach numbers are evaluated and one is
+    // selected (the unused one may divide by ~0; its result is dropped)
+    float B1, G1, B2, G2;
+    {
+        const float mp = MaL + 1.0f, m2 = __fmaf_rn(MaL, MaL, -1.0f);
+        const float mp2 = __fmul_rn(mp, mp), m22 = __fmul_rn(m2, m2);
+        const float b_sub = __fmaf_rn(0.125f, m22, __fmul_rn(0.25f, mp2));
+        const float g_sub = __fmaf_rn(__fmul_rn(0.1875f, MaL), m22, __fmul_rn(__fmul_rn(0.25f, mp2), 2.0f - MaL));
+        const float b_sup = __fmul_rn(0.5f, MaL + fabsf(MaL));
+        const bool sub = fabsf(MaL) < 1.0f;
+        B1 = sub ? b_sub : b_sup;
+        G1 = sub ? g_sub : __fdividef(b_sup, MaL);
+    }
+    {
+        const float mm = MaR - 1.0f, m2 = __fmaf_rn(MaR, MaR, -1.0f);
+        const float mm2 = __fmul_rn(mm, mm), m22 = __fmul_rn(m2, m2);
+        const float b_sub = __fmaf_rn(-0.125f, m22, __fmul_rn(-0.25f, mm2));
+        const float g_sub = __fmaf_rn(__fmul_rn(-0.1875f, MaR), m22, __fmul_rn(__fmul_rn(0.25f, mm2), 2.0f + MaR));
+        const float b_sup = __fmul_rn(0.5f, MaR - fabsf(MaR));
+        const bool sub = fabsf(MaR) < 1.0f;
+        B2 = sub ? b_sub : b_sup;
+        G2 = sub ? g_sub : __fdividef(b_sup, MaR);
+    }
+    const float VI = __fmul_rn(B1 + B2, CI);
+    const bool left = VI >= 0.0f;
+    const float seps = left ? 1e-12f : -1e-12f;
+    auto up = [&](int f) -> float {
+        float far, ctr, oth;
+        src.up3(f, left, far, ctr, oth);
+        if (DIFF == EU3D_DIFF_MUSCL1) return ctr;
+        return up_muscl2(far, ctr, oth, seps);
+    };
+    const float Ds = left ? DL : DR;
+    const float Us = DIR == 1 ? (left ? NL : NR) : up(PU);
+    const float Vs = DIR == 2 ? (left ? NL : NR) : up(PV);
+    const float Ws = DIR == 3 ? (left ? NL : NR) : up(PW);
+    const float Hs = up(PH);
+    const float VD = __fmul_rn(VI, Ds);
+#pragma unroll
+    for (int s = 0; s < NS; s++) out[s] = zspec ? __fmul_rn(0.0f, VD) : __fmul_rn(VD, up(PY + s));
+    // normal momentum: VD u_n + G1 PL + G2 PR
+    const float pn = __fmaf_rn(G2, PR, __fmul_rn(G1, PL));
+    out[NS] = DIR == 1 ? __fmaf_rn(VD, Us, pn) : __fmul_rn(VD, Us);
+    out[NS + 1] = DIR == 2 ? __fmaf_rn(VD, Vs, pn) : __fmul_rn(VD, Vs);
+    out[NS + 2] = DIR == 3 ? __fmaf_rn(VD, Ws, pn) : __fmul_rn(VD, Ws);
+    // energy: VI (D H + D/2 |u|^2)
+    const float q2 = __fmaf_rn(Ws, Ws, __fmaf_rn(Vs, Vs, __fmul_rn(Us, Us)));
+    out[NS + 3] = __fmul_rn(VI, __fmaf_rn(__fmul_rn(0.5f, Ds), q2, __fmul_rn(Ds, Hs)));
+}
+
+// Cells a-1 .. a+2 at element step st from qc (cell a-1 of field 0), fields
+// fs elements apart; global memory through the read-only path (LDG) or
+// shared memory.
+template <bool LDG>
+struct StridedSrc {
+    const float *qc;
+    int fs, st;
+    __device__ __forceinline__ float ld(const float *p) const { return LDG ? __ldg(p) : *p; }
+    __device__ __forceinline__ float v(int f, int n) const { return ld(qc + f * fs + n * st); }
+    __device__ __forceinline__ void up3(int f, bool left, float &far, float &ctr, float &oth) const
+    {
+        const float *p = left ? qc : qc + 3 * st;
+        const int s = left ? st : -st;
+        far = ld(p + f * fs);
+        ctr = ld(p + f * fs + s);
+        oth = ld(p + f * fs + 2 * s);
+    }
+};
+
 // Face flux between cells a and a+1 (cells a-1 .. a+2 along the direction,
-// element stride st, c0 the index of cell a-1).  Only the states AUSM reads
-// are reconstructed: both sides of P, D, gamma and the normal velocity (they
-// set the interface Mach number), then only the upwind side of the
-// tangential velocities, H and the species.  Same values as face_flux_g.
+// element stride st, qc the index of cell a-1 of field 0).  FP64: the
+// reference's reconstruction with divisions; FP32: face_flux_src.
 template <class P, int DIR, int DIFF, bool LDG = true>
 __device__ __forceinline__ void face_flux_up(const P *__restrict__ qc, int fs, int st, bool zspec, P out[NV])
 {
+    if constexpr (sizeof(P) == 4) {
+        face_flux_src<DIR, DIFF>(StridedSrc<LDG>{qc, fs, st}, zspec, out);
+        return;
+    } else {
     // qc points at cell a-1 of field 0; field f of cell a-1+n is qc[f * fs + n * st]
-    // (global memory through the read-only path, or shared memory with LDG = false)
     auto ld = [&](int f, int n) -> P { return LDG ? __ldg(qc + f * fs + n * st) : qc[f * fs + n * st]; };
     auto both = [&](int f, P &L, P &R) {
         const P v0 = ld(f, 0), v1 = ld(f, 1), v2 = ld(f, 2), v3 = ld(f, 3);
@@ -230,6 +346,7 @@ __device__ __forceinline__ void face_flux_up(const P *__restrict__ qc, int fs, i
     if (DIR == 2) out[NS + 1] = VD * Vs + G1 * PL + G2 * PR;
     if (DIR == 3) out[NS + 2] = VD * Ws + G1 * PL + G2 * PR;
     out[NS + 3] = VI * (Ds * Hs + P(0.5) * Ds * (Us * Us + Vs * Vs + Ws * Ws));
+    }
 }
 
 constexpr int FT_X = 32;
@@ -397,6 +514,167 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
                 qb[v] = qa[v];
             }
         }
+    }
+}
+
+// FP32 flux kernel fed by TMA.  Same tile (32 x 8 cells plus two face
+// warps), face ownership and residual order as k_flux_stage.  Differences:
+//  * each z plane of the tile with its two-cell halo (36 x 12 cells x 16
+//    primitives, 27 KB) arrives by one TMA box load into a ring of three
+//    shared-memory buffers: while plane c is processed, planes c and c+1 are
+//    resident and c+2 is in flight, so no thread computes load addresses;
+//  * a z face reads cells c and c+1 from the ring and only c-1 and c+2 from
+//    global memory (L2);
+//  * a cell's right x face is its right neighbour's left face, passed by a
+//    warp shuffle (row ends through shared memory from the face warp);
+//  * the upwind side is reconstructed without branches (face_flux_src).
+// Every wait on the ring is bounded: when one runs out the block counts a
+// timeout in the status, waits (bounded) for its copies in flight and stops.
+constexpr int FR_TY = 8, FR_HX = FT_X + 4, FR_HY = FR_TY + 4, FR_PL = FR_HX * FR_HY, FR_NBUF = 3;
+struct FluxRing {
+    static constexpr int PLANE = NPRIM * FR_PL;         // floats of one staged plane
+    static constexpr uint32_t PLANE_BYTES = PLANE * 4;  // bytes of one TMA box (27648)
+    static constexpr int FY = (FR_TY + 1) * FT_X * NV;  // y-face fluxes
+    static constexpr int FXE = FR_TY * NV;              // the last x face of each row
+    static constexpr size_t BYTES = FR_NBUF * PLANE_BYTES + 4 * (FY + FXE) + 8 * FR_NBUF;
+    static constexpr size_t SMEM = BYTES + 1024;        // slack to align the ring to 1 KB
+    // TMA box {x, y, z, field}
+    static constexpr unsigned BOX[4] = {FR_HX, FR_HY, 1, NPRIM};
+};
+
+// Source of the z face between planes c and c+1 of one column: cells c-1
+// and c+2 from global memory, c and c+1 from the ring.
+struct ZSrc {
+    const float *gm, *gp;  // cell (i, j, c-1) and (i, j, c+2), field 0
+    const float *sc, *sn;  // the cell in the staged planes c and c+1, field 0
+    int fs;                // global field stride
+    __device__ __forceinline__ float v(int f, int n) const
+    {
+        return n == 0 ? __ldg(gm + f * fs) : n == 1 ? sc[f * FR_PL] : n == 2 ? sn[f * FR_PL] : __ldg(gp + f * fs);
+    }
+    __device__ __forceinline__ void up3(int f, bool left, float &far, float &ctr, float &oth) const
+    {
+        far = __ldg((left ? gm : gp) + f * fs);
+        ctr = (left ? sc : sn)[f * FR_PL];
+        oth = (left ? sn : sc)[f * FR_PL];
+    }
+};
+
+template <int DIFF>
+__global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
+    const __grid_constant__ CUtensorMap tq, Layout L, const float *__restrict__ q, const double *__restrict__ xn,
+    const double *__restrict__ yn, const double *__restrict__ zn, const double *__restrict__ dtp,
+    double *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat)
+{
+    constexpr int TY = FR_TY, HX = FR_HX, PL = FR_PL;
+    extern __shared__ unsigned char fr_raw[];
+    const uint32_t raw_s = tc::smem_u32(fr_raw);
+    float *ring = reinterpret_cast<float *>(fr_raw + (((raw_s + 1023u) & ~1023u) - raw_s));
+    auto fy = reinterpret_cast<float(*)[FT_X][NV]>(ring + FR_NBUF * FluxRing::PLANE);
+    auto fxe = reinterpret_cast<float(*)[NV]>(ring + FR_NBUF * FluxRing::PLANE + FluxRing::FY);
+    const uint32_t ring_s = tc::smem_u32(ring);
+    const uint32_t mb_s = ring_s + 4u * (FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FT_X + tx;
+    const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
+    const int kb = L.bc + blockIdx.z * kz;
+    const int np = min(kz, L.nk + L.bc - kb);  // planes whose residual this block forms
+    const int i = i0 + tx, j = j0 + ty;
+    const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
+    const bool cellw = ty < TY;
+    const bool act = cellw && i <= ilast && j <= jlast;
+    const int fs = (int)L.fs, sz = L.px * L.NJ;
+    // plane kb + p into buffer p % 3; the block loads planes kb .. kb + np
+    // (the last one only feeds the top z face).  x = i0 - 2 = 32 blockIdx.x
+    // keeps the box start on a 16-byte boundary.
+    auto issue = [&](int p) {
+        const uint32_t b = (uint32_t)(p % FR_NBUF);
+        tc::mbar_expect_tx(mb_s + 8u * b, FluxRing::PLANE_BYTES);
+        tc::tma_load_4d(ring_s + b * FluxRing::PLANE_BYTES, &tq, i0 - 2, j0 - 2, kb + p, 0, mb_s + 8u * b);
+    };
+    if (tid == 0) {
+        for (int b = 0; b < FR_NBUF; b++) tc::mbar_init(mb_s + 8u * b, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    int issued = min(FR_NBUF, np + 1);
+    if (tid == 0)
+        for (int p = 0; p < issued; p++) issue(p);
+    const double dt = *dtp;
+    const bool zs_cell = species_quirk && i >= L.ni;
+    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
+    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    float qb[NV], qa[NV], fo[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) qb[v] = qa[v] = fo[v] = 0.f;
+    // the z face below the first plane, from global memory
+    if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
+    const float *gcol = q + (act ? L.at(i, j, kb) : 0);
+    const int so = (ty + 2) * HX + tx + 2;  // the cell inside a staged field plane
+    bool ok = true;
+    int p = 0;
+    for (; p < np; p++) {
+        const int b0 = p % FR_NBUF, b1 = (p + 1) % FR_NBUF;
+        if (p == 0) ok = tc::mbar_wait(mb_s + 8u * b0, 0) && ok;
+        ok = tc::mbar_wait(mb_s + 8u * b1, ((p + 1) / FR_NBUF) & 1) && ok;
+        const float *S0 = ring + b0 * FluxRing::PLANE, *S1 = ring + b1 * FluxRing::PLANE;
+        const int k = kb + p;
+        // y face g = ty of column i, between b = j0+g-1 and b+1 (staged rows
+        // g .. g+3): faces 0..7 by the cell warps, face 8 by warp TY
+        if (ty <= TY && i <= ilast && j0 + ty - 1 <= jlast)
+            face_flux_src<2, DIFF>(StridedSrc<false>{S0 + ty * HX + tx + 2, PL, HX}, species_quirk && i >= L.ni,
+                                   fy[ty][tx]);
+        // z face above the cell (between planes k and k+1)
+        if (act) {
+            const ZSrc zsrc{gcol + (long long)(p - 1) * sz, gcol + (long long)(p + 2) * sz, S0 + so, S1 + so, fs};
+            face_flux_src<3, DIFF>(zsrc, zs_cell, qa);
+        }
+        // x face f of row r, between a = i0+f-1 and a+1 (staged columns
+        // f .. f+3): f = tx by the cell warps, f = 32 of row tx by warp TY+1
+        {
+            const bool xw = cellw || (ty == TY + 1 && tx < TY);
+            const int r = cellw ? ty : tx;
+            const int f = cellw ? tx : FT_X;
+            const int a = i0 + f - 1;
+            if (xw && j0 + r <= jlast && a <= ilast) {
+                face_flux_src<1, DIFF>(StridedSrc<false>{S0 + (r + 2) * HX + f, PL, 1}, species_quirk && a >= L.ni, fo);
+                if (!cellw)
+#pragma unroll
+                    for (int v = 0; v < NV; v++) fxe[r][v] = fo[v];
+            }
+        }
+        if (__syncthreads_or(!ok)) break;
+        if (cellw) {
+            // every lane of a cell warp evaluates (inactive lanes on values
+            // that are never stored): only the stores are predicated
+            // The right x face comes from the next lane; lane 31's (face 32
+            // of the row) is sent by lane 0 from the face warp's slot.
+            const double cz = dt / (zn[k] - zn[k - 1]);
+            double *out = rhs + L.at(min(i, ilast), min(j, jlast), k);
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                float send = fo[v];
+                if (tx == 0) send = fxe[ty][v];
+                const float fr = __shfl_sync(0xffffffffu, send, (tx + 1) & (FT_X - 1));
+                double r = ax * ((double)fr - (double)fo[v]);
+                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
+                const double val = r - cz * ((double)qa[v] - (double)qb[v]);
+                if (act) out[v * L.fs] = val;
+                qb[v] = qa[v];
+            }
+        }
+        __syncthreads();
+        if (p + FR_NBUF <= np) {
+            if (tid == 0) issue(p + FR_NBUF);
+            issued++;
+        }
+    }
+    if (p < np) {
+        // a wait ran out: count it, let the copies in flight land, stop
+        if (tid == 0) {
+            atomicAdd(&stat->wait_timeouts, 1ull);
+            for (int pl = p; pl < issued; pl++) tc::mbar_wait(mb_s + 8u * (pl % FR_NBUF), (pl / FR_NBUF) & 1);
+        }
+        __syncthreads();
     }
 }
 

@@ -164,6 +164,23 @@ __device__ __forceinline__ uint32_t gelu_bf16x2(float z0, float z1)
     return h;
 }
 
+// Twice gelu_bf16x2, in one packed operation fewer: h2 = z + z tanh(u).
+// Because halving and doubling are exact in BF16, h2 = 2 gelu_bf16x2(z0, z1)
+// bit for bit; the inference kernel feeds h2 to weights staged at half
+// their value, so every tensor-core product equals the unscaled one.
+__device__ __forceinline__ uint32_t gelu2_bf16x2(float z0, float z1)
+{
+    uint32_t z, z2, a, u, t, h;
+    const uint32_t C1 = 0x3F4C3F4Cu, C3 = 0x3D123D12u, NZ = 0x80008000u;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(z) : "f"(z1), "f"(z0));
+    asm("fma.rn.bf16x2 %0, %1, %1, %2;" : "=r"(z2) : "r"(z), "r"(NZ));
+    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(a) : "r"(z2), "r"(C3), "r"(C1));
+    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(u) : "r"(z), "r"(a), "r"(NZ));
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(u));
+    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(h) : "r"(z), "r"(t), "r"(z));
+    return h;
+}
+
 __device__ __forceinline__ float gelu_grad_f(float z)
 {
     const float c = 0.7978845608028654f, c3 = 0.7978845608028654f * 0.044715f;

@@ -442,15 +442,23 @@ struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
     }
 };
 
-// stage a row-major (R x K) bf16 matrix into the canonical K-major operand layout
+// stage a row-major (R x K) bf16 matrix into the canonical K-major operand
+// layout; half: every weight halved (exact in BF16) for layers fed by
+// gelu2_bf16x2
 __device__ __forceinline__ void sur_stage(unsigned char *dst, const __nv_bfloat16 *src, int R, int K, int tid,
-                                          int nthr)
+                                          int nthr, bool half = false)
 {
     const int vec = K >> 3;
+    const __nv_bfloat162 h2 = __floats2bfloat162_rn(0.5f, 0.5f);
     for (int v = tid; v < R * vec; v += nthr) {
         const int r = v / vec, kk = (v % vec) * 8;
-        *reinterpret_cast<uint4 *>(dst + tc::op_off(R, r, kk)) =
-            *reinterpret_cast<const uint4 *>(src + (size_t)r * K + kk);
+        uint4 w = *reinterpret_cast<const uint4 *>(src + (size_t)r * K + kk);
+        if (half) {
+            __nv_bfloat162 *e = reinterpret_cast<__nv_bfloat162 *>(&w);
+#pragma unroll
+            for (int q = 0; q < 4; q++) e[q] = __hmul2(e[q], h2);
+        }
+        *reinterpret_cast<uint4 *>(dst + tc::op_off(R, r, kk)) = w;
     }
 }
 
@@ -462,8 +470,8 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-// hidden-layer epilogue of one row: 128 accumulators (bias included) -> GELU
-// -> bf16 A tile
+// hidden-layer epilogue of one row: 128 accumulators (bias included) ->
+// 2 GELU -> bf16 A tile (the next layer's weights are staged halved)
 __device__ __forceinline__ void sur_hidden_epilogue(uint32_t tmem_row, unsigned char *A, int row)
 {
 #pragma unroll
@@ -473,10 +481,10 @@ __device__ __forceinline__ void sur_hidden_epilogue(uint32_t tmem_row, unsigned 
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             uint4 w;
-            w.x = gelu_bf16x2(v[8 * q + 0], v[8 * q + 1]);
-            w.y = gelu_bf16x2(v[8 * q + 2], v[8 * q + 3]);
-            w.z = gelu_bf16x2(v[8 * q + 4], v[8 * q + 5]);
-            w.w = gelu_bf16x2(v[8 * q + 6], v[8 * q + 7]);
+            w.x = gelu2_bf16x2(v[8 * q + 0], v[8 * q + 1]);
+            w.y = gelu2_bf16x2(v[8 * q + 2], v[8 * q + 3]);
+            w.z = gelu2_bf16x2(v[8 * q + 4], v[8 * q + 5]);
+            w.w = gelu2_bf16x2(v[8 * q + 6], v[8 * q + 7]);
             *reinterpret_cast<uint4 *>(A + tc::op_off(128, row, c0 + 8 * q)) = w;
         }
     }
@@ -511,9 +519,9 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
     unsigned char *A = sm + SURK_A + g * SURK_ATILE;
 
     sur_stage(sm + SURK_W1, W.Wt[0], SUR_H, SUR_IN, tid, nthr);
-    sur_stage(sm + SURK_W2, W.Wt[1], SUR_H, SUR_H, tid, nthr);
-    sur_stage(sm + SURK_W3, W.Wt[2], SUR_H, SUR_H, tid, nthr);
-    sur_stage(sm + SURK_W4, W.Wt[3], SUR_OUT, SUR_H, tid, nthr);
+    sur_stage(sm + SURK_W2, W.Wt[1], SUR_H, SUR_H, tid, nthr, true);
+    sur_stage(sm + SURK_W3, W.Wt[2], SUR_H, SUR_H, tid, nthr, true);
+    sur_stage(sm + SURK_W4, W.Wt[3], SUR_OUT, SUR_H, tid, nthr, true);
     sur_stage_col(sm + SURK_ONES, nullptr, 128, tid, nthr);
     sur_stage_col(sm + SURK_BB2, W.p + SUR_OFF_B2, SUR_H, tid, nthr);
     sur_stage_col(sm + SURK_BB3, W.p + SUR_OFF_B3, SUR_H, tid, nthr);
@@ -763,8 +771,6 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
     const int lane = threadIdx.x & 31;
     const int total = min((long long)*qu.count, qu.cap);
     const long long fs = a.L.fs;
-    const unsigned qk = a.quirks;
-    const double dt = a.scal[0];
     for (;;) {
         int base = 0;
         if (lane == 0) base = atomicAdd(qu.count + 1, 32);

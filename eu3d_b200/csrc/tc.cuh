@@ -104,6 +104,27 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32
     return false;
 }
 
+// arm an mbarrier for one arrival plus `bytes` of asynchronous copy
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// make mbarrier initialisation visible to the asynchronous (TMA) proxy
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// TMA tiled load of one 4-D box (coordinates innermost first) into shared
+// memory, completing on mbar.  No multicast.  The innermost coordinate x
+// times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const void *tmap, int x, int y, int z, int w, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(dst),
+        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(w), "r"(mbar)
+        : "memory");
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // make generic-proxy shared-memory writes visible to the tensor core (async proxy)

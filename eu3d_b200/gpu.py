@@ -68,7 +68,7 @@ class Status(C.Structure):
                 ("nchem_max", C.c_int), ("substep_capped", C.c_int), ("surrogate_cells", C.c_longlong),
                 ("surrogate_fallback", C.c_longlong), ("dt", C.c_double), ("time", C.c_double),
                 ("surrogate_audited", C.c_longlong), ("surrogate_audit_max_dT", C.c_double),
-                ("surrogate_rejects", C.c_longlong * 4)]
+                ("surrogate_rejects", C.c_longlong * 4), ("wait_timeouts", C.c_longlong)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

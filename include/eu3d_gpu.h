@@ -97,6 +97,8 @@ typedef struct {
     long long surrogate_rejects[4]; /* why cells fell back: outside the envelope, network output
                                        (non-finite, |dT| too large, negative fraction), energy
                                        residual, failed decode */
+    long long wait_timeouts;     /* kernels that gave up a bounded wait on an asynchronous copy
+                                    (their results for that launch are incomplete) */
 } eu3d_status;
 
 const char *eu3d_last_error(void);
@@ -170,9 +172,11 @@ int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time
 int eu3d_synchronize(eu3d_handle *h);
 /* Launch settings picked per handle (new): z planes walked by one flux block,
    adaptive trapezoid on the persistent work queue (1) or one thread per cell
-   (0), resident queue blocks per SM, and (FP32 flux) primitives staged
-   through shared memory (1) or read through L1 (0).  Changing them drops the
-   recorded step graphs. */
+   (0), resident queue blocks per SM, and how the FP32 flux kernel reads the
+   primitives: 2 (default) tile planes brought into a shared-memory ring by
+   TMA, 1 staged into shared memory by loads, 0 read through L1.  flux_stage
+   2 needs the driver's tensor-map encoder and falls back to 1 without it.
+   Changing them drops the recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
