@@ -20,6 +20,11 @@ runs.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
+--gpus N (under torchrun, one rank per GPU): the same case split into N x
+slabs (strong scaling), halos exchanged by NCCL send/recv and dt reduced by
+an all-reduce MIN on each handle's stream (eu3d_b200.slabs); the time is the
+max over ranks and the value counts the whole case's cells.
+
 --impl reference times the reference's own CPU solver (oracle/_ref, the
 reference sources compiled unmodified) on bounded samples of the same
 workload on every host core and prints the same JSON line.
@@ -218,8 +223,11 @@ KERNEL_WORK = {
 
 
 def timed_steps(dev, step, K, W, torch, world, dist, clocks=False, local=0):
+    """K steps timed with CUDA events on the handle's stream (max over ranks).
+    step: a callable (one step) or eu3d_step's keyword arguments."""
+    one = step if callable(step) else (lambda: dev.step(**step))
     for _ in range(W):
-        dev.step(**step)
+        one()
     dev.synchronize()
     stream = torch.cuda.ExternalStream(dev.stream)
     if world > 1:
@@ -231,7 +239,7 @@ def timed_steps(dev, step, K, W, torch, world, dist, clocks=False, local=0):
         clk.__enter__()
     ev0.record(stream)
     for _ in range(K):
-        dev.step(**step)
+        one()
     ev1.record(stream)
     dev.synchronize()
     if clk:
@@ -249,9 +257,10 @@ def timed_steps(dev, step, K, W, torch, world, dist, clocks=False, local=0):
 
 def profiled(dev, step, K):
     """Per-kernel CUDA-event durations over K steps (no graph)."""
+    one = step if callable(step) else (lambda: dev.step(**step))
     dev.profile(True)
     for _ in range(K):
-        dev.step(**step)
+        one()
     prof = dev.profile_read()
     dev.profile(False)
     return prof
@@ -308,29 +317,43 @@ def run_ours(a, rank, world, local):
     from eu3d_b200.cases import extrude_state, setup_odw
     from eu3d_b200.readers import load_h2_ja919
 
+    from eu3d_b200.slabs import DeviceSlab, SlabRun, StepSpec, TorchTransport, slab_extents, slab_grid
+
     torch.cuda.set_device(local)
     ni, nj, nk = (int(x) for x in a.grid.split(","))
     mech = load_h2_ja919()
-    cells = ni * nj * nk
+    cells = ni * nj * nk  # the whole case; N > 1 splits it into x slabs
     model = S.SurrogateModel.load(a.model)
-    d2, case = developed_state(mech, ni, nj, nk, a.develop, seed=rank)
-    dev = gpu.DeviceFlowfield(mech, case.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=a.flux_bits, device=local)
+    d2, case = developed_state(mech, ni, nj, nk, a.develop, seed=0)
+    i0, n_loc = slab_extents(ni, world)[rank] if world > 1 else (0, ni)
+    grid = slab_grid(case.grid, i0, n_loc) if world > 1 else case.grid
+    dev = gpu.DeviceFlowfield(mech, grid, quirks=gpu.QUIRKS_FIXED, flux_bits=a.flux_bits, device=local)
     setup_odw(dev, case)
     dev.set_elements(S.atoms_matrix(mech))
     model.attach(dev, 4099)
 
     def reset():
-        extrude_state(d2, dev)
+        extrude_state(d2, dev, i0=i0)
         dev.set_time(0.0)
         dev.reset_status()
 
     base = dict(type_=0, timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
     forms = {"surrogate": gpu.REACT_SURROGATE, "imex": gpu.REACT_IMEX, "adaptive": gpu.REACT_ADAPTIVE}
+    # N > 1: the slab of this rank, halos by NCCL send/recv and dt by an
+    # all-reduce MIN on the handle's stream (eu3d_b200.slabs); N = 1: eu3d_step
+    run = SlabRun([DeviceSlab(dev, rank, world, wedge=True)], TorchTransport()) if world > 1 else None
+
+    def stepper(step):
+        if run is None:
+            return step
+        spec = StepSpec(**step)
+        return lambda: run.step(spec)
+
     W = max(a.warmup, 3)
     timing, profs, statuses, clocks = {}, {}, {}, None
     for name, react in forms.items():
         reset()
-        step = dict(base, react=react)
+        step = stepper(dict(base, react=react))
         ms, clk = timed_steps(dev, step, a.steps, W, torch, world, dist, clocks=(name == "surrogate"), local=local)
         if clk:
             clocks = clk
@@ -343,23 +366,25 @@ def run_ours(a, rank, world, local):
     launches = sum(v[1] for v in prof.values()) * a.steps // max(a.steps, 1)
     rf = roofline(prof, cells, hbm, tfl, src)
     ms = timing["surrogate"]
-    value = cells * a.steps * world / (ms * 1e-3) / 1e6
-    integ = {k: cells * a.steps * world / (timing[k] * 1e-3) / 1e6 for k in ("imex", "adaptive")}
+    value = cells * a.steps / (ms * 1e-3) / 1e6
+    integ = {k: cells * a.steps / (timing[k] * 1e-3) / 1e6 for k in ("imex", "adaptive")}
     st = statuses["surrogate"]
     tot = st["surrogate_cells"] + st["surrogate_fallback"]
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": W,
-        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "bf16 (network) + f64 (state, decode, fallback integrator)", "data": "synthetic",
         "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge, "
                                f"1 % seeded inflow density perturbation)",
-                   "cells_per_gpu": cells, "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback",
+                   "cells": cells, "cells_per_gpu": n_loc * nj * nk, "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback",
                    "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state",
                    "time": f"SSP-RK2, CFL {CFL}",
                    "state": f"developed: 2D case advanced {a.develop} steps with the FP64 adaptive integrator, "
                             f"extruded along z",
-                   "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
-                   "l2": "state ~12 GB per GPU >> 126 MB L2 (no flush needed)", "graph": "one CUDA graph per step"},
+                   "parallelism": (f"{world} x slabs of {n_loc} cells (NCCL halo send/recv, all-reduce MIN of dt)"
+                                   if world > 1 else "1 GPU"),
+                   "l2": "state ~12 GB per GPU >> 126 MB L2 (no flush needed)",
+                   "graph": "one CUDA graph per step" if world == 1 else "per-op launches (halo exchanges between)"},
         "integrator": {"imex_value": integ["imex"], "adaptive_value": integ["adaptive"],
                        "ratio_vs_imex": value / integ["imex"], "ratio_vs_adaptive": value / integ["adaptive"],
                        "ms_per_step": {k: timing[k] / a.steps for k in timing},
@@ -382,7 +407,7 @@ def run_ours(a, rank, world, local):
         out["accuracy"] = accuracy_2d(mech, model, a.accuracy_steps, cfl=CFL)
     if not a.no_e2e:
         reset()
-        out["e2e"] = run_e2e(dev, dict(base, react=gpu.REACT_SURROGATE), a.steps, cells, torch)
+        out["e2e"] = run_e2e(dev, stepper(dict(base, react=gpu.REACT_SURROGATE)), a.steps, cells, torch, world, dist)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     dev.close()
@@ -390,10 +415,12 @@ def run_ours(a, rank, world, local):
     return out
 
 
-def run_e2e(dev, step, K, cells, torch):
+def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
     """The same metric through the C ABI with host buffers: upload CS, T, E
     from pinned host memory, decode, K steps each followed by a status read,
-    download CS and T -- all inside the timed region."""
+    download CS and T -- all inside the timed region (N > 1: each rank its
+    slab, the time the max over ranks)."""
+    one = step if callable(step) else (lambda: dev.step(**step))
     shapes = {n: dev.shape(n) for n in ("CS", "T", "E")}
     host = {n: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy() for n, s in shapes.items()}
     for n in host:
@@ -406,13 +433,17 @@ def run_e2e(dev, step, K, cells, torch):
         dev.upload(n, host[n])
     dev.update_after_cs()
     for _ in range(K):
-        dev.step(**step)
+        one()
         dev.status()
     dev.download("CS", host["CS"])
     dev.download("T", host["T"])
     ev1.record(stream)
     dev.synchronize()
     ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
     h2d = sum(host[n].nbytes for n in ("CS", "T", "E"))
     d2h = host["CS"].nbytes + host["T"].nbytes + K * 96
     return {"value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
@@ -434,7 +465,7 @@ def run_reference(a, rank, world):
     cb = dict(vals[0])
     cb["value"] = v
     return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "warmup": a.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW), bounded host samples"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -130,15 +130,17 @@ def upload_primitive_state(dev, st: dict) -> None:
 STATE_FIELDS = ("U", "V", "W", "P", "D", "T", "H", "Gamma", "E", "Yi", "CS")
 
 
-def extrude_state(src, dst, k_src: int = None) -> None:
+def extrude_state(src, dst, k_src: int = None, i0: int = 0) -> None:
     """Copy the state of one z plane of handle `src` (default: its first
-    interior plane) into every plane of handle `dst` (same NI, NJ): a
-    spanwise-uniform 3D state from a 2D solution."""
-    if (src.NI, src.NJ) != (dst.NI, dst.NJ):
-        raise ValueError("extrude_state: x-y extents differ")
+    interior plane) into every plane of handle `dst`: a spanwise-uniform 3D
+    state from a 2D solution.  dst takes src's x planes i0 .. i0 + dst.NI - 1
+    (ghosts included; i0 > 0 for an x slab of src's extent) and all of its y
+    extent."""
+    if src.NJ != dst.NJ or i0 < 0 or i0 + dst.NI > src.NI:
+        raise ValueError("extrude_state: extents differ")
     k = src.grid.bc if k_src is None else k_src
     for n in STATE_FIELDS:
-        a = src.download(n)[:, :, k]
+        a = src.download(n)[i0:i0 + dst.NI, :, k]
         b = np.ascontiguousarray(np.broadcast_to(a[:, :, None], (dst.NI, dst.NJ, dst.NK) + a.shape[2:]))
         dst.upload(n, b)
         del b

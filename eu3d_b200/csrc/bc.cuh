@@ -222,7 +222,10 @@ __global__ void k_cfl_partial(Layout L, const P *__restrict__ q, double dx, doub
 
 // dt = cfl * min, clipped so that time + dt does not pass final_time;
 // time += dt (src/Flowfield.cpp:258-271).  scal[0] = dt, scal[1] = time.
-__global__ void k_cfl_final(const double *partial, int nparts, double cfl, double final_time, double *scal)
+// advance: time += dt as well (one rank); 0 leaves time for after the
+// all-ranks minimum of dt (k_advance_time)
+__global__ void k_cfl_final(const double *partial, int nparts, double cfl, double final_time, double *scal,
+                            int advance)
 {
     double m = 1e10;
     for (int t = threadIdx.x; t < nparts; t += blockDim.x) m = fmin(m, partial[t]);
@@ -237,7 +240,41 @@ __global__ void k_cfl_final(const double *partial, int nparts, double cfl, doubl
             double dt = cfl * m;
             if (scal[1] + dt > final_time) dt = final_time - scal[1];
             scal[0] = dt;
-            scal[1] += dt;
+            if (advance) scal[1] += dt;
+        }
+    }
+}
+
+__global__ void k_advance_time(double *scal) { scal[1] += scal[0]; }
+
+// x-slab halo: two x planes of every field the ghost fills write (NPRIM
+// primitives, T, E) over the whole y-z extent, ghost rows included, to or
+// from a contiguous buffer laid out [field][plane][k][j].  The primitives
+// come first in P, then T and E in FP64.  src/Flowfield.cpp:775-1083
+// (Mpi_Boundary) exchanges the same planes field by field.
+template <class P>
+__global__ void k_halo(Layout L, P *__restrict__ q, double *__restrict__ T, double *__restrict__ E,
+                       unsigned char *__restrict__ buf, int i0, int pack)
+{
+    const long long plane = (long long)L.NJ * L.NK;
+    const long long n = 2 * plane;
+    P *bp = reinterpret_cast<P *>(buf);
+    double *bd = reinterpret_cast<double *>(buf + (size_t)NPRIM * n * sizeof(P));
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int p = (int)(t / plane);
+        const long long r = t - p * plane;
+        const int j = (int)(r % L.NJ), k = (int)(r / L.NJ);
+        const long long c = L.at(i0 + p, j, k);
+        if (pack) {
+#pragma unroll
+            for (int f = 0; f < NPRIM; f++) bp[f * n + t] = q[f * L.fs + c];
+            bd[t] = T[c];
+            bd[n + t] = E[c];
+        } else {
+#pragma unroll
+            for (int f = 0; f < NPRIM; f++) q[f * L.fs + c] = bp[f * n + t];
+            T[c] = bd[t];
+            E[c] = bd[n + t];
         }
     }
 }

@@ -413,7 +413,7 @@ struct Spacing {
 };
 
 template <class P>
-void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time)
+void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time, int advance)
 {
     const int use_z = (h->quirks & EU3D_Q_CFL_NO_Z) ? 0 : 1;
     {
@@ -423,17 +423,17 @@ void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time
                                                        h->partial);
     }
     ProfScope ps(h, "cfl_final");
-    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, cfl, final_time, h->scal);
+    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, cfl, final_time, h->scal, advance);
 }
 
 Spacing g_spacing(eu3d_handle *h);
 
-int cfl_op(eu3d_handle *h, double cfl, double final_time, const Spacing &sp)
+int cfl_op(eu3d_handle *h, double cfl, double final_time, const Spacing &sp, int advance = 1)
 {
     if (h->flux_bits == 64)
-        launch_cfl<double>(h, sp, cfl, final_time);
+        launch_cfl<double>(h, sp, cfl, final_time, advance);
     else
-        launch_cfl<float>(h, sp, cfl, final_time);
+        launch_cfl<float>(h, sp, cfl, final_time, advance);
     CK(cudaGetLastError());
     return EU3D_OK;
 }
@@ -647,21 +647,31 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
 
 int sur_chem_op(eu3d_handle *h, bool decoded);  // learned chemistry step, sur_host.cuh
 
-int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
+// The step after the CFL and the first ghost fill, in three parts so that a
+// multi-rank driver can exchange x-slab halos between them (eu3d_step_part):
+// the advection stage (SSP-RK2: stage 1), the second SSP-RK2 stage after its
+// own ghost fill, and the chemistry.
+int stage1_op(eu3d_handle *h, const eu3d_step_desc *s)
 {
     int rc;
-    if (s->cfl != 0 && (rc = cfl_op(h, s->cfl, s->final_time, sp))) return rc;
-    if ((rc = ghost_op(h, s->bc_kind))) return rc;
     if (s->timeadv == EU3D_ADV_SSPRK2) {
         if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
-        if ((rc = cell_op(h, M_RK_STAGE1))) return rc;
-        if ((rc = ghost_op(h, s->bc_kind))) return rc;
-        if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
-        if ((rc = cell_op(h, M_RK_STAGE2))) return rc;
-        CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
-    } else {
-        if ((rc = adv_op(h, s->timeadv, s->diff))) return rc;
+        return cell_op(h, M_RK_STAGE1);
     }
+    return adv_op(h, s->timeadv, s->diff);
+}
+
+int stage2_op(eu3d_handle *h, const eu3d_step_desc *s)
+{
+    int rc;
+    if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
+    if ((rc = cell_op(h, M_RK_STAGE2))) return rc;
+    CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
+    return EU3D_OK;
+}
+
+int react_op(eu3d_handle *h, const eu3d_step_desc *s)
+{
     switch (s->react) {
     case EU3D_REACT_IMEX: return cell_op(h, M_IMEX);
     case EU3D_REACT_TRAPEZOID: return cell_op(h, s->type == 0 ? M_TRAP0 : M_TRAP1);
@@ -678,6 +688,19 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
     }
     default: return fail(EU3D_ERR_ARG, "unsupported reaction scheme for eu3d_step");
     }
+}
+
+int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
+{
+    int rc;
+    if (s->cfl != 0 && (rc = cfl_op(h, s->cfl, s->final_time, sp))) return rc;
+    if ((rc = ghost_op(h, s->bc_kind))) return rc;
+    if ((rc = stage1_op(h, s))) return rc;
+    if (s->timeadv == EU3D_ADV_SSPRK2) {
+        if ((rc = ghost_op(h, s->bc_kind))) return rc;
+        if ((rc = stage2_op(h, s))) return rc;
+    }
+    return react_op(h, s);
 }
 
 }  // namespace
@@ -1107,6 +1130,90 @@ int eu3d_cfl(eu3d_handle *h, double cfl, double final_time, double *dt_out)
     return dt_out ? eu3d_get_dt(h, dt_out) : EU3D_OK;
 }
 
+// ------------------------------------------------------- x-slab decomposition
+// A multi-rank run splits the x extent into slabs, one handle per rank, and
+// replaces Flowfield::Mpi_Boundary (src/Flowfield.cpp:775-1083) and the
+// MPI_Reduce/Bcast of CFLcondition (:242-272) with these calls around a
+// collective library of the caller's choice (NCCL over NVLink).
+
+int eu3d_halo_bytes(eu3d_handle *h, long long *bytes)
+{
+    if (!h || !bytes) return fail(EU3D_ERR_ARG, "null argument");
+    const long long n = 2LL * h->L.NJ * h->L.NK;
+    *bytes = n * (NPRIM * (long long)prim_bytes(h) + 2 * (long long)sizeof(double));
+    return EU3D_OK;
+}
+
+namespace {
+int halo_op(eu3d_handle *h, int side, int overlap, void *buf, int pack)
+{
+    if (!h || !buf) return fail(EU3D_ERR_ARG, "null argument");
+    if (side != 0 && side != 1) return fail(EU3D_ERR_ARG, "side must be 0 (low x) or 1 (high x)");
+    if (overlap != 0 && overlap != 1) return fail(EU3D_ERR_ARG, "overlap must be 0 or 1");
+    if (h->L.ni < 2 + overlap) return fail(EU3D_ERR_ARG, "slab narrower than the planes it sends");
+    if ((uintptr_t)buf % 16) return fail(EU3D_ERR_ARG, "halo buffer must be 16-byte aligned");
+    const Layout &L = h->L;
+    // packed: the two interior planes next to the face (past the shared
+    // node when overlap = 1); unpacked: the face's two ghost planes
+    const int i0 = pack ? (side == 0 ? L.bc + overlap : L.ni + L.bc - 2 - overlap) : (side == 0 ? 0 : L.ni + L.bc);
+    const long long n = 2LL * L.NJ * L.NK;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+    ProfScope ps(h, pack ? "halo_pack" : "halo_unpack");
+    if (h->flux_bits == 64)
+        k_halo<double><<<blocks, 256, 0, h->st>>>(L, (double *)h->prim, h->T, h->E, (unsigned char *)buf, i0, pack);
+    else
+        k_halo<float><<<blocks, 256, 0, h->st>>>(L, (float *)h->prim, h->T, h->E, (unsigned char *)buf, i0, pack);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+}  // namespace
+
+int eu3d_halo_pack(eu3d_handle *h, int side, int overlap, void *dst) { return halo_op(h, side, overlap, dst, 1); }
+int eu3d_halo_unpack(eu3d_handle *h, int side, const void *src)
+{
+    return halo_op(h, side, 0, const_cast<void *>(src), 0);
+}
+
+int eu3d_cfl_local(eu3d_handle *h, double cfl, double final_time)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    return cfl_op(h, cfl, final_time, g_spacing(h), 0);
+}
+
+double *eu3d_dt_device(eu3d_handle *h) { return h ? h->scal : nullptr; }
+
+int eu3d_advance_time(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    k_advance_time<<<1, 1, 0, h->st>>>(h->scal);
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+int eu3d_wedge_fill(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    return ghost_op(h, EU3D_BC_NONE);
+}
+
+namespace {
+int prepare_step(eu3d_handle *h, const eu3d_step_desc *s);
+}
+
+int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part)
+{
+    int rc = prepare_step(h, s);
+    if (rc) return rc;
+    switch (part) {
+    case EU3D_PART_STAGE1: return stage1_op(h, s);
+    case EU3D_PART_STAGE2:
+        if (s->timeadv != EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "stage 2 exists for SSP-RK2 only");
+        return stage2_op(h, s);
+    case EU3D_PART_REACT: return react_op(h, s);
+    default: return fail(EU3D_ERR_ARG, "unknown step part");
+    }
+}
+
 int eu3d_boundary(eu3d_handle *h, int kind)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
@@ -1133,7 +1240,10 @@ int eu3d_react_trapezoid(eu3d_handle *h, int type)
     return cell_op(h, type == 0 ? M_TRAP0 : M_TRAP1);
 }
 
-int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
+namespace {
+// argument and state checks of a step, and the buffers it needs (the SSP-RK2
+// stage copy, the trapezoid work queue), for eu3d_step and eu3d_step_part
+int prepare_step(eu3d_handle *h, const eu3d_step_desc *s)
 {
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "unknown time scheme");
@@ -1145,11 +1255,20 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
         return fail(EU3D_ERR_STATE, "element composition not set (eu3d_set_elements)");
     if (s->react == EU3D_REACT_SURROGATE && !h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached");
     if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
+    CK(cudaSetDevice(h->dev));
     if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
     if (s->react == EU3D_REACT_TRAPEZOID && s->type == 1 && h->chem_queue) {
         int rc = ensure_queue(h);
         if (rc) return rc;
     }
+    return EU3D_OK;
+}
+}  // namespace
+
+int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s)
+{
+    int prc = prepare_step(h, s);
+    if (prc) return prc;
     if (h->profile) return enqueue_step(h, s, g_spacing(h));
     StepKey key{s->react, s->type, s->timeadv, s->diff, s->bc_kind, s->cfl, s->final_time};
     auto it = h->graphs.find(key);

@@ -40,7 +40,11 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_sur_get_dataset", "eu3d_sur_set_norm", "eu3d_sur_get_norm", "eu3d_sur_set_params",
            "eu3d_sur_get_params", "eu3d_sur_train", "eu3d_sur_loss_grad", "eu3d_sur_predict", "eu3d_sur_infer",
            "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune",
-           "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive"]
+           "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive", "eu3d_halo_bytes", "eu3d_halo_pack",
+           "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
+           "eu3d_step_part"]
+
+PART_STAGE1, PART_STAGE2, PART_REACT = 0, 1, 2
 
 SUR_NPARAM = 37264
 SUR_NORM_LEN = 80
@@ -149,12 +153,21 @@ def load_library(path: Optional[str] = None):
     L.eu3d_set_tuning.argtypes = h + [C.POINTER(Tuning)]
     L.eu3d_get_tuning.argtypes = h + [C.POINTER(Tuning)]
     L.eu3d_autotune.argtypes = h + [C.POINTER(StepDesc), C.c_int, C.POINTER(Tuning), _dp]
+    L.eu3d_halo_bytes.argtypes = h + [C.POINTER(C.c_longlong)]
+    L.eu3d_halo_pack.argtypes = h + [C.c_int, C.c_int, C.c_void_p]
+    L.eu3d_halo_unpack.argtypes = h + [C.c_int, C.c_void_p]
+    L.eu3d_cfl_local.argtypes = h + [C.c_double, C.c_double]
+    L.eu3d_dt_device.argtypes = h
+    L.eu3d_advance_time.argtypes = h
+    L.eu3d_wedge_fill.argtypes = h
+    L.eu3d_step_part.argtypes = h + [C.POINTER(StepDesc), C.c_int]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]
     for fn in EXPORTS:
-        if fn not in ("eu3d_last_error", "eu3d_stream"):
+        if fn not in ("eu3d_last_error", "eu3d_stream", "eu3d_dt_device"):
             getattr(L, fn).restype = C.c_int
+    L.eu3d_dt_device.restype = C.c_void_p
     if path is None:
         _LIB = L
     return L
@@ -177,6 +190,7 @@ class DeviceFlowfield:
     def __init__(self, mech, grid, quirks: int = QUIRKS_FIXED, flux_bits: int = 64, device: int = 0):
         self.L = load_library()
         self.mech, self.grid = mech, grid
+        self.device = device
         self.NS = mech.NS
         self.NI, self.NJ, self.NK = grid.ni + 2 * grid.bc, grid.nj + 2 * grid.bc, grid.nk + 2 * grid.bc
         keep = []
@@ -259,6 +273,10 @@ class DeviceFlowfield:
     def set_time(self, t: float):
         _check(self.L.eu3d_set_time(self.h, t))
 
+    @property
+    def time(self) -> float:
+        return self.status()["time"]
+
     def cfl(self, cfl: float, final_time: float) -> float:
         v = C.c_double()
         _check(self.L.eu3d_cfl(self.h, cfl, final_time, C.byref(v)))
@@ -315,6 +333,42 @@ class DeviceFlowfield:
 
     def synchronize(self):
         _check(self.L.eu3d_synchronize(self.h))
+
+    # ---- x-slab decomposition (one handle per rank; eu3d_b200.slabs drives them)
+    def halo_bytes(self) -> int:
+        n = C.c_longlong()
+        _check(self.L.eu3d_halo_bytes(self.h, C.byref(n)))
+        return n.value
+
+    def halo_pack(self, side: int, dst_ptr: int, overlap: int = 0):
+        """Pack the two interior planes next to face `side` (0 low x, 1 high x;
+        overlap 1: past a node shared with the neighbour) into the device
+        buffer at dst_ptr (eu3d_halo_bytes bytes)."""
+        _check(self.L.eu3d_halo_pack(self.h, side, overlap, C.c_void_p(dst_ptr)))
+
+    def halo_unpack(self, side: int, src_ptr: int):
+        """Fill the two ghost planes of face `side` from the device buffer at src_ptr."""
+        _check(self.L.eu3d_halo_unpack(self.h, side, C.c_void_p(src_ptr)))
+
+    def cfl_local(self, cfl: float, final_time: float):
+        """This rank's CFL dt into the device scalar (time not advanced)."""
+        _check(self.L.eu3d_cfl_local(self.h, cfl, final_time))
+
+    @property
+    def dt_device_ptr(self) -> int:
+        """Device address of dt (one FP64), for an in-place all-reduce MIN."""
+        return self.L.eu3d_dt_device(self.h)
+
+    def advance_time(self):
+        _check(self.L.eu3d_advance_time(self.h))
+
+    def wedge_fill(self):
+        _check(self.L.eu3d_wedge_fill(self.h))
+
+    def step_part(self, part: int, react=REACT_IMEX, type_=0, timeadv=ADV_EE, diff=DIFF_MUSCL2, bc_kind=BC_RSBI,
+                  cfl=0.0, final_time=1.0):
+        s = StepDesc(react, type_, timeadv, diff, bc_kind, cfl, final_time)
+        _check(self.L.eu3d_step_part(self.h, C.byref(s), part))
 
     def tuning(self) -> dict:
         t = Tuning()

@@ -170,6 +170,42 @@ int eu3d_step(eu3d_handle *h, const eu3d_step_desc *s);
    after each step only when check_time is nonzero). */
 int eu3d_run(eu3d_handle *h, const eu3d_step_desc *s, int nsteps, int check_time);
 int eu3d_synchronize(eu3d_handle *h);
+/* x-slab decomposition (replaces Flowfield::Mpi_Boundary, src/Flowfield.cpp:775-1083,
+   and the MPI_Reduce/MPI_Bcast of dt in CFLcondition, :242-272).  One handle per rank
+   holds a slab of the x extent; the caller moves the buffers between ranks with its
+   collective library (NCCL send/recv over NVLink) on the handle's stream (eu3d_stream).
+   A step of a rank, as eu3d_step does it on one rank:
+     eu3d_cfl_local; all-reduce MIN of the double at eu3d_dt_device across ranks;
+     eu3d_advance_time;
+     eu3d_boundary; halo exchange; [wedge set: eu3d_wedge_fill; halo exchange];
+     eu3d_step_part(STAGE1);
+     SSP-RK2: eu3d_boundary; halo exchange; [wedge ...]; eu3d_step_part(STAGE2);
+     eu3d_step_part(REACT).
+   Halo exchange: eu3d_halo_pack(side) into a device buffer of eu3d_halo_bytes bytes,
+   send it to the neighbour on that side, receive the neighbour's buffer and
+   eu3d_halo_unpack(side) it.  Side 0 is the low-x face, 1 the high-x face; a pack
+   takes the two interior planes next to the face, an unpack fills the face's two
+   ghost planes (all y and z, ghosts included; primitives, T and E).  overlap 0:
+   slabs partition the cells; overlap 1: neighbouring slabs share their end node, as
+   the reference's mesh blocks do (src/Mesh.cpp:77-93), and the pack skips it
+   (Mpi_Boundary sends planes bc+1, bc+2 and ni-1, ni).  Buffers are device memory,
+   16-byte aligned. */
+int eu3d_halo_bytes(eu3d_handle *h, long long *bytes);
+int eu3d_halo_pack(eu3d_handle *h, int side, int overlap, void *dst);
+int eu3d_halo_unpack(eu3d_handle *h, int side, const void *src);
+/* CFLcondition without the time update: the rank's dt (clipped to final_time) into
+   the device scalar at eu3d_dt_device; eu3d_advance_time then adds it to time. */
+int eu3d_cfl_local(eu3d_handle *h, double cfl, double final_time);
+double *eu3d_dt_device(eu3d_handle *h);
+int eu3d_advance_time(eu3d_handle *h);
+/* the immersed-wedge ghost band alone (eu3d_boundary runs it after the faces) */
+int eu3d_wedge_fill(eu3d_handle *h);
+/* the parts of eu3d_step after its CFL and first ghost fill */
+#define EU3D_PART_STAGE1 0 /* advection (SSP-RK2: with the stage-1 update and decode) */
+#define EU3D_PART_STAGE2 1 /* SSP-RK2 stage 2: advection, update, decode */
+#define EU3D_PART_REACT 2  /* chemistry */
+int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
+
 /* Launch settings picked per handle (new): z planes walked by one flux block,
    adaptive trapezoid on the persistent work queue (1) or one thread per cell
    (0), resident queue blocks per SM, and how the FP32 flux kernel reads the

@@ -1,0 +1,137 @@
+"""x-slab decomposition on the GPU: slabs of one flowfield, each its own
+handle, stepped through eu3d_b200.slabs (halo pack/unpack kernels, local CFL
+and time update, the parts of eu3d_step) with the in-process loopback
+transport give the single-domain CUDA-graph step's result bit for bit.
+Flowfield::Mpi_Boundary, src/Flowfield.cpp:775-1083."""
+import numpy as np
+import pytest
+
+from _slab_cases import dyadic_grid
+from eu3d_b200 import gpu
+from eu3d_b200 import surrogate as S
+from eu3d_b200.cases import STATE_FIELDS, odw_case, setup_odw
+from eu3d_b200.slabs import DeviceSlab, LoopbackTransport, SlabRun, StepSpec, slab_extents, slab_grid
+
+pytestmark = pytest.mark.gpu
+
+
+def _cut(full, mech, grid, nranks, layout, flux_bits, setup=None):
+    out = []
+    for i0, n in slab_extents(grid.ni, nranks, layout):
+        d = gpu.DeviceFlowfield(mech, slab_grid(grid, i0, n), gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+        if setup:
+            setup(d)
+        for f in STATE_FIELDS:
+            d.upload(f, full.download(f)[i0:i0 + n + 2 * grid.bc])
+        d.dt = full.dt
+        d.set_time(full.time)
+        d.synchronize()
+        out.append((i0, n, d))
+    return out
+
+
+def _compare(full, pieces, bc=2, names=("CS", "T", "P", "Yi")):
+    ref = {f: full.download(f) for f in names}
+    for i0, n, d in pieces:
+        for f in names:
+            a = d.download(f)[bc:-bc, bc:-bc, bc:-bc]
+            b = ref[f][bc:-bc, bc:-bc, bc:-bc][i0:i0 + n]
+            assert np.all(np.isfinite(b)), f
+            assert np.array_equal(a, b), (f, i0, n, float(np.max(np.abs(a - b))))
+        assert d.dt == full.dt and d.time == full.time
+        assert d.status()["wait_timeouts"] == 0
+
+
+@pytest.mark.parametrize("nranks,layout,flux_bits,timeadv", [
+    (3, "partition", 64, gpu.ADV_EE),
+    (2, "partition", 32, gpu.ADV_SSPRK2),
+    (3, "reference", 32, gpu.ADV_SSPRK2),
+])
+def test_rsbi_slabs_equal_single_domain(mech, nranks, layout, flux_bits, timeadv):
+    from _cases import fill_state
+    from pyoracle import Oracle
+    ni = 97 if layout == "reference" else 96
+    g = dyadic_grid(ni, 20, 9)
+    o = Oracle(mech, g, gpu.QUIRKS_FIXED)
+    fill_state(o, 7, 1100.0, 2600.0)
+    full = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+    full.upload_state(o)
+    full.dt = 1e-8
+    pieces = _cut(full, mech, g, nranks, layout, flux_bits)
+    spec = StepSpec(react=gpu.REACT_IMEX, timeadv=timeadv, bc_kind=gpu.BC_RSBI, cfl=0.5, final_time=1.0)
+    slabs = [DeviceSlab(d, r, nranks, overlap=1 if layout == "reference" else 0) for r, (_, _, d) in enumerate(pieces)]
+    run = SlabRun(slabs, LoopbackTransport())
+    for _ in range(3):
+        full.step(**spec.kw())
+        run.step(spec)
+    full.synchronize()
+    for _, _, d in pieces:
+        d.synchronize()
+    _compare(full, pieces)
+
+
+@pytest.mark.parametrize("react", [gpu.REACT_IMEX, gpu.REACT_SURROGATE])
+def test_odw_wedge_slabs_equal_single_domain(mech, react):
+    """Inflow / wall x faces on the end slabs only, the immersed wedge across
+    every slab face (band refilled after the exchange), SSP-RK2, FP32 flux;
+    with the learned chemistry and its FP64 fallback as well."""
+    case = odw_case(mech, 128, 48, 6, L=0.05)
+    model = S.SurrogateModel.load(S.DEFAULT_MODEL) if react == gpu.REACT_SURROGATE else None
+
+    def setup(d):
+        setup_odw(d, case)
+        if model is not None:
+            d._model_sur = model.attach(d, 0)
+
+    full = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=32)
+    setup(full)
+    spec = StepSpec(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0, final_time=1.0)
+    full.dt = 4e-8
+    # develop a flow with the wedge shock first (one domain), then split it
+    for _ in range(30):
+        full.step(**spec.kw())
+    full.synchronize()
+    pieces = _cut(full, mech, case.grid, 3, "partition", 32, setup)
+    spec.react = react
+    slabs = [DeviceSlab(d, r, 3, wedge=True) for r, (_, _, d) in enumerate(pieces)]
+    run = SlabRun(slabs, LoopbackTransport())
+    for _ in range(4):
+        full.step(**spec.kw())
+        run.step(spec)
+    full.synchronize()
+    for _, _, d in pieces:
+        d.synchronize()
+    _compare(full, pieces)
+    if react == gpu.REACT_SURROGATE:
+        assert sum(d.status()["surrogate_cells"] for _, _, d in pieces) == full.status()["surrogate_cells"]
+
+
+def test_halo_pack_unpack_roundtrip(mech):
+    """pack(side) of one slab unpacked into the other side's ghosts of a copy
+    puts exactly the planes next to the face there (all fields, ghost rows
+    included); overlap 1 skips the shared end plane."""
+    from _cases import fill_state
+    from pyoracle import Oracle
+    g = dyadic_grid(12, 6, 5)
+    o = Oracle(mech, g, gpu.QUIRKS_FIXED)
+    fill_state(o, 11, 900.0, 2000.0)
+    import torch
+    for bits in (32, 64):
+        a = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=bits)
+        a.upload_state(o)
+        buf = torch.empty(a.halo_bytes(), dtype=torch.uint8, device="cuda")
+        for overlap in (0, 1):
+            for side in (0, 1):
+                a.halo_pack(side, buf.data_ptr(), overlap)
+                b = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=bits)
+                b.upload_state(o)
+                b.halo_unpack(1 - side, buf.data_ptr())
+                b.synchronize()
+                src = slice(2 + overlap, 4 + overlap) if side == 0 else slice(g.ni - overlap, g.ni + 2 - overlap)
+                dst = slice(g.ni + 2, g.ni + 4) if side == 0 else slice(0, 2)
+                for f in ("D", "U", "P", "T", "E", "H", "Gamma", "Yi"):
+                    assert np.array_equal(b.download(f)[dst], a.download(f)[src]), (bits, overlap, side, f)
+                b.close()
+        a.close()
+    with pytest.raises(gpu.Eu3dError):
+        gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED).halo_pack(2, buf.data_ptr())
