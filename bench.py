@@ -217,7 +217,9 @@ KERNEL_WORK = {
     # MLP 12 -> 3 x 128 -> 10 forward: 2 (16 128 + 2 128 128 + 128 16) FLOP
     "sur_mlp": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
     "cell_imex": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
-    "cell_rk1": ("hbm", 13 * 8 * 4 + 2 * 8 * 2 + 16 * 4),
+    # stage 1: CS^n and RHS in, the stage state out (CS^n stays in place)
+    "cell_rk1": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
+    # stage 2: CS^n, the stage state and RHS in, CS out
     "cell_rk2": ("hbm", 13 * 8 * 4 + 2 * 8 * 2 + 16 * 4),
 }
 

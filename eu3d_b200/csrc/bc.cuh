@@ -182,61 +182,116 @@ __global__ void k_wedge_band(GhostArgs a, P *q, const int4 *__restrict__ band, i
 // CFL: block minima of min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C)]) over the
 // interior (solid wedge cells excluded), C = sqrt(Gamma P / D) as the decode
 // defines it.
+// CFLcondition (src/Flowfield.cpp:242-272) as block maxima: because IEEE
+// division is monotone in the divisor, the smallest dx / (|U| + C) over the
+// cells is dx over the largest |U| + C, bit for bit; so each block keeps the
+// largest |U| + C, |V| + C, |W| + C of its cells and k_cfl_final divides
+// once.  A cell whose x time is NaN is skipped, as the reference's
+// comparisons skip it; NaN y or z times drop out of fmax as they drop out of
+// the reference's min.  One warp walks one (j, k) row of interior cells.
 template <class P>
-__global__ void k_cfl_partial(Layout L, const P *__restrict__ q, double dx, double dy, double dz, int use_z,
-                              const double *xn, const double *yn, double x0, double y0, double tn, int wedge_on,
-                              double *partial)
+__global__ void k_cfl_partial(Layout L, const P *__restrict__ q, int use_z, const double *__restrict__ xn,
+                              const double *__restrict__ yn, double x0, double y0, double tn, int wedge_on,
+                              double *__restrict__ partial)
 {
-    const long long n = L.interior_cells();
-    double m = 1e10;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int i = L.bc + (int)(t % L.ni);
-        const int j = L.bc + (int)((t / L.ni) % L.nj);
-        const int k = L.bc + (int)(t / ((long long)L.ni * L.nj));
-        if (wedge_on) {
-            const double x = xn[i], y = yn[j];
-            if (x > x0 && (y - y0) < (x - x0) * tn) continue;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int rows = L.nj * L.nk;
+    const long long fs = L.fs;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int r = blockIdx.x * wpb + wid; r < rows; r += gridDim.x * wpb) {
+        const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
+        const double y = yn[j];
+        const long long base = L.at(0, j, k);
+        for (int i = L.bc + lane; i < L.ni + L.bc; i += 32) {
+            if (wedge_on) {
+                const double x = xn[i];
+                if (x > x0 && (y - y0) < (x - x0) * tn) continue;
+            }
+            const long long c = base + i;
+            const double D = (double)q[PD * fs + c], Pp = (double)q[PP * fs + c], G = (double)q[PG * fs + c];
+            const double C = sqrt(G * Pp / D);
+            const double ax = fabs((double)q[PU * fs + c]) + C;
+            if (isnan(ax)) continue;
+            sx = fmax(sx, ax);
+            sy = fmax(sy, fabs((double)q[PV * fs + c]) + C);
+            if (use_z) sz = fmax(sz, fabs((double)q[PW * fs + c]) + C);
         }
-        const long long c = L.at(i, j, k);
-        const long long fs = L.fs;
-        const double D = (double)q[PD * fs + c], Pp = (double)q[PP * fs + c], G = (double)q[PG * fs + c];
-        const double C = sqrt(G * Pp / D);
-        const double a = dx / (fabs((double)q[PU * fs + c]) + C), b = dy / (fabs((double)q[PV * fs + c]) + C);
-        double tmp = (b < a) ? b : a;
-        if (use_z) {
-            const double z = dz / (fabs((double)q[PW * fs + c]) + C);
-            tmp = (z < tmp) ? z : tmp;
-        }
-        if (tmp < m) m = tmp;
     }
-    __shared__ double sm[32];
-    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __shared__ double sm[3][32];
+    for (int o = 16; o > 0; o >>= 1) {
+        sx = fmax(sx, __shfl_down_sync(0xffffffffu, sx, o));
+        sy = fmax(sy, __shfl_down_sync(0xffffffffu, sy, o));
+        sz = fmax(sz, __shfl_down_sync(0xffffffffu, sz, o));
+    }
+    if (lane == 0) {
+        sm[0][wid] = sx;
+        sm[1][wid] = sy;
+        sm[2][wid] = sz;
+    }
     __syncthreads();
     if (threadIdx.x < 32) {
-        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
-        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
-        if (threadIdx.x == 0) partial[blockIdx.x] = m;
+        sx = lane < wpb ? sm[0][lane] : 0.0;
+        sy = lane < wpb ? sm[1][lane] : 0.0;
+        sz = lane < wpb ? sm[2][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            sx = fmax(sx, __shfl_down_sync(0xffffffffu, sx, o));
+            sy = fmax(sy, __shfl_down_sync(0xffffffffu, sy, o));
+            sz = fmax(sz, __shfl_down_sync(0xffffffffu, sz, o));
+        }
+        if (lane == 0) {
+            partial[3 * blockIdx.x + 0] = sx;
+            partial[3 * blockIdx.x + 1] = sy;
+            partial[3 * blockIdx.x + 2] = sz;
+        }
     }
 }
 
-// dt = cfl * min, clipped so that time + dt does not pass final_time;
-// time += dt (src/Flowfield.cpp:258-271).  scal[0] = dt, scal[1] = time.
 // advance: time += dt as well (one rank); 0 leaves time for after the
-// all-ranks minimum of dt (k_advance_time)
-__global__ void k_cfl_final(const double *partial, int nparts, double cfl, double final_time, double *scal,
-                            int advance)
+// all-ranks minimum of dt (k_advance_time).  dt_conv starts at 1e10 as in the
+// reference, so a domain without fluid cells gets cfl * 1e10.
+__global__ void k_cfl_final(const double *partial, int nparts, double dx, double dy, double dz, int use_z, double cfl,
+                            double final_time, double *scal, int advance)
 {
-    double m = 1e10;
-    for (int t = threadIdx.x; t < nparts; t += blockDim.x) m = fmin(m, partial[t]);
-    __shared__ double sm[32];
-    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int t = threadIdx.x; t < nparts; t += blockDim.x) {
+        sx = fmax(sx, partial[3 * t + 0]);
+        sy = fmax(sy, partial[3 * t + 1]);
+        sz = fmax(sz, partial[3 * t + 2]);
+    }
+    __shared__ double sm[3][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        sx = fmax(sx, __shfl_down_sync(0xffffffffu, sx, o));
+        sy = fmax(sy, __shfl_down_sync(0xffffffffu, sy, o));
+        sz = fmax(sz, __shfl_down_sync(0xffffffffu, sz, o));
+    }
+    if (lane == 0) {
+        sm[0][wid] = sx;
+        sm[1][wid] = sy;
+        sm[2][wid] = sz;
+    }
     __syncthreads();
     if (threadIdx.x < 32) {
-        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 1e10;
-        for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+        const int nw = blockDim.x >> 5;
+        sx = lane < nw ? sm[0][lane] : 0.0;
+        sy = lane < nw ? sm[1][lane] : 0.0;
+        sz = lane < nw ? sm[2][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            sx = fmax(sx, __shfl_down_sync(0xffffffffu, sx, o));
+            sy = fmax(sy, __shfl_down_sync(0xffffffffu, sy, o));
+            sz = fmax(sz, __shfl_down_sync(0xffffffffu, sz, o));
+        }
         if (threadIdx.x == 0) {
+            // the smallest of dx/sx, dy/sy (and dz/sz); a zero speed gives an
+            // infinite time, which the reference's 1e10 start caps
+            double m = 1e10;
+            const double a = dx / sx, b = dy / sy;
+            if (a < m) m = a;
+            if (b < m) m = b;
+            if (use_z) {
+                const double z = dz / sz;
+                if (z < m) m = z;
+            }
             double dt = cfl * m;
             if (scal[1] + dt > final_time) dt = final_time - scal[1];
             scal[0] = dt;

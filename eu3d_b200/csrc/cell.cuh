@@ -634,15 +634,16 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
     } else if (MODE == M_RK_STAGE1 || MODE == M_RK_STAGE2) {
+        // Stage 1 leaves CS^n where it is and puts the stage state
+        // CS^n + R(q^n) into cs0; stage 2 forms 0.5 CS^n + 0.5 (CS1 + R(q1))
+        // back into cs.  No copy of CS^n is made.
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             const double r = a.rhs[v * fs + c];
-            if (MODE == M_RK_STAGE1) {
-                a.cs0[v * fs + c] = cs[v];
+            if (MODE == M_RK_STAGE1)
                 cs[v] = cs[v] + r;
-            } else {
-                cs[v] = 0.5 * a.cs0[v * fs + c] + 0.5 * (cs[v] + r);
-            }
+            else
+                cs[v] = 0.5 * cs[v] + 0.5 * (a.cs0[v * fs + c] + r);
         }
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
@@ -723,7 +724,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
             atomicAdd(&a.st->substeps, (unsigned long long)n);
         }
     }
-    store_cs(a.cs, fs, c, cs);
+    store_cs(MODE == M_RK_STAGE1 ? a.cs0 : a.cs, fs, c, cs);
     a.T[c] = o.T;
     a.E[c] = o.E;
     store_prims<P>(o, q, fs, c);

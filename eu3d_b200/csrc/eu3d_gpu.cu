@@ -418,12 +418,12 @@ void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time
     const int use_z = (h->quirks & EU3D_Q_CFL_NO_Z) ? 0 : 1;
     {
         ProfScope ps(h, "cfl_partial");
-        k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, sp.dx, sp.dy, sp.dz, use_z, h->xn,
-                                                       h->yn, h->wedge[0], h->wedge[1], h->wedge[2], h->wedge_on,
-                                                       h->partial);
+        k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, use_z, h->xn, h->yn, h->wedge[0],
+                                                       h->wedge[1], h->wedge[2], h->wedge_on, h->partial);
     }
     ProfScope ps(h, "cfl_final");
-    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, cfl, final_time, h->scal, advance);
+    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, sp.dx, sp.dy, sp.dz, use_z, cfl, final_time, h->scal,
+                                       advance);
 }
 
 Spacing g_spacing(eu3d_handle *h);
@@ -863,7 +863,7 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     ALLOC(h->zn, L.NK * sizeof(double));
     ALLOC(h->scal, 8 * sizeof(double));
     h->nparts = 148 * 4;
-    ALLOC(h->partial, h->nparts * sizeof(double));
+    ALLOC(h->partial, 3 * h->nparts * sizeof(double));  // per block: largest |U|+C, |V|+C, |W|+C
     ALLOC(h->status, sizeof(Status));
 #undef ALLOC
     cudaMemsetAsync(h->cs, 0, NV * f8, h->st);

@@ -201,7 +201,8 @@ int eu3d_advance_time(eu3d_handle *h);
 /* the immersed-wedge ghost band alone (eu3d_boundary runs it after the faces) */
 int eu3d_wedge_fill(eu3d_handle *h);
 /* the parts of eu3d_step after its CFL and first ghost fill */
-#define EU3D_PART_STAGE1 0 /* advection (SSP-RK2: with the stage-1 update and decode) */
+#define EU3D_PART_STAGE1 0 /* advection (SSP-RK2: with the stage-1 update and decode; the stage's
+                              conserved state is held apart and CS keeps CS^n until STAGE2) */
 #define EU3D_PART_STAGE2 1 /* SSP-RK2 stage 2: advection, update, decode */
 #define EU3D_PART_REACT 2  /* chemistry */
 int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
