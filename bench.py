@@ -216,6 +216,8 @@ KERNEL_WORK = {
     "sur_apply": ("hbm", 13 * 8 + 16 + 40 + 9 * 8 + 16 + 16 * 4),
     # MLP 12 -> 3 x 128 -> 10 forward: 2 (16 128 + 2 128 128 + 128 16) FLOP
     "sur_mlp": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
+    # the network and its apply in one kernel: the network's FLOPs
+    "sur_mlp_apply": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
     "cell_imex": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
     # stage 1: CS^n and RHS in, the stage state out (CS^n stays in place)
     "cell_rk1": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),

@@ -376,6 +376,36 @@ struct AdaptCfg {
     int nmax;
 };
 
+// One substep of chem_adaptive: cs, T advance by h, the time left trem
+// shrinks by h, the count k grows by one.
+template <bool SPEC>
+__device__ __forceinline__ void adapt_substep(double cs[NV], double &T, double Eold, unsigned qk, double &trem, int &k,
+                                              double hmin, const AdaptCfg &cfg, Decoded &o, int &capped_any)
+{
+    double CMS[NS], MD[NS];
+    imex_source<SPEC>(cs, T, qk, CMS, MD, false);
+    double D = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; s++) D += cs[s];
+    double h = trem;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const double w = fabs(CMS[s]);
+        if (w > 0.0) h = fmin(h, cfg.rel * (cs[s] + 1e-9 * D) / w);
+        if (MD[s] > 0.0) h = fmin(h, cfg.amp / MD[s]);
+    }
+    h = fmin(fmax(h, hmin), trem);
+    if (k == cfg.nmax - 1) h = trem;
+#pragma unroll
+    for (int s = 0; s < NS; s++) cs[s] = fmax(cs[s] + h * CMS[s] / (1.0 - h * MD[s]), 0.0);
+    int cp = 0;
+    decode(cs, T, Eold, qk, o, cp);
+    capped_any |= cp;
+    T = o.T;
+    trem -= h;
+    k++;
+}
+
 template <bool SPEC>
 __device__ __forceinline__ int chem_adaptive(double cs[NV], double &T, double Eold, unsigned qk, double dt,
                                              const AdaptCfg &cfg, int &capped_any)
@@ -384,30 +414,7 @@ __device__ __forceinline__ int chem_adaptive(double cs[NV], double &T, double Eo
     int k = 0;
     const double hmin = dt / cfg.nmax;
     Decoded o;
-    while (trem > 0.0 && k < cfg.nmax) {
-        double CMS[NS], MD[NS];
-        imex_source<SPEC>(cs, T, qk, CMS, MD, false);
-        double D = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; s++) D += cs[s];
-        double h = trem;
-#pragma unroll
-        for (int s = 0; s < NS; s++) {
-            const double w = fabs(CMS[s]);
-            if (w > 0.0) h = fmin(h, cfg.rel * (cs[s] + 1e-9 * D) / w);
-            if (MD[s] > 0.0) h = fmin(h, cfg.amp / MD[s]);
-        }
-        h = fmin(fmax(h, hmin), trem);
-        if (k == cfg.nmax - 1) h = trem;
-#pragma unroll
-        for (int s = 0; s < NS; s++) cs[s] = fmax(cs[s] + h * CMS[s] / (1.0 - h * MD[s]), 0.0);
-        int cp = 0;
-        decode(cs, T, Eold, qk, o, cp);
-        capped_any |= cp;
-        T = o.T;
-        trem -= h;
-        k++;
-    }
+    while (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Eold, qk, trem, k, hmin, cfg, o, capped_any);
     return k;
 }
 

@@ -83,6 +83,7 @@ struct eu3d_handle {
     bool tq_ok = false;
     int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
     int queue_blocks = 3;  // resident queue blocks per SM
+    int sur_fused = 0;     // surrogate: network and apply in one kernel (1) or two kernels (0, faster)
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
@@ -1442,6 +1443,7 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     if (t->flux_stage < 0 || t->flux_stage > 2) return fail(EU3D_ERR_ARG, "flux_stage must be 0, 1 or 2");
     // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
     h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
+    h->sur_fused = t->sur_fused ? 1 : 0;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;
@@ -1454,6 +1456,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
     t->chem_queue = h->chem_queue;
     t->queue_blocks = h->queue_blocks;
     t->flux_stage = h->flux_stage;
+    t->sur_fused = h->sur_fused;
     return EU3D_OK;
 }
 
@@ -1462,7 +1465,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
     CK(cudaSetDevice(h->dev));
-    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage};
+    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage, h->sur_fused};
     // the trials advance the state: keep a copy and put it back after each
     const size_t fs = (size_t)h->L.fs;
     const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
@@ -1494,7 +1497,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
                     if (h->flux_bits == 64 && fst != start.flux_stage) continue;
                     if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
                     if (q && cq == 0 && qb != start.queue_blocks) continue;
-                    cands.push_back({kz, cq, qb, fst});
+                    cands.push_back({kz, cq, qb, fst, start.sur_fused});
                 }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -214,6 +214,10 @@ int sur_set_attrs()
     CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcArray>, cudaFuncAttributeMaxDynamicSharedMemorySize, SURK_SMEM));
     CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcField<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize, SURK_SMEM));
     CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcField<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize, SURK_SMEM));
+    CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcFieldApply<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            SURK_SMEM));
+    CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcFieldApply<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            SURK_SMEM));
     done = true;
     return EU3D_OK;
 }
@@ -230,17 +234,26 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     // split step: the flux update and its decode first (Update_after_Adv),
     // unless the time scheme left the state decoded with the update in
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
-    {
-        ProfScope ps(h, "sur_mlp");
-        SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
-        const long long ntiles = src.ntiles();
-        k_sur_mlp<SurSrcField<P>><<<sur_grid(ntiles), 128 * SUR_NG, SURK_SMEM, h->st>>>(sur_weights(s), s->norm_d, src,
-                                                                                    ntiles, s->err);
-    }
     SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n};
-    {
+    SurApplyArgs a{cell_args(h), s->norm_d, h->sur_out, n, qu, h->sur_audit_stride};
+    const SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
+    const long long ntiles = src.ntiles();
+    if (h->sur_fused) {
+        // network and apply in one kernel (outputs stay on chip)
+        ProfScope ps(h, "sur_mlp_apply");
+        SurSrcFieldApply<P> fsrc;
+        static_cast<SurSrcField<P> &>(fsrc) = src;
+        fsrc.ap = a;
+        fsrc.q = q;
+        k_sur_mlp<SurSrcFieldApply<P>><<<sur_grid(ntiles), 128 * SUR_NG, SURK_SMEM, h->st>>>(sur_weights(s), s->norm_d,
+                                                                                         fsrc, ntiles, s->err);
+    } else {
+        {
+            ProfScope ps(h, "sur_mlp");
+            k_sur_mlp<SurSrcField<P>><<<sur_grid(ntiles), 128 * SUR_NG, SURK_SMEM, h->st>>>(sur_weights(s), s->norm_d,
+                                                                                        src, ntiles, s->err);
+        }
         ProfScope ps(h, "sur_apply");
-        SurApplyArgs a{cell_args(h), s->norm_d, h->sur_out, n, qu, h->sur_audit_stride};
         k_sur_apply<P><<<cell_grid(L, 128), 128, 0, h->st>>>(a, q);
     }
     {

@@ -396,7 +396,7 @@ struct SurSrcArray {  // normalised features, n x 16 FP32; outputs n x 16
         }
         return true;
     }
-    __device__ __forceinline__ void store(long long idx, const float o[SUR_OUT]) const
+    __device__ __forceinline__ void store(long long, int, long long idx, const float o[SUR_OUT]) const
     {
         float4 *p = reinterpret_cast<float4 *>(out + idx * SUR_OUT);
 #pragma unroll
@@ -435,7 +435,7 @@ struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
         sur_features(nrm, raw, f);
         return true;
     }
-    __device__ __forceinline__ void store(long long idx, const float o[SUR_OUT]) const
+    __device__ __forceinline__ void store(long long, int, long long idx, const float o[SUR_OUT]) const
     {
 #pragma unroll
         for (int k = 0; k < SUR_NOUT; k++) out[k * n + idx] = o[k];
@@ -600,7 +600,7 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
             } else {
                 float o[SUR_OUT];
                 tc::tmem_ld16(trow, o);
-                if (have) src.store(idx, o);
+                if (have) src.store(tile, t, idx, o);
             }
         }
         tc::fence_before();
@@ -653,16 +653,13 @@ __device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int valu
 // against the training envelope, for negative mass fractions and for the
 // energy balance at the predicted temperature, then applied to the species
 // and decoded in FP64.  Rejected cells (and audited ones) go to the fallback
-// list untouched.
+// list untouched.  (i, j, k): ghosted indices; net: the cell's network outputs.
 template <class P>
-__global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
+__device__ __forceinline__ void sur_apply_cell(const SurApplyArgs &s, P *__restrict__ q, int i, int j, int k,
+                                               const float net[SUR_NOUT])
 {
     const CellArgs &a = s.a;
     const Layout &L = a.L;
-    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = L.bc + blockIdx.y;
-    const int k = L.bc + blockIdx.z;
-    if (i >= L.ni + L.bc) return;
     if (solid_cell(a, i, j)) return;
     const long long c = L.at(i, j, k);
     const long long fs = L.fs;
@@ -709,8 +706,8 @@ __global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restr
     double dY[NS];
 #pragma unroll
     for (int sp = 0; sp < NS; sp++)
-        dY[sp] = (double)sur_unscale_f(n, sp, s.out[sp * s.n + idx], delta > 0.f ? sc * ((float)Y[sp] + delta) : sc);
-    const double dTn = (double)sur_unscale_f(n, NS, s.out[NS * s.n + idx], delta > 0.f ? sc * Tf : sc);
+        dY[sp] = (double)sur_unscale_f(n, sp, net[sp], delta > 0.f ? sc * ((float)Y[sp] + delta) : sc);
+    const double dTn = (double)sur_unscale_f(n, NS, net[NS], delta > 0.f ? sc * Tf : sc);
     sur_project(Y, dY, n.v[SN_PROJ_EPS]);
     double Yn[NS];
 #pragma unroll
@@ -741,7 +738,8 @@ __global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restr
         ok = ok_res && !capped && isfinite(o.T) && isfinite(o.D) && o.T >= 0.8 * n.v[SN_ENV + 0] &&
              o.T <= 1.2 * n.v[SN_ENV + 1];
     }
-    const bool audit = ok && s.audit_stride > 0 && (idx % s.audit_stride) == 0;
+    // (interior cells are fewer than 2^31)
+    const bool audit = ok && s.audit_stride > 0 && ((unsigned)idx % (unsigned)s.audit_stride) == 0;
     if (ok) {
         if (!audit) {
 #pragma unroll
@@ -760,45 +758,142 @@ __global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restr
     warp_count(&a.st->sur_reject[3], ok_res && !ok);
 }
 
-// Persistent fallback queue: warps pull 32 listed cells at a time from a
-// global cursor and run the FP64 adaptive integrator the network was trained
-// on (chem_increment, the M_ADAPT cell update) on each.  For audited cells the
-// surrogate's temperature is compared with the integrator's and the largest
-// difference recorded.
+// One thread per interior cell: the network outputs from the MLP kernel's
+// output buffer.
+template <class P>
+__global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
+{
+    const Layout &L = s.a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    float o[SUR_NOUT];
+#pragma unroll
+    for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + idx];
+    sur_apply_cell<P>(s, q, i, j, k, o);
+}
+
+// The MLP kernel's source for the fused form: features from the flowfield
+// (SurSrcField) and, instead of writing the outputs, the apply of each cell
+// right after its output layer, so that the outputs never travel through
+// HBM.  Same decisions as the network kernel followed by k_sur_apply; on the
+// 33.5 M-cell ODW it takes 10.4 ms against 4.55 + 3.94 ms for the two
+// kernels (the apply's memory latency has only the network kernel's 16
+// warps per SM to hide behind, and the kernel spills), so it is off by
+// default.
+template <class P>
+struct SurSrcFieldApply : SurSrcField<P> {
+    SurApplyArgs ap;
+    P *q;
+    __device__ __forceinline__ void store(long long tile, int lane, long long, const float o[SUR_OUT]) const
+    {
+        const Layout &L = this->L;
+        const int t = (int)tile;
+        const int r = t / this->tpr;
+        const int i = (t - r * this->tpr) * 128 + lane;
+        sur_apply_cell<P>(ap, q, L.bc + i, L.bc + r % L.nj, L.bc + r / L.nj, o);
+    }
+};
+
+// Persistent fallback queue, one listed cell per lane: a lane whose cell is
+// done takes the next listed cell at once (the lanes of a warp that need one
+// take them with one atomic on the global cursor), so a warp keeps stepping
+// the substeps of cells with different substep counts instead of waiting for
+// the slowest of a batch.  Each cell runs the FP64 adaptive split step the
+// network was trained on (adapt_split_step with the flux update applied
+// already: chem_increment, then the species update and a decode), one
+// substep per pass.  For audited cells the surrogate's temperature is
+// compared with the integrator's and the largest difference recorded.
 template <class P, bool SPEC>
 __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restrict__ q, SurQueue qu)
 {
     const int lane = threadIdx.x & 31;
-    const int total = min((long long)*qu.count, qu.cap);
+    const int total = (int)min((long long)*qu.count, qu.cap);
     const long long fs = a.L.fs;
+    const unsigned qk = a.quirks;
+    const double dt = a.scal[0];
+    const AdaptCfg cfg = a.acfg;
+    const double hmin = dt / cfg.nmax;
+    int slot = -1;  // list slot of the lane's cell; -1: needs one; >= total: none left
+    bool audit = false;
+    long long c = 0;
+    double cs0[NV], cs[NV];  // the cell's state before the chemistry; the integrator's copy
+    double T = 0.0, Esub = 0.0, trem = 0.0;
+    int k = 0, capped = 0;
+    Decoded o;
     for (;;) {
-        int base = 0;
-        if (lane == 0) base = atomicAdd(qu.count + 1, 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= total) break;
-        const int slot = base + lane;
+        const bool need = slot < 0;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(qu.count + 1, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                slot = base + __popc(m & ((1u << lane) - 1u));
+                if (slot < total) {
+                    const int ent = qu.list[slot];
+                    audit = ent < 0;
+                    c = (long long)(ent & 0x7fffffff);
+                    load_cs(a.cs, fs, c, cs0);
+                    // the decoded state (adapt_split_step without the flux
+                    // update): the integrator runs at its energy from its T
+                    double D = 0.0;
+#pragma unroll
+                    for (int s = 0; s < NS; s++) D += cs0[s];
+                    const double iD = 1.0 / D;
+                    const double U = cs0[NS] * iD, V = cs0[NS + 1] * iD, W = cs0[NS + 2] * iD;
+                    Esub = (cs0[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) * iD;
+                    T = a.T[c];
+#pragma unroll
+                    for (int v = 0; v < NV; v++) cs[v] = cs0[v];
+                    trem = dt;
+                    k = 0;
+                    capped = 0;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, slot >= total)) break;
         if (slot < total) {
-            const int ent = qu.list[slot];
-            const bool audit = ent < 0;
-            const long long c = (long long)(ent & 0x7fffffff);
-            double cs[NV];
-            load_cs(a.cs, fs, c, cs);
-            const double T = a.T[c], Eold = a.E[c];
-            Decoded o;
-            int capped = 0;
-            const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, false, o, capped);
-            atomicAdd(&a.st->substeps, (unsigned long long)nsub);
-            store_cs(a.cs, fs, c, cs);
-            a.T[c] = o.T;
-            a.E[c] = o.E;
-            store_prims<P>(o, q, fs, c);
-            if (capped) atomicAdd(&a.st->newton_capped, 1ull);
-            if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
-            if (audit) {
-                const double d = fabs(qu.audit[slot] - o.T);
-                atomicAdd(&a.st->audit_cells, 1ull);
-                if (isfinite(d)) atomicMax(&a.st->audit_max_dT_bits, (unsigned long long)__double_as_longlong(d));
-                else atomicMax(&a.st->audit_max_dT_bits, 0x7ff0000000000000ull);
+            if (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Esub, qk, trem, k, hmin, cfg, o, capped);
+            if (!(trem > 0.0 && k < cfg.nmax)) {
+                // chem_increment's projection, then adapt_split_step's update and decode
+                double D0 = 0.0, Dn = 0.0;
+#pragma unroll
+                for (int s = 0; s < NS; s++) {
+                    D0 += cs0[s];
+                    Dn += cs[s];
+                }
+                double Y0[NS], dY[NS];
+#pragma unroll
+                for (int s = 0; s < NS; s++) {
+                    Y0[s] = cs0[s] / D0;
+                    dY[s] = cs[s] / Dn - Y0[s];
+                }
+                elem_project(Y0, dY, a.proj_eps);
+                const double Tc = T;
+                const double iD = 1.0 / D0;
+#pragma unroll
+                for (int s = 0; s < NS; s++) cs0[s] = fmax(D0 * (cs0[s] * iD + dY[s]), 0.0);
+                int cp = 0;
+                decode(cs0, Tc, Esub, qk, o, cp);
+                capped |= cp;
+                atomicAdd(&a.st->substeps, (unsigned long long)k);
+                store_cs(a.cs, fs, c, cs0);
+                a.T[c] = o.T;
+                a.E[c] = o.E;
+                store_prims<P>(o, q, fs, c);
+                if (capped) atomicAdd(&a.st->newton_capped, 1ull);
+                if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
+                if (audit) {
+                    const double d = fabs(qu.audit[slot] - o.T);
+                    atomicAdd(&a.st->audit_cells, 1ull);
+                    if (isfinite(d)) atomicMax(&a.st->audit_max_dT_bits, (unsigned long long)__double_as_longlong(d));
+                    else atomicMax(&a.st->audit_max_dT_bits, 0x7ff0000000000000ull);
+                }
+                slot = -1;
             }
         }
     }

@@ -81,7 +81,8 @@ class Status(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int), ("flux_stage", C.c_int)]
+    _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int), ("flux_stage", C.c_int),
+                ("sur_fused", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -375,7 +376,7 @@ class DeviceFlowfield:
         _check(self.L.eu3d_get_tuning(self.h, C.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None):
+    def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None, sur_fused=None):
         t = Tuning(**self.tuning())
         if flux_kz is not None:
             t.flux_kz = flux_kz
@@ -385,6 +386,8 @@ class DeviceFlowfield:
             t.queue_blocks = queue_blocks
         if flux_stage is not None:
             t.flux_stage = int(flux_stage)
+        if sur_fused is not None:
+            t.sur_fused = 1 if sur_fused else 0
         _check(self.L.eu3d_set_tuning(self.h, C.byref(t)))
 
     def autotune(self, steps=3, react=REACT_IMEX, type_=0, timeadv=ADV_EE, diff=DIFF_MUSCL2, bc_kind=BC_RSBI,

@@ -213,12 +213,14 @@ int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
    primitives: 2 (default) tile planes brought into a shared-memory ring by
    TMA, 1 staged into shared memory by loads, 0 read through L1.  flux_stage
    2 needs the driver's tensor-map encoder and falls back to 1 without it.
-   Changing them drops the recorded step graphs. */
+   sur_fused 1: the surrogate's network and its apply in one kernel; 0
+   (default, faster on B200): two kernels; the same decisions either way.  Changing them drops the recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
     int queue_blocks;
     int flux_stage;
+    int sur_fused;
 } eu3d_tuning;
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t);
 int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t);

@@ -389,3 +389,52 @@ def test_adaptive_step_matches_oracle_and_survives_ignition(mech):
     el1 = cs[..., :9] @ A.T
     assert np.max(np.abs(el1 / el0 - 1)) < 1e-9
     d.close()
+
+
+@pytest.mark.parametrize("flux_bits", [32, 64])
+def test_fused_apply_equals_two_kernels(mech, flux_bits):
+    """The network and its apply in one kernel (sur_fused) give the same
+    accept/reject decisions, counters and conserved state as the network
+    kernel followed by k_sur_apply, on an ODW with accepted, rejected and
+    audited cells (FP32 flux: the conserved state bit for bit).  The decode's
+    outputs (T, E, P) agree to 1e-8: inlined into the network kernel, the
+    FP32 unscaling and the FP64 Newton polynomials are contracted into FMAs
+    differently, and a Newton start that differs in its last bit converges to
+    within the 1e-6 K tolerance of a slightly different temperature."""
+    from eu3d_b200.cases import odw_case, setup_odw
+    case = odw_case(mech, 160, 64, 3, L=0.05)
+    m0 = S.SurrogateModel.load(S.DEFAULT_MODEL)
+    norm = m0.norm.copy()
+    norm[S.N_ENV + 0] = 320.0  # the 300 K free stream leaves the envelope: it falls back
+    model = S.SurrogateModel(m0.params, norm, m0.meta)
+    out = []
+    for fused in (0, 1):
+        d = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+        setup_odw(d, case)
+        s = model.attach(d, 7)
+        d.set_tuning(sur_fused=fused)
+        assert d.tuning()["sur_fused"] == fused
+        kw = dict(timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0, final_time=1.0)
+        d.dt = 4e-8
+        d.run(40, react=gpu.REACT_IMEX, **kw)
+        d.run(3, react=gpu.REACT_SURROGATE, **kw)
+        d.synchronize()
+        st = d.status()
+        out.append(({f: d.download(f) for f in ("CS", "T", "E", "P", "Yi")}, st))
+        d.set_surrogate(None)
+        s.close()
+        d.close()
+    (a, sa), (b, sb) = out
+    assert sa["surrogate_cells"] > 0 and sa["surrogate_fallback"] > 0 and sa["surrogate_audited"] > 0, sa
+    for k in ("surrogate_cells", "surrogate_fallback", "surrogate_rejects", "surrogate_audited",
+              "nonfinite_cells", "wait_timeouts"):
+        assert sa[k] == sb[k], k
+    # FP32 primitives round the decode's last-bit differences away before the
+    # next flux; FP64 primitives carry them into the next steps' state
+    for f in ("CS", "Yi"):
+        if flux_bits == 32:
+            assert np.array_equal(a[f], b[f]), f
+        else:
+            assert np.max(np.abs(a[f] - b[f])) <= 1e-10 * np.max(np.abs(a[f])), f
+    for f in ("T", "E", "P"):
+        assert np.max(np.abs(a[f] - b[f]) / np.maximum(np.abs(a[f]), 1e-300)) <= 1e-8, f
