@@ -77,7 +77,7 @@ struct eu3d_handle {
     int4 *wedge_band = nullptr;  // solid cells the stencils reach, with their mirror sources
     int wedge_nband = 0;
     bool spec = false;  // mechanism equals the compiled-in H2_JA919 tables
-    int flux_kz = 16;   // z planes walked by one flux block
+    int flux_kz = 16;   // z planes walked by one flux block (set per grid at creation)
     int flux_stage = 2; // FP32 flux: 2 TMA ring (k_flux_ring), 1 staged by loads (k_flux_stage), 0 through L1
     CUtensorMap tq{};   // TMA map of the FP32 primitive array (k_flux_ring)
     bool tq_ok = false;
@@ -836,6 +836,15 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     L.NK = d->nk + 2 * d->bc;
     L.px = (L.NI + 31) / 32 * 32;
     L.fs = (long long)L.px * L.NJ * L.NK;
+    // z planes per flux block: deep walks load fewer extra planes per cell
+    // (one per block), but the grid should keep at least four waves of two
+    // blocks per SM; 64 on the 512 x 256 x 256 ODW
+    {
+        const long long cols = (long long)((L.ni + 31) / 32) * ((L.nj + 7) / 8);
+        int kz = 64;
+        while (kz > 4 && cols * ((L.nk + kz - 1) / kz) < 4LL * 2 * 148) kz /= 2;
+        h->flux_kz = kz;
+    }
     if ((long long)NPRIM * L.fs >= (1LL << 31)) {
         delete h;
         return fail(EU3D_ERR_ARG, "grid too large for one handle (primitive fields exceed 2^31 elements)");

@@ -207,7 +207,8 @@ int eu3d_wedge_fill(eu3d_handle *h);
 #define EU3D_PART_REACT 2  /* chemistry */
 int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
 
-/* Launch settings picked per handle (new): z planes walked by one flux block,
+/* Launch settings picked per handle (new): z planes walked by one flux block
+   (default: 64, halved while the flux grid has fewer than four waves),
    adaptive trapezoid on the persistent work queue (1) or one thread per cell
    (0), resident queue blocks per SM, and how the FP32 flux kernel reads the
    primitives: 2 (default) tile planes brought into a shared-memory ring by
