@@ -67,7 +67,8 @@ struct eu3d_handle {
     double *xn = nullptr, *yn = nullptr, *zn = nullptr;
     double *scal = nullptr;  // [0] dt, [1] time
     double *partial = nullptr;
-    int nparts = 0;
+    int nparts = 0;     // persistent-queue blocks (fallback queue)
+    int cfl_parts = 0;  // CFL reduction blocks (one partial triple each)
     Status *status = nullptr;
     double *inflow = nullptr;
     double *stage = nullptr;
@@ -419,11 +420,11 @@ void launch_cfl(eu3d_handle *h, const Spacing &sp, double cfl, double final_time
     const int use_z = (h->quirks & EU3D_Q_CFL_NO_Z) ? 0 : 1;
     {
         ProfScope ps(h, "cfl_partial");
-        k_cfl_partial<P><<<h->nparts, 256, 0, h->st>>>(h->L, (const P *)h->prim, use_z, h->xn, h->yn, h->wedge[0],
+        k_cfl_partial<P><<<h->cfl_parts, 256, 0, h->st>>>(h->L, (const P *)h->prim, use_z, h->xn, h->yn, h->wedge[0],
                                                        h->wedge[1], h->wedge[2], h->wedge_on, h->partial);
     }
     ProfScope ps(h, "cfl_final");
-    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->nparts, sp.dx, sp.dy, sp.dz, use_z, cfl, final_time, h->scal,
+    k_cfl_final<<<1, 1024, 0, h->st>>>(h->partial, h->cfl_parts, sp.dx, sp.dy, sp.dz, use_z, cfl, final_time, h->scal,
                                        advance);
 }
 
@@ -873,7 +874,10 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     ALLOC(h->zn, L.NK * sizeof(double));
     ALLOC(h->scal, 8 * sizeof(double));
     h->nparts = 148 * 4;
-    ALLOC(h->partial, 3 * h->nparts * sizeof(double));  // per block: largest |U|+C, |V|+C, |W|+C
+    // CFL: 16 blocks of 8 warps per SM, each warp walking a few rows, keep
+    // enough loads in flight to stream the six primitive fields
+    h->cfl_parts = 148 * 16;
+    ALLOC(h->partial, 3 * h->cfl_parts * sizeof(double));  // per block: largest |U|+C, |V|+C, |W|+C
     ALLOC(h->status, sizeof(Status));
 #undef ALLOC
     cudaMemsetAsync(h->cs, 0, NV * f8, h->st);
