@@ -761,7 +761,7 @@ __device__ __forceinline__ void sur_apply_cell(const SurApplyArgs &s, P *__restr
 // One thread per interior cell: the network outputs from the MLP kernel's
 // output buffer.
 template <class P>
-__global__ void __launch_bounds__(128, 4) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
+__global__ void __launch_bounds__(128, 7) k_sur_apply(SurApplyArgs s, P *__restrict__ q)
 {
     const Layout &L = s.a.L;
     const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
