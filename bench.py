@@ -407,8 +407,9 @@ def run_ours(a, rank, world, local):
     if clocks:
         out["clocks"] = clocks
     if not a.no_accuracy and rank == 0:
-        from eu3d_b200.validate import accuracy_2d
+        from eu3d_b200.validate import accuracy_2d, accuracy_3d
         out["accuracy"] = accuracy_2d(mech, model, a.accuracy_steps, cfl=CFL)
+        out["accuracy_3d"] = accuracy_3d(mech, model, a.accuracy_steps, nk=16, cfl=CFL)
     if not a.no_e2e:
         reset()
         out["e2e"] = run_e2e(dev, stepper(dict(base, react=gpu.REACT_SURROGATE)), a.steps, cells, torch, world, dist)
