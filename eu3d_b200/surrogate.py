@@ -129,7 +129,7 @@ def unscale(out, X, norm) -> np.ndarray:
     return label_scale(X, norm) * norm[N_LIN:N_LIN + N_OUT] * np.sinh(y)
 
 
-def make_norm(mech, X, Lb, Ta=0.0, Tr=1500.0, env=None, ratio_tol=0.02, res_abs=5.0, res_rel=0.05,
+def make_norm(mech, X, Lb, Ta=0.0, Tr=1500.0, env=None, ratio_tol=0.02, res_abs=4.0, res_rel=0.04,
               neg_tol=1e-6, proj_eps=1e-4, lin_quantile=0.05, dT_max=2500.0, delta=1e-10,
               lin_T=900.0) -> np.ndarray:
     """Normalisation and acceptance vector from (a sample of) the raw set.
