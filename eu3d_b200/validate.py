@@ -8,6 +8,22 @@ from __future__ import annotations
 import numpy as np
 
 
+def front_position(T, thr=1800.0):
+    """Detonation-front position per line along x (axis 0) of a temperature
+    field (ni, ...): the first x, in cells and linearly interpolated, where T
+    exceeds thr; NaN where no cell does or the first cell already does."""
+    T = np.asarray(T, dtype=np.float64)
+    hot = T > thr
+    k = np.argmax(hot, axis=0)
+    f = np.full(k.shape, np.nan)
+    ok = hot.any(axis=0) & (k > 0)
+    idx = np.nonzero(ok)
+    i = k[idx]
+    a, b = T[(i - 1,) + idx], T[(i,) + idx]
+    f[idx] = i - 1 + (thr - a) / (b - a)
+    return f
+
+
 def accuracy_2d(mech, model, steps, ni=512, nj=256, cfl=0.5):
     """Coupled 2D ODW (the 3D case's cells) with the surrogate, the FP64
     adaptive integrator (its teacher) and the plain FP64 IMEX integrator:
@@ -29,20 +45,11 @@ def accuracy_2d(mech, model, steps, ni=512, nj=256, cfl=0.5):
         stats[name] = d.status()
         d.close()
 
-    def fronts(T, thr=1800.0):
-        f = np.full(T.shape[1], np.nan)
-        for j in range(T.shape[1]):
-            r = T[:, j]
-            k = int(np.argmax(r > thr))
-            if r[k] > thr and k > 0:
-                f[j] = k - 1 + (thr - r[k - 1]) / (r[k] - r[k - 1])
-        return f
-
-    fa = fronts(res["adaptive"])
+    fa = front_position(res["adaptive"])
     out = {"case": f"2D ODW {ni}x{nj} (the 3D case's cells), SSP-RK2, CFL {cfl}, {steps} steps",
            "peak_T_adaptive": float(np.nanmax(res["adaptive"]))}
     for name in ("surrogate", "imex"):
-        fx = fronts(res[name])
+        fx = front_position(res[name])
         both = np.isfinite(fa) & np.isfinite(fx)
         d = np.abs(fa - fx)[both]
         st = stats[name]
@@ -81,22 +88,11 @@ def accuracy_3d(mech, model, steps, ni=512, nj=256, nk=16, cfl=0.5):
         stats[name] = d.status()
         d.close()
 
-    def fronts(T, thr=1800.0):
-        hot = T > thr
-        k = np.argmax(hot, axis=0)
-        f = np.full(k.shape, np.nan)
-        ok = hot.any(axis=0) & (k > 0)
-        jj, kk = np.nonzero(ok)
-        i = k[jj, kk]
-        a, b = T[i - 1, jj, kk], T[i, jj, kk]
-        f[jj, kk] = i - 1 + (thr - a) / (b - a)
-        return f
-
-    fa = fronts(res["adaptive"])
+    fa = front_position(res["adaptive"])
     out = {"case": f"3D ODW {ni}x{nj}x{nk} (the benchmark's cells, spanwise slice), SSP-RK2, CFL {cfl}, {steps} steps",
            "peak_T_adaptive": float(np.nanmax(res["adaptive"]))}
     for name in ("surrogate", "imex"):
-        fx = fronts(res[name])
+        fx = front_position(res[name])
         both = np.isfinite(fa) & np.isfinite(fx)
         dd = np.abs(fa - fx)[both]
         st = stats[name]
