@@ -280,19 +280,24 @@ def roofline(prof, cells, hbm, tflops, src):
     if bound == "hbm":
         ach = work * cells / (avg_ms * 1e-3) / 1e9
         return {"bound": "hbm", "kernel": k, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": TRAFFIC.get(k), "per_cell": f"{work} B", "avg_ms": avg_ms,
+                "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
+                "traffic_note": "ncu DRAM bytes of one launch on a 2.10 M-cell case, scaled by cells",
+                "per_cell": f"{work} B", "avg_ms": avg_ms,
                 "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; peak {src} "
                         f"(MEASURED_PEAKS.json hbm_gbs)"}
     ach = work * cells / (avg_ms * 1e-3) / 1e12
     return {"bound": "tensor", "kernel": k, "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops,
-            "traffic": TRAFFIC.get(k), "per_cell": f"{work} FLOP", "avg_ms": avg_ms,
+            "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
+            "per_cell": f"{work} FLOP", "avg_ms": avg_ms,
             "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; peak {src} "
                     f"(MEASURED_PEAKS.json bf16_tflops)"}
 
 
-# DRAM bytes per launch of the full-size workload (ncu dram__bytes_read + _write,
-# summarised under profiles/; scaled from the captured case by cells)
-TRAFFIC = {}
+# DRAM bytes per cell of a launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch on the 256 x 128 x 64 ODW, 2.10 M cells: the full 33.5 M-cell
+# case is too large to capture under the profiling rule), scaled to a launch
+# by cells; the flux kernel's traffic grows with cells (one pass, no re-reads)
+TRAFFIC_PER_CELL = {"advection": (192.838656e6 + 180.969216e6) / 2097152}
 
 
 def developed_state(mech, ni, nj, nk, steps2d, seed):
