@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -21,6 +22,7 @@
 #include "flux.cuh"
 #include "mlp.cuh"
 #include "surrogate.cuh"
+#include "tecplot.cuh"
 
 using namespace eu3d;
 
@@ -107,6 +109,13 @@ struct eu3d_handle {
     double *sur_audit = nullptr;
     long long sur_cap = 0;
     int sur_audit_stride = 0;
+    // result files (eu3d_write_tecplot): gathered columns on the device and in
+    // pinned host memory, and the background writer
+    double *tp_dev = nullptr, *tp_host = nullptr;
+    int *tp_ldev = nullptr, *tp_lhost = nullptr;
+    std::vector<double> tp_nodes;  // ghosted x, y, z node coordinates
+    std::thread writer;
+    std::string writer_err;
 };
 
 namespace {
@@ -632,6 +641,11 @@ void free_handle(eu3d_handle *h)
                     h->sur_audit, h->qlist,   h->qbins,  h->wedge_band};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (h->writer.joinable()) h->writer.join();
+    if (h->tp_dev) cudaFree(h->tp_dev);
+    if (h->tp_ldev) cudaFree(h->tp_ldev);
+    if (h->tp_host) cudaFreeHost(h->tp_host);
+    if (h->tp_lhost) cudaFreeHost(h->tp_lhost);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -947,6 +961,74 @@ int eu3d_destroy(eu3d_handle *h)
 }
 
 void *eu3d_stream(eu3d_handle *h) { return h ? (void *)h->st : nullptr; }
+
+// ------------------------------------------------------------ result files
+int eu3d_write_wait(eu3d_handle *h)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (h->writer.joinable()) h->writer.join();
+    if (!h->writer_err.empty()) {
+        const std::string e = h->writer_err;
+        h->writer_err.clear();
+        return fail(EU3D_ERR_IO, e);
+    }
+    return EU3D_OK;
+}
+
+int eu3d_write_tecplot(eu3d_handle *h, const char *path, double wait_time, int background)
+{
+    if (!h || !path) return fail(EU3D_ERR_ARG, "null argument");
+    int rc = eu3d_write_wait(h);  // one file at a time per handle
+    if (rc) return rc;
+    CK(cudaSetDevice(h->dev));
+    const Layout &L = h->L;
+    const long long n = L.interior_cells();
+    if (!h->tp_dev) {
+        CK(cudaMalloc(&h->tp_dev, (size_t)TP_COLS * n * sizeof(double)));
+        CK(cudaMalloc(&h->tp_ldev, (size_t)n * sizeof(int)));
+        CK(cudaHostAlloc(&h->tp_host, (size_t)TP_COLS * n * sizeof(double), cudaHostAllocDefault));
+        CK(cudaHostAlloc(&h->tp_lhost, (size_t)n * sizeof(int), cudaHostAllocDefault));
+    }
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    if (h->flux_bits == 64)
+        k_tecplot_gather<double><<<blocks, 256, 0, h->st>>>(L, (const double *)h->prim, h->T, h->nchem, h->tp_dev,
+                                                            h->tp_ldev);
+    else
+        k_tecplot_gather<float><<<blocks, 256, 0, h->st>>>(L, (const float *)h->prim, h->T, h->nchem, h->tp_dev,
+                                                           h->tp_ldev);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->tp_host, h->tp_dev, (size_t)TP_COLS * n * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(h->tp_lhost, h->tp_ldev, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    h->tp_nodes.resize((size_t)L.NI + L.NJ + L.NK);
+    CK(cudaMemcpyAsync(h->tp_nodes.data(), h->xn, L.NI * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(h->tp_nodes.data() + L.NI, h->yn, L.NJ * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaMemcpyAsync(h->tp_nodes.data() + L.NI + L.NJ, h->zn, L.NK * sizeof(double), cudaMemcpyDeviceToHost,
+                       h->st));
+    CK(cudaStreamSynchronize(h->st));  // the snapshot is on the host: the device may step on
+    const std::string p(path);
+    auto job = [h, p, wait_time, L]() {
+        const double *nodes = h->tp_nodes.data();
+        h->writer_err = tecplot::write(p.c_str(), L.ni, L.nj, L.nk, L.bc, nodes, nodes + L.NI, nodes + L.NI + L.NJ,
+                                       h->tp_host, h->tp_lhost, wait_time);
+    };
+    if (background) {
+        h->writer = std::thread(job);
+        return EU3D_OK;
+    }
+    job();
+    return eu3d_write_wait(h);
+}
+
+int eu3d_tecplot_write_host(const char *path, int ni, int nj, int nk, int bc, const double *xnode, const double *ynode,
+                            const double *znode, const double *cols, const int *lcol, double wait_time)
+{
+    if (!path || !xnode || !ynode || !znode || !cols || !lcol) return fail(EU3D_ERR_ARG, "null argument");
+    if (ni < 1 || nj < 1 || nk < 1 || bc < 0) return fail(EU3D_ERR_ARG, "bad extents");
+    const std::string e = tecplot::write(path, ni, nj, nk, bc, xnode, ynode, znode, cols, lcol, wait_time);
+    return e.empty() ? EU3D_OK : fail(EU3D_ERR_IO, e);
+}
+
+
 
 int eu3d_upload_field(eu3d_handle *h, int field, const double *host)
 {

@@ -42,7 +42,7 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune",
            "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive", "eu3d_halo_bytes", "eu3d_halo_pack",
            "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
-           "eu3d_step_part"]
+           "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host"]
 
 PART_STAGE1, PART_STAGE2, PART_REACT = 0, 1, 2
 
@@ -162,6 +162,10 @@ def load_library(path: Optional[str] = None):
     L.eu3d_advance_time.argtypes = h
     L.eu3d_wedge_fill.argtypes = h
     L.eu3d_step_part.argtypes = h + [C.POINTER(StepDesc), C.c_int]
+    L.eu3d_write_tecplot.argtypes = h + [C.c_char_p, C.c_double, C.c_int]
+    L.eu3d_write_wait.argtypes = h
+    L.eu3d_tecplot_write_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+                                          C.POINTER(C.c_int), C.c_double]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]
@@ -334,6 +338,13 @@ class DeviceFlowfield:
 
     def synchronize(self):
         _check(self.L.eu3d_synchronize(self.h))
+
+    def write_tecplot(self, path: str, wait_time: float = 0.0, background: bool = False):
+        """The reference's Tecplot block result file of this handle (Euler::Output)."""
+        _check(self.L.eu3d_write_tecplot(self.h, path.encode(), wait_time, 1 if background else 0))
+
+    def write_wait(self):
+        _check(self.L.eu3d_write_wait(self.h))
 
     # ---- x-slab decomposition (one handle per rank; eu3d_b200.slabs drives them)
     def halo_bytes(self) -> int:
@@ -543,3 +554,18 @@ class DeviceSurrogate:
 
     def infer_device(self, x_ptr: int, n: int, out_ptr: int, stream: int = 0):
         _check(self.L.eu3d_sur_infer(self.s, x_ptr, n, out_ptr, stream or None))
+
+
+def write_tecplot_host(path: str, grid, cols, lcol, wait_time: float = 0.0):
+    """The Tecplot block file from host arrays: cols (13, n) T D P U V Ma Y1..Y7 and
+    lcol (n,) counts, both in the file's cell order (k outer, i inner)."""
+    L = load_library()
+    n = grid.ni * grid.nj * grid.nk
+    c = np.ascontiguousarray(cols, dtype=np.float64)
+    lc = np.ascontiguousarray(lcol, dtype=np.int32)
+    if c.shape != (13, n) or lc.shape != (n,):
+        raise Eu3dError("cols must be (13, n) and lcol (n,)")
+    xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (grid.xnode, grid.ynode, grid.znode)]
+    _check(L.eu3d_tecplot_write_host(path.encode(), grid.ni, grid.nj, grid.nk, grid.bc,
+                                     *(a.ctypes.data_as(_dp) for a in xs), c.ctypes.data_as(_dp),
+                                     lc.ctypes.data_as(C.POINTER(C.c_int)), wait_time))

@@ -41,6 +41,7 @@ extern "C" {
 #define EU3D_ERR_MECH (-4)      /* mechanism differs from the one already loaded */
 #define EU3D_ERR_STATE (-5)     /* call not valid in the handle's current state */
 #define EU3D_ERR_NONFINITE (-6) /* a NaN/Inf density or temperature was found */
+#define EU3D_ERR_IO (-7)        /* a result file could not be written */
 
 /* Interior node counts, ghost width and node coordinates come from the
    reference's Mesh (include/Mesh.hpp:22-46, src/Mesh.cpp:75-130); the
@@ -242,6 +243,23 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
 int eu3d_profile_enable(eu3d_handle *h, int on);
 int eu3d_profile_read(eu3d_handle *h, char *names, size_t names_cap, double *ms, long long *counts,
                       int max_kernels, int *n_out);
+/* Euler::Output (src/Euler.cpp:792-973): the rank's Tecplot block file at `path`
+   (the caller picks the name; the reference uses output_<n>/results/Series<react><num>_<rank>.dat
+   for one rank and output_<n>/results<react><num>_<rank>.dat for several).  Header
+   "Variables = X,Y,Z,T,D,P,U,V,Ma,Y1,...,Y7,L,WaitTime", "ZONE I=ni<TAB>J=nj<TAB>K=nk",
+   "datapacking=block", then 18 blocks over the interior cells, k outer, i inner, one
+   value per line as std::ostream prints them (%.6g; L, the substep counts, as
+   integers; WaitTime the caller's wait_time).  The fields are gathered on the device
+   and copied to pinned host memory before the call returns; background != 0 formats
+   and writes on a host thread while the caller steps on, and eu3d_write_wait returns
+   its outcome (a new write waits for the previous one). */
+int eu3d_write_tecplot(eu3d_handle *h, const char *path, double wait_time, int background);
+int eu3d_write_wait(eu3d_handle *h);
+/* The same file from host arrays (no device): ghosted node coordinates, 13 x ni*nj*nk
+   columns T D P U V Ma Y1..Y7 and the counts L, both in the file's cell order. */
+int eu3d_tecplot_write_host(const char *path, int ni, int nj, int nk, int bc, const double *xnode,
+                            const double *ynode, const double *znode, const double *cols, const int *lcol,
+                            double wait_time);
 /* Status counters; a D/T NaN scan replaces D.IsNan()/T.IsNan() (src/Euler.cpp:319-331). */
 int eu3d_get_status(eu3d_handle *h, eu3d_status *st);
 int eu3d_reset_status(eu3d_handle *h);

@@ -12,6 +12,11 @@
    RSBI case (output_8/resultsIMEX0_{rank}.dat of an EU3D checkout; 8 ranks,
    4 x 2 x 1 blocks, 6 significant digits), columns X Y T D P U V Y1..Y7, for
    ranks 0 and 5.
+3. rsbi_t0_text.npz -- the whole text of output_8/resultsIMEX0_0.dat (the
+   reference's Euler::Output file of rank 0), zlib-compressed, to pin the
+   result-file writer's format.
+
+    python tests/golden/make_golden.py --text    (3. only)
 """
 from __future__ import annotations
 
@@ -92,7 +97,18 @@ def run_reference(mech, name, quirks, react, typ, cfl, dt, steps, bc_kind, st):
     return res, rc.dt, rc.time
 
 
+def text_fixture():
+    import zlib
+    path = os.path.join(REF_DIR, "output_8", "resultsIMEX0_0.dat")
+    with open(path, "rb") as fh:
+        raw = fh.read()
+    np.savez_compressed(os.path.join(HERE, "rsbi_t0_text.npz"),
+                        rank0=np.frombuffer(zlib.compress(raw, 9), dtype=np.uint8))
+    print("wrote", os.path.join(HERE, "rsbi_t0_text.npz"), len(raw), "bytes of text")
+
+
 def main():
+    text_fixture()
     mech = load_h2_ja919()
     out = {}
     for c in CASES:
@@ -120,4 +136,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "--text" in sys.argv:
+        text_fixture()
+    else:
+        main()
