@@ -507,7 +507,9 @@ enum CellMode {
     M_RK_STAGE2 = 6,
     M_NOCHEM = 7,
     M_TRAP1_PREDICT = 8,
-    M_ADAPT = 9
+    M_ADAPT = 9,
+    M_RK3_STAGE2 = 10,
+    M_RK3_STAGE3 = 11
 };
 
 // Work queue of the adaptive trapezoid: cells binned by floor(log2 Nchem),
@@ -594,7 +596,8 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
 //  M_IMEX    Diagonalized + Update_IMEX (+ decode, + GetPartial_T for the next step)
 //  M_TRAP0   Update_after_Adv, field Trapezoid, Explicit()
 //  M_TRAP1   Update_after_Adv, TrapezoidPrediction and the per-cell substeps
-//  M_RK_STAGE1/2  SSP-RK2 stage updates (new)
+//  M_RK_STAGE1/2  SSP-RK2 stage updates (new); M_RK_STAGE1 is also SSP-RK3's first
+//  M_RK3_STAGE2/3 SSP-RK3 stage updates (new)
 //  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
 template <class P, int MODE, bool SPEC>
 __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
@@ -640,17 +643,22 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
-    } else if (MODE == M_RK_STAGE1 || MODE == M_RK_STAGE2) {
+    } else if (MODE == M_RK_STAGE1 || MODE == M_RK_STAGE2 || MODE == M_RK3_STAGE2 || MODE == M_RK3_STAGE3) {
         // Stage 1 leaves CS^n where it is and puts the stage state
-        // CS^n + R(q^n) into cs0; stage 2 forms 0.5 CS^n + 0.5 (CS1 + R(q1))
-        // back into cs.  No copy of CS^n is made.
+        // CS^n + R(q^n) into cs0; SSP-RK2's stage 2 forms
+        // 0.5 CS^n + 0.5 (CS1 + R(q1)) back into cs.  SSP-RK3 (Shu and Osher,
+        // J. Comput. Phys. 77, 1988) forms CS2 = 3/4 CS^n + 1/4 (CS1 + R(q1))
+        // into cs0 and CS^{n+1} = 1/3 CS^n + 2/3 (CS2 + R(q2)) into cs.  No
+        // copy of CS^n is made.
+        constexpr double wn = MODE == M_RK_STAGE2 ? 0.5 : MODE == M_RK3_STAGE2 ? 0.75 : 1.0 / 3.0;
+        constexpr double ws = MODE == M_RK_STAGE2 ? 0.5 : MODE == M_RK3_STAGE2 ? 0.25 : 2.0 / 3.0;
 #pragma unroll
         for (int v = 0; v < NV; v++) {
             const double r = a.rhs[v * fs + c];
             if (MODE == M_RK_STAGE1)
                 cs[v] = cs[v] + r;
             else
-                cs[v] = 0.5 * cs[v] + 0.5 * (a.cs0[v * fs + c] + r);
+                cs[v] = __dadd_rn(__dmul_rn(wn, cs[v]), __dmul_rn(ws, __dadd_rn(a.cs0[v * fs + c], r)));
         }
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
@@ -731,7 +739,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
             atomicAdd(&a.st->substeps, (unsigned long long)n);
         }
     }
-    store_cs(MODE == M_RK_STAGE1 ? a.cs0 : a.cs, fs, c, cs);
+    store_cs(MODE == M_RK_STAGE1 || MODE == M_RK3_STAGE2 ? a.cs0 : a.cs, fs, c, cs);
     a.T[c] = o.T;
     a.E[c] = o.E;
     store_prims<P>(o, q, fs, c);

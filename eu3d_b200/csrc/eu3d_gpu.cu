@@ -193,7 +193,7 @@ void launch_cell_t(eu3d_handle *h, int mode)
     dim3 g = cell_grid(h->L, 128);
     static const char *names[] = {"cell_decode", "cell_adv",   "cell_imex",          "cell_trap0", "cell_trap1",
                                   "cell_rk1",    "cell_rk2",   "cell_nochem",        "cell_trap1_predict",
-                                  "cell_adapt"};
+                                  "cell_adapt",  "cell_rk3_2", "cell_rk3_3"};
     ProfScope ps(h, names[mode]);
     switch (mode) {
     case M_DECODE: k_cell<P, M_DECODE, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
@@ -205,6 +205,8 @@ void launch_cell_t(eu3d_handle *h, int mode)
     case M_RK_STAGE2: k_cell<P, M_RK_STAGE2, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     case M_NOCHEM: k_cell<P, M_NOCHEM, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     case M_ADAPT: k_cell<P, M_ADAPT, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK3_STAGE2: k_cell<P, M_RK3_STAGE2, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
+    case M_RK3_STAGE3: k_cell<P, M_RK3_STAGE3, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     }
 }
 
@@ -663,26 +665,32 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
 
 int sur_chem_op(eu3d_handle *h, bool decoded);  // learned chemistry step, sur_host.cuh
 
-// The step after the CFL and the first ghost fill, in three parts so that a
+bool is_rk(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 || timeadv == EU3D_ADV_SSPRK3; }
+int rk_stages(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 ? 2 : timeadv == EU3D_ADV_SSPRK3 ? 3 : 1; }
+
+// The step after the CFL and the first ghost fill, in parts so that a
 // multi-rank driver can exchange x-slab halos between them (eu3d_step_part):
-// the advection stage (SSP-RK2: stage 1), the second SSP-RK2 stage after its
+// the advection stage (SSP-RK: stage 1), each further SSP-RK stage after its
 // own ghost fill, and the chemistry.
 int stage1_op(eu3d_handle *h, const eu3d_step_desc *s)
 {
     int rc;
-    if (s->timeadv == EU3D_ADV_SSPRK2) {
+    if (is_rk(s->timeadv)) {
         if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
         return cell_op(h, M_RK_STAGE1);
     }
     return adv_op(h, s->timeadv, s->diff);
 }
 
-int stage2_op(eu3d_handle *h, const eu3d_step_desc *s)
+// stage 2 or 3 of an SSP-RK step; the last stage leaves RHS zero for the chemistry
+int stage_op(eu3d_handle *h, const eu3d_step_desc *s, int stage)
 {
     int rc;
     if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
-    if ((rc = cell_op(h, M_RK_STAGE2))) return rc;
-    CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
+    const int mode = s->timeadv == EU3D_ADV_SSPRK2 ? M_RK_STAGE2 : stage == 2 ? M_RK3_STAGE2 : M_RK3_STAGE3;
+    if ((rc = cell_op(h, mode))) return rc;
+    if (stage == rk_stages(s->timeadv))
+        CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
     return EU3D_OK;
 }
 
@@ -694,10 +702,10 @@ int react_op(eu3d_handle *h, const eu3d_step_desc *s)
     case EU3D_REACT_NONE:
         // Euler::DNN (src/Euler.cpp:773-780): Update_after_Adv, then Explicit()
         return cell_op(h, M_NOCHEM);
-    // after SSP-RK2 the state is decoded and RHS holds zeros already
-    case EU3D_REACT_SURROGATE: return sur_chem_op(h, s->timeadv == EU3D_ADV_SSPRK2);
+    // after SSP-RK the state is decoded and RHS holds zeros already
+    case EU3D_REACT_SURROGATE: return sur_chem_op(h, is_rk(s->timeadv));
     case EU3D_REACT_ADAPTIVE: {
-        h->rhs_applied = s->timeadv == EU3D_ADV_SSPRK2;
+        h->rhs_applied = is_rk(s->timeadv);
         const int rc = cell_op(h, M_ADAPT);
         h->rhs_applied = false;
         return rc;
@@ -712,9 +720,9 @@ int enqueue_step(eu3d_handle *h, const eu3d_step_desc *s, const Spacing &sp)
     if (s->cfl != 0 && (rc = cfl_op(h, s->cfl, s->final_time, sp))) return rc;
     if ((rc = ghost_op(h, s->bc_kind))) return rc;
     if ((rc = stage1_op(h, s))) return rc;
-    if (s->timeadv == EU3D_ADV_SSPRK2) {
+    for (int stage = 2; stage <= rk_stages(s->timeadv); stage++) {
         if ((rc = ghost_op(h, s->bc_kind))) return rc;
-        if ((rc = stage2_op(h, s))) return rc;
+        if ((rc = stage_op(h, s, stage))) return rc;
     }
     return react_op(h, s);
 }
@@ -1303,8 +1311,11 @@ int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part)
     switch (part) {
     case EU3D_PART_STAGE1: return stage1_op(h, s);
     case EU3D_PART_STAGE2:
-        if (s->timeadv != EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "stage 2 exists for SSP-RK2 only");
-        return stage2_op(h, s);
+        if (!is_rk(s->timeadv)) return fail(EU3D_ERR_ARG, "stage 2 exists for SSP-RK2/RK3 only");
+        return stage_op(h, s, 2);
+    case EU3D_PART_STAGE3:
+        if (s->timeadv != EU3D_ADV_SSPRK3) return fail(EU3D_ERR_ARG, "stage 3 exists for SSP-RK3 only");
+        return stage_op(h, s, 3);
     case EU3D_PART_REACT: return react_op(h, s);
     default: return fail(EU3D_ERR_ARG, "unknown step part");
     }
@@ -1337,12 +1348,12 @@ int eu3d_react_trapezoid(eu3d_handle *h, int type)
 }
 
 namespace {
-// argument and state checks of a step, and the buffers it needs (the SSP-RK2
-// stage copy, the trapezoid work queue), for eu3d_step and eu3d_step_part
+// argument and state checks of a step, and the buffers it needs (the SSP-RK
+// stage state, the trapezoid work queue), for eu3d_step and eu3d_step_part
 int prepare_step(eu3d_handle *h, const eu3d_step_desc *s)
 {
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
-    if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK2) return fail(EU3D_ERR_ARG, "unknown time scheme");
+    if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK3) return fail(EU3D_ERR_ARG, "unknown time scheme");
     if (s->diff != EU3D_DIFF_MUSCL1 && s->diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
     if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE &&
         s->react != EU3D_REACT_SURROGATE && s->react != EU3D_REACT_ADAPTIVE)
@@ -1352,7 +1363,7 @@ int prepare_step(eu3d_handle *h, const eu3d_step_desc *s)
     if (s->react == EU3D_REACT_SURROGATE && !h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached");
     if (s->bc_kind == EU3D_BC_ODM && !h->inflow) return fail(EU3D_ERR_STATE, "ODM boundary needs eu3d_set_inflow first");
     CK(cudaSetDevice(h->dev));
-    if (s->timeadv == EU3D_ADV_SSPRK2 && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
+    if (is_rk(s->timeadv) && !h->cs0) CK(cudaMalloc(&h->cs0, (size_t)NV * h->L.fs * sizeof(double)));
     if (s->react == EU3D_REACT_TRAPEZOID && s->type == 1 && h->chem_queue) {
         int rc = ensure_queue(h);
         if (rc) return rc;

@@ -24,7 +24,7 @@ QUIRKS_FIXED = 0x000
 BC_RSBI, BC_ODM, BC_TRANSMISSIVE, BC_NONE = 0, 1, 2, 3
 REACT_TRAPEZOID, REACT_IMEX, REACT_NONE, REACT_SURROGATE, REACT_ADAPTIVE = 0, 1, 2, 3, 4
 DIFF_MUSCL1, DIFF_MUSCL2 = 0, 1
-ADV_EE, ADV_TVD_RK3, ADV_SSPRK2 = 0, 1, 2
+ADV_EE, ADV_TVD_RK3, ADV_SSPRK2, ADV_SSPRK3 = 0, 1, 2, 3
 
 FIELDS = {"U": 0, "V": 1, "W": 2, "P": 3, "D": 4, "T": 5, "H": 6, "Gamma": 7, "E": 8, "Yi": 9, "CS": 10, "RHS": 11,
           "C": 12, "Mc": 13, "Di": 14, "Nchem": 15}
@@ -44,7 +44,7 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
            "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host"]
 
-PART_STAGE1, PART_STAGE2, PART_REACT = 0, 1, 2
+PART_STAGE1, PART_STAGE2, PART_REACT, PART_STAGE3 = 0, 1, 2, 3
 
 SUR_NPARAM = 37264
 SUR_NORM_LEN = 80

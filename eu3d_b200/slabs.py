@@ -13,8 +13,9 @@ A step of one slab, as `eu3d_step` does it on a single rank:
 
     CFL: local dt -> all-reduce MIN -> time += dt
     boundary fill -> halo exchange [-> wedge band -> halo exchange]
-    stage 1 (advection; SSP-RK2: + stage-1 update and decode)
-    SSP-RK2: boundary fill -> halo exchange [...] -> stage 2
+    stage 1 (advection; SSP-RK: + stage-1 update and decode)
+    SSP-RK2/RK3: boundary fill -> halo exchange [...] -> stage 2
+    SSP-RK3: boundary fill -> halo exchange [...] -> stage 3
     chemistry
 
 With an immersed wedge the band is filled again after the first exchange (its
@@ -121,9 +122,12 @@ class Slab:
             self.advance_time()
         yield from self._fill(spec.bc_kind)
         self.part(gpu.PART_STAGE1, spec)
-        if spec.timeadv == gpu.ADV_SSPRK2:
+        if spec.timeadv in (gpu.ADV_SSPRK2, gpu.ADV_SSPRK3):
             yield from self._fill(spec.bc_kind)
             self.part(gpu.PART_STAGE2, spec)
+        if spec.timeadv == gpu.ADV_SSPRK3:
+            yield from self._fill(spec.bc_kind)
+            self.part(gpu.PART_STAGE3, spec)
         self.part(gpu.PART_REACT, spec)
 
     def _fill(self, kind):

@@ -180,7 +180,8 @@ int eu3d_synchronize(eu3d_handle *h);
      eu3d_advance_time;
      eu3d_boundary; halo exchange; [wedge set: eu3d_wedge_fill; halo exchange];
      eu3d_step_part(STAGE1);
-     SSP-RK2: eu3d_boundary; halo exchange; [wedge ...]; eu3d_step_part(STAGE2);
+     SSP-RK2/RK3: eu3d_boundary; halo exchange; [wedge ...]; eu3d_step_part(STAGE2);
+     SSP-RK3: eu3d_boundary; halo exchange; [wedge ...]; eu3d_step_part(STAGE3);
      eu3d_step_part(REACT).
    Halo exchange: eu3d_halo_pack(side) into a device buffer of eu3d_halo_bytes bytes,
    send it to the neighbour on that side, receive the neighbour's buffer and
@@ -202,10 +203,11 @@ int eu3d_advance_time(eu3d_handle *h);
 /* the immersed-wedge ghost band alone (eu3d_boundary runs it after the faces) */
 int eu3d_wedge_fill(eu3d_handle *h);
 /* the parts of eu3d_step after its CFL and first ghost fill */
-#define EU3D_PART_STAGE1 0 /* advection (SSP-RK2: with the stage-1 update and decode; the stage's
-                              conserved state is held apart and CS keeps CS^n until STAGE2) */
-#define EU3D_PART_STAGE2 1 /* SSP-RK2 stage 2: advection, update, decode */
+#define EU3D_PART_STAGE1 0 /* advection (SSP-RK: with the stage-1 update and decode; the stage's
+                              conserved state is held apart and CS keeps CS^n until the last stage) */
+#define EU3D_PART_STAGE2 1 /* SSP-RK2/RK3 stage 2: advection, update, decode */
 #define EU3D_PART_REACT 2  /* chemistry */
+#define EU3D_PART_STAGE3 3 /* SSP-RK3 stage 3: advection, update, decode */
 int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
 
 /* Launch settings picked per handle (new): z planes walked by one flux block

@@ -62,5 +62,6 @@
 #define EU3D_ADV_EE 0
 #define EU3D_ADV_TVD_RK3 1 /* the reference's no-op: RHS is left unchanged */
 #define EU3D_ADV_SSPRK2 2  /* two-stage SSP Runge-Kutta (new) */
+#define EU3D_ADV_SSPRK3 3  /* three-stage SSP Runge-Kutta, Shu-Osher form (new) */
 
 #endif

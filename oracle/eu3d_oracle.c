@@ -835,9 +835,13 @@ void orc_step(orc_field *f, const orc_mech *m, int react, int type, int timeadv,
     const int NS = f->NS, bc = f->bc;
     if (cfl != 0) orc_cfl(f, cfl, final_time);
     orc_boundary(f, m, bc_kind, wedge);
-    if (timeadv == EU3D_ADV_SSPRK2) {
-        /* two-stage SSP Runge-Kutta for the advection (new), followed by the
-           chemistry as a split step with a zero flux residual */
+    if (timeadv == EU3D_ADV_SSPRK2 || timeadv == EU3D_ADV_SSPRK3) {
+        /* SSP Runge-Kutta for the advection (new), followed by the chemistry
+           as a split step with a zero flux residual.  Two stages:
+           CS1 = CS^n + R(CS^n), CS^{n+1} = 1/2 CS^n + 1/2 (CS1 + R(CS1)).
+           Three (Shu-Osher): CS1 as above, CS2 = 3/4 CS^n + 1/4 (CS1 + R(CS1)),
+           CS^{n+1} = 1/3 CS^n + 2/3 (CS2 + R(CS2)). */
+        const int stages = timeadv == EU3D_ADV_SSPRK2 ? 2 : 3;
         size_t n = (size_t)f->NI * f->NJ * f->NK * (NS + 4);
         double *cs0 = (double *)malloc(n * sizeof(double));
         memcpy(cs0, f->CS, n * sizeof(double));
@@ -847,15 +851,20 @@ void orc_step(orc_field *f, const orc_mech *m, int react, int type, int timeadv,
                 for (int k = bc; k < f->nk + bc; k++)
                     for (int s = 0; s < NS + 4; s++) f->CS[ID4(f, i, j, k, s, NS + 4)] += f->RHS[ID4(f, i, j, k, s, NS + 4)];
         orc_update_after_cs(f, m);
-        orc_boundary(f, m, bc_kind, wedge);
-        orc_advection(f, EU3D_ADV_EE, diff);
-        for (int i = bc; i < f->ni + bc; i++)
-            for (int j = bc; j < f->nj + bc; j++)
-                for (int k = bc; k < f->nk + bc; k++)
-                    for (int s = 0; s < NS + 4; s++) {
-                        size_t o = ID4(f, i, j, k, s, NS + 4);
-                        f->CS[o] = 0.5 * cs0[o] + 0.5 * (f->CS[o] + f->RHS[o]);
-                    }
+        for (int stage = 2; stage <= stages; stage++) {
+            const double wn = stages == 2 ? 0.5 : stage == 2 ? 0.75 : 1.0 / 3.0;
+            const double ws = stages == 2 ? 0.5 : stage == 2 ? 0.25 : 2.0 / 3.0;
+            orc_boundary(f, m, bc_kind, wedge);
+            orc_advection(f, EU3D_ADV_EE, diff);
+            for (int i = bc; i < f->ni + bc; i++)
+                for (int j = bc; j < f->nj + bc; j++)
+                    for (int k = bc; k < f->nk + bc; k++)
+                        for (int s = 0; s < NS + 4; s++) {
+                            size_t o = ID4(f, i, j, k, s, NS + 4);
+                            f->CS[o] = wn * cs0[o] + ws * (f->CS[o] + f->RHS[o]);
+                        }
+            if (stage < stages) orc_update_after_cs(f, m);
+        }
         free(cs0);
         orc_update_after_cs(f, m);
         memset(f->RHS, 0, n * sizeof(double));

@@ -67,9 +67,9 @@ class OracleSlab(Slab):
 
     def part(self, part, spec):
         o = self.o
-        rk2 = spec.timeadv == gpu.ADV_SSPRK2
+        rk = spec.timeadv in (gpu.ADV_SSPRK2, gpu.ADV_SSPRK3)
         if part == gpu.PART_STAGE1:
-            if rk2:
+            if rk:
                 self._cs0 = o.view("CS").copy()
                 o.advection(gpu.ADV_EE, spec.diff)
                 cs = self._interior("CS")
@@ -77,16 +77,21 @@ class OracleSlab(Slab):
                 o.update_after_cs()
             else:
                 o.advection(spec.timeadv, spec.diff)
-        elif part == gpu.PART_STAGE2:
+        elif part in (gpu.PART_STAGE2, gpu.PART_STAGE3):
+            # SSP-RK2: 1/2, 1/2; SSP-RK3 (Shu-Osher): 3/4, 1/4 then 1/3, 2/3
+            wn, ws = ((0.5, 0.5) if spec.timeadv == gpu.ADV_SSPRK2 else
+                      (0.75, 0.25) if part == gpu.PART_STAGE2 else (1.0 / 3.0, 2.0 / 3.0))
+            last = spec.timeadv == gpu.ADV_SSPRK2 or part == gpu.PART_STAGE3
             o.advection(gpu.ADV_EE, spec.diff)
             b = o.bc
             cs0 = self._cs0[b:o.ni + b, b:o.nj + b, b:o.nk + b]
             cs, rhs = self._interior("CS"), self._interior("RHS")
-            cs[...] = 0.5 * cs0 + 0.5 * (cs + rhs)
+            cs[...] = wn * cs0 + ws * (cs + rhs)
             o.update_after_cs()
-            o.view("RHS")[...] = 0.0
+            if last:
+                o.view("RHS")[...] = 0.0
         elif part == gpu.PART_REACT:
-            if rk2:
+            if rk:
                 if spec.react == gpu.REACT_IMEX:
                     o.partial_t()
                     o.imex()

@@ -55,6 +55,12 @@ def test_constants_match_quirk_header():
     assert num(vals["EU3D_BC_ODM"]) == gpu.BC_ODM
     assert num(vals["EU3D_REACT_IMEX"]) == gpu.REACT_IMEX
     assert num(vals["EU3D_ADV_SSPRK2"]) == gpu.ADV_SSPRK2
+    assert num(vals["EU3D_ADV_SSPRK3"]) == gpu.ADV_SSPRK3
+    text = open(os.path.join(ROOT, "include", "eu3d_gpu.h")).read()
+    parts = dict(re.findall(r"#define (EU3D_PART_\w+) (\d+)", text))
+    assert {k: int(v) for k, v in parts.items()} == {"EU3D_PART_STAGE1": gpu.PART_STAGE1, "EU3D_PART_STAGE2":
+                                                     gpu.PART_STAGE2, "EU3D_PART_REACT": gpu.PART_REACT,
+                                                     "EU3D_PART_STAGE3": gpu.PART_STAGE3}
 
 
 def test_null_arguments_are_rejected_without_a_device(lib):

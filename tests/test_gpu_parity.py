@@ -162,6 +162,8 @@ STEP_CASES = {
     ("imex", QUIRKS_REF): (COOL, 0.3, 0.0, 4),
     ("imex_rk2", QUIRKS_FIXED): (HOT, 0.3, 0.0, 4),
     ("imex_rk2", QUIRKS_REF): (COOL, 0.3, 0.0, 4),
+    ("imex_rk3", QUIRKS_FIXED): (HOT, 0.3, 0.0, 4),
+    ("imex_rk3", QUIRKS_REF): (COOL, 0.3, 0.0, 4),
     ("trap0", QUIRKS_FIXED): (MILD, 0.0, 1e-8, 4),
     ("trap0", QUIRKS_REF): (COOL, 0.0, 1e-8, 1),
     ("trap1", QUIRKS_FIXED): (SUBSTEP, 0.0, 1e-8, 2),
@@ -169,7 +171,7 @@ STEP_CASES = {
     ("nochem", QUIRKS_FIXED): (HOT, 0.3, 0.0, 4),
     ("nochem", QUIRKS_REF): (COOL, 0.3, 0.0, 1),
 }
-SCHEMES = {"imex": (1, 0, 0), "imex_rk2": (1, 0, 2), "trap0": (0, 0, 0), "trap1": (0, 1, 0), "nochem": (2, 0, 0)}
+SCHEMES = {"imex": (1, 0, 0), "imex_rk2": (1, 0, 2), "imex_rk3": (1, 0, 3), "trap0": (0, 0, 0), "trap1": (0, 1, 0), "nochem": (2, 0, 0)}
 
 
 @pytest.mark.parametrize("gname", list(GRIDS))

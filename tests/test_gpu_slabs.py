@@ -46,6 +46,8 @@ def _compare(full, pieces, bc=2, names=("CS", "T", "P", "Yi")):
     (3, "partition", 64, gpu.ADV_EE),
     (2, "partition", 32, gpu.ADV_SSPRK2),
     (3, "reference", 32, gpu.ADV_SSPRK2),
+    (2, "partition", 64, gpu.ADV_SSPRK3),
+    (3, "reference", 32, gpu.ADV_SSPRK3),
 ])
 def test_rsbi_slabs_equal_single_domain(mech, nranks, layout, flux_bits, timeadv):
     from _cases import fill_state

@@ -38,6 +38,7 @@ def _full_run(full, spec, steps):
 @pytest.mark.parametrize("nranks,layout,react,timeadv,cfl,bc", [
     (3, "partition", gpu.REACT_IMEX, gpu.ADV_EE, 0.5, gpu.BC_RSBI),
     (2, "partition", gpu.REACT_IMEX, gpu.ADV_SSPRK2, 0.5, gpu.BC_RSBI),
+    (3, "reference", gpu.REACT_IMEX, gpu.ADV_SSPRK3, 0.5, gpu.BC_RSBI),
     (3, "reference", gpu.REACT_IMEX, gpu.ADV_EE, 0.0, gpu.BC_RSBI),
     (4, "partition", gpu.REACT_NONE, gpu.ADV_EE, 0.3, gpu.BC_TRANSMISSIVE),
 ])
@@ -59,7 +60,8 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("layout,timeadv", [("partition", gpu.ADV_EE), ("partition", gpu.ADV_SSPRK2)])
+@pytest.mark.parametrize("layout,timeadv", [("partition", gpu.ADV_EE), ("partition", gpu.ADV_SSPRK2),
+                                            ("partition", gpu.ADV_SSPRK3)])
 def test_two_gloo_ranks_equal_single_domain(mech, tmp_path, layout, timeadv):
     port, world, steps, cfl = _free_port(), 2, 3, 0.5
     outs = [str(tmp_path / f"rank{r}.npz") for r in range(world)]
