@@ -315,8 +315,8 @@ bool make_prim_map(eu3d_handle *h)
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <class P>
-void launch_adv(eu3d_handle *h, int diff)
+template <class P, int DIFF>
+void launch_adv_t(eu3d_handle *h)
 {
     const int sq = (h->quirks & EU3D_Q_SPECIES_FACES) ? 1 : 0;
     const Layout &L = h->L;
@@ -326,36 +326,50 @@ void launch_adv(eu3d_handle *h, int diff)
     dim3 b(FT_X, TY + 2);
     constexpr size_t smem = FluxTile<P>::SMEM;
     ProfScope ps(h, "advection");
-    if (sizeof(P) == 4 && h->flux_stage == 2 && h->tq_ok) {
-        dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
-        dim3 bs(FT_X, FR_TY + 2);
+    if constexpr (sizeof(P) == 4) {
         const float *qf = (const float *)h->prim;
-        if (diff == EU3D_DIFF_MUSCL1)
-            k_flux_ring<EU3D_DIFF_MUSCL1><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn,
-                                                                            h->scal, h->rhs, sq, kz, h->status);
-        else
-            k_flux_ring<EU3D_DIFF_MUSCL2><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn,
-                                                                            h->scal, h->rhs, sq, kz, h->status);
-        return;
+        if (h->flux_stage == 2 && h->tq_ok) {
+            dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
+            dim3 bs(FT_X, FR_TY + 2);
+            k_flux_ring<DIFF><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, h->rhs,
+                                                                 sq, kz, h->status);
+            return;
+        }
+        if (h->flux_stage) {
+            dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
+            dim3 bs(FT_X, FS_TY + 2);
+            k_flux_stage<DIFF><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal, h->rhs, sq,
+                                                                   kz);
+            return;
+        }
     }
-    if (sizeof(P) == 4 && h->flux_stage) {
-        dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
-        dim3 bs(FT_X, FS_TY + 2);
-        const float *qf = (const float *)h->prim;
-        if (diff == EU3D_DIFF_MUSCL1)
-            k_flux_stage<EU3D_DIFF_MUSCL1><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal,
-                                                                              h->rhs, sq, kz);
-        else
-            k_flux_stage<EU3D_DIFF_MUSCL2><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal,
-                                                                              h->rhs, sq, kz);
-        return;
-    }
+    k_flux_tile<P, DIFF><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal, h->rhs, sq, kz);
+}
+
+template <class P>
+void launch_adv(eu3d_handle *h, int diff)
+{
     if (diff == EU3D_DIFF_MUSCL1)
-        k_flux_tile<P, EU3D_DIFF_MUSCL1><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                                 h->rhs, sq, kz);
+        launch_adv_t<P, EU3D_DIFF_MUSCL1>(h);
+    else if (diff == EU3D_DIFF_MUSCL2)
+        launch_adv_t<P, EU3D_DIFF_MUSCL2>(h);
     else
-        k_flux_tile<P, EU3D_DIFF_MUSCL2><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal,
-                                                                 h->rhs, sq, kz);
+        launch_adv_t<P, EU3D_DIFF_WENO>(h);
+}
+
+// dynamic shared memory of the tiled flux kernels (above the 48 KB default);
+// the TMA ring kernel runs two blocks per SM
+template <int DIFF>
+void flux_attributes()
+{
+    cudaFuncSetAttribute(k_flux_ring<DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FluxRing::SMEM);
+    cudaFuncSetAttribute(k_flux_ring<DIFF>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_flux_stage<DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FluxStage::SMEM);
+    cudaFuncSetAttribute(k_flux_tile<float, DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)FluxTile<float>::SMEM);
+    cudaFuncSetAttribute(k_flux_tile<double, DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)FluxTile<double>::SMEM);
 }
 
 int adv_op(eu3d_handle *h, int timeadv, int diff)
@@ -914,30 +928,11 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     cudaMemcpyAsync(h->yn, d->ynode, L.NJ * sizeof(double), cudaMemcpyHostToDevice, h->st);
     cudaMemcpyAsync(h->zn, d->znode, L.NK * sizeof(double), cudaMemcpyHostToDevice, h->st);
     {
-        // dynamic shared memory of the tiled flux kernels (above the 48 KB default);
-        // the TMA ring kernel runs two blocks per SM
-        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxRing::SMEM);
-        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxRing::SMEM);
-        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL1>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        cudaFuncSetAttribute(k_flux_ring<EU3D_DIFF_MUSCL2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
+        flux_attributes<EU3D_DIFF_MUSCL1>();
+        flux_attributes<EU3D_DIFF_MUSCL2>();
+        flux_attributes<EU3D_DIFF_WENO>();
         h->tq_ok = make_prim_map(h);
         if (!h->tq_ok) h->flux_stage = 1;
-        cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxStage::SMEM);
-        cudaFuncSetAttribute(k_flux_stage<EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxStage::SMEM);
-        cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxTile<float>::SMEM);
-        cudaFuncSetAttribute(k_flux_tile<float, EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxTile<float>::SMEM);
-        cudaFuncSetAttribute(k_flux_tile<double, EU3D_DIFF_MUSCL1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxTile<double>::SMEM);
-        cudaFuncSetAttribute(k_flux_tile<double, EU3D_DIFF_MUSCL2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)FluxTile<double>::SMEM);
     }
     if (g_mech_refs == 0) {
         cudaError_t e = cudaMemcpyToSymbol(cM, &m, sizeof(m));
@@ -1331,7 +1326,7 @@ int eu3d_advection(eu3d_handle *h, int timeadv, int diff)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
     if (timeadv != EU3D_ADV_EE && timeadv != EU3D_ADV_TVD_RK3) return fail(EU3D_ERR_ARG, "timeadv must be EE or TVD_RK3");
-    if (diff != EU3D_DIFF_MUSCL1 && diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
+    if (diff < EU3D_DIFF_MUSCL1 || diff > EU3D_DIFF_WENO) return fail(EU3D_ERR_ARG, "unknown difference scheme");
     return adv_op(h, timeadv, diff);
 }
 
@@ -1354,7 +1349,7 @@ int prepare_step(eu3d_handle *h, const eu3d_step_desc *s)
 {
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (s->timeadv < EU3D_ADV_EE || s->timeadv > EU3D_ADV_SSPRK3) return fail(EU3D_ERR_ARG, "unknown time scheme");
-    if (s->diff != EU3D_DIFF_MUSCL1 && s->diff != EU3D_DIFF_MUSCL2) return fail(EU3D_ERR_ARG, "unknown difference scheme");
+    if (s->diff < EU3D_DIFF_MUSCL1 || s->diff > EU3D_DIFF_WENO) return fail(EU3D_ERR_ARG, "unknown difference scheme");
     if (s->react != EU3D_REACT_IMEX && s->react != EU3D_REACT_TRAPEZOID && s->react != EU3D_REACT_NONE &&
         s->react != EU3D_REACT_SURROGATE && s->react != EU3D_REACT_ADAPTIVE)
         return fail(EU3D_ERR_ARG, "unsupported reaction scheme");

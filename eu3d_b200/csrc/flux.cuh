@@ -29,13 +29,42 @@ __device__ __forceinline__ P minmod_lim(P R)
     return (R > P(0)) ? ((P(1) < R) ? P(1) : R) : P(0);
 }
 
+// Third-order WENO (Jiang and Shu, J. Comput. Phys. 126, 1996; new -- the
+// reference's WENO enum value has no scheme behind it): the state at the face
+// of cell ctr towards oth from the candidates ctr + (ctr - far)/2 and
+// ctr + (oth - ctr)/2, linear weights 1/3 and 2/3, smoothness indicators the
+// squared differences, epsilon 1e-6; w0 = q1 / (q1 + 2 q0), q = (eps + beta)^2.
+// Every operation is rounded explicitly so that no kernel contracts it
+// differently (FP64: the oracle's IEEE sequence; FP32: one sequence for all
+// FP32 kernels).
+__device__ __forceinline__ double weno3(double far, double ctr, double oth)
+{
+    const double A0 = ctr - far, A1 = oth - ctr;
+    double q0 = __dadd_rn(1e-6, __dmul_rn(A0, A0)), q1 = __dadd_rn(1e-6, __dmul_rn(A1, A1));
+    q0 = __dmul_rn(q0, q0);
+    q1 = __dmul_rn(q1, q1);
+    const double w0 = __ddiv_rn(q1, __dadd_rn(q1, __dmul_rn(2.0, q0)));
+    return __dadd_rn(ctr, __dmul_rn(0.5, __dadd_rn(A1, __dmul_rn(w0, __dsub_rn(A0, A1)))));
+}
+
+__device__ __forceinline__ float weno3(float far, float ctr, float oth)
+{
+    const float A0 = ctr - far, A1 = oth - ctr;
+    const float s0 = __fmaf_rn(A0, A0, 1e-6f), s1 = __fmaf_rn(A1, A1, 1e-6f);
+    const float q0 = __fmul_rn(s0, s0), q1 = __fmul_rn(s1, s1);
+    const float w0 = __fdividef(q1, __fmaf_rn(2.0f, q0, q1));
+    return __fmaf_rn(0.5f, __fmaf_rn(w0, A0 - A1, A1), ctr);
+}
+
 // MUSCL_2 (limiter 0) face states, include/Differ.hpp:149-238 (MUSCL_1 when
-// DIFF == 0, :110-136): the left state of the face (i, i+1) from f(i-1),
-// f(i), f(i+1), the right state from f(i), f(i+1), f(i+2).
+// DIFF == 0, :110-136; WENO above when DIFF == 2): the left state of the face
+// (i, i+1) from f(i-1), f(i), f(i+1), the right state from f(i), f(i+1),
+// f(i+2).
 template <class P, int DIFF>
 __device__ __forceinline__ P recon_left(P a, P b, P c)
 {
     if (DIFF == EU3D_DIFF_MUSCL1) return b;
+    if (DIFF == EU3D_DIFF_WENO) return weno3(a, b, c);
     const P kk = P(1.0) / P(3.0);
     P A0 = b - a, A1 = c - b;
     P Lr = A1 / (A0 + P(1e-12));
@@ -47,6 +76,7 @@ template <class P, int DIFF>
 __device__ __forceinline__ P recon_right(P b, P c, P d)
 {
     if (DIFF == EU3D_DIFF_MUSCL1) return c;
+    if (DIFF == EU3D_DIFF_WENO) return weno3(d, c, b);
     const P kk = P(1.0) / P(3.0);
     P A1 = c - b, A2 = d - c;
     P Rr = A1 / (A2 + P(1e-12));
@@ -153,6 +183,7 @@ __device__ __forceinline__ void face_flux_src(const Src &src, bool zspec, float 
         float far, ctr, oth;
         src.up3(f, left, far, ctr, oth);
         if (DIFF == EU3D_DIFF_MUSCL1) return ctr;
+        if (DIFF == EU3D_DIFF_WENO) return weno3(far, ctr, oth);
         return up_muscl2(far, ctr, oth, seps);
     };
     const float Ds = left ? DL : DR;

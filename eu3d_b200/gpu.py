@@ -23,7 +23,7 @@ QUIRKS_REF = 0x1FF
 QUIRKS_FIXED = 0x000
 BC_RSBI, BC_ODM, BC_TRANSMISSIVE, BC_NONE = 0, 1, 2, 3
 REACT_TRAPEZOID, REACT_IMEX, REACT_NONE, REACT_SURROGATE, REACT_ADAPTIVE = 0, 1, 2, 3, 4
-DIFF_MUSCL1, DIFF_MUSCL2 = 0, 1
+DIFF_MUSCL1, DIFF_MUSCL2, DIFF_WENO = 0, 1, 2
 ADV_EE, ADV_TVD_RK3, ADV_SSPRK2, ADV_SSPRK3 = 0, 1, 2, 3
 
 FIELDS = {"U": 0, "V": 1, "W": 2, "P": 3, "D": 4, "T": 5, "H": 6, "Gamma": 7, "E": 8, "Yi": 9, "CS": 10, "RHS": 11,

@@ -57,6 +57,9 @@
 /* Spatial schemes (include/Global.hpp DIFF) */
 #define EU3D_DIFF_MUSCL1 0
 #define EU3D_DIFF_MUSCL2 1
+#define EU3D_DIFF_WENO 2 /* the reference's WENO value (no scheme behind it there, src/Flowfield.cpp:1101-1109):
+                            here third-order WENO, Jiang-Shu weights, epsilon 1e-6, on the same
+                            three-cell stencils as MUSCL_2 (two ghost layers suffice) (new) */
 
 /* Time schemes (include/Global.hpp ADV) */
 #define EU3D_ADV_EE 0

@@ -125,8 +125,24 @@ static double minmod(double R)
     return mm;
 }
 
+/* Third-order WENO (Jiang and Shu, J. Comput. Phys. 126, 1996; new -- the
+   reference's WENO enum value has no scheme behind it): the state at the face
+   of cell `ctr` towards `oth`, from the two-point candidates
+   ctr + (ctr - far)/2 and ctr + (oth - ctr)/2 with linear weights 1/3, 2/3 and
+   smoothness indicators (ctr - far)^2, (oth - ctr)^2, epsilon 1e-6:
+   w0 = (1/3)/q0 / ((1/3)/q0 + (2/3)/q1) = q1 / (q1 + 2 q0), q = (eps + beta)^2. */
+static double weno3(double far, double ctr, double oth)
+{
+    const double A0 = ctr - far, A1 = oth - ctr;
+    double q0 = 1e-6 + A0 * A0, q1 = 1e-6 + A1 * A1;
+    q0 = q0 * q0;
+    q1 = q1 * q1;
+    const double w0 = q1 / (q1 + 2.0 * q0);
+    return ctr + 0.5 * (A1 + w0 * (A0 - A1));
+}
+
 /* MUSCL_2 with limiter 0 (include/Differ.hpp:149-238) or MUSCL_1
-   (include/Differ.hpp:110-136) into FLR (NI x NJ x NK x 2) */
+   (include/Differ.hpp:110-136), or WENO (above), into FLR (NI x NJ x NK x 2) */
 static void muscl(const orc_field *f, int dir, int diff, const double *fi, size_t stride, double *FLR)
 {
     const int bc = f->bc;
@@ -145,6 +161,11 @@ static void muscl(const orc_field *f, int dir, int diff, const double *fi, size_
                     continue;
                 }
                 double f2 = fi[ID3(f, i + 2 * di, j + 2 * dj, k + 2 * dk) * stride];
+                if (diff == EU3D_DIFF_WENO) {
+                    FLR[o] = weno3(fm1, f0, f1);
+                    FLR[o + 1] = weno3(f2, f1, f0);
+                    continue;
+                }
                 double A0 = f0 - fm1;
                 double A1 = f1 - f0;
                 double A2 = f2 - f1;

@@ -56,6 +56,7 @@ def test_constants_match_quirk_header():
     assert num(vals["EU3D_REACT_IMEX"]) == gpu.REACT_IMEX
     assert num(vals["EU3D_ADV_SSPRK2"]) == gpu.ADV_SSPRK2
     assert num(vals["EU3D_ADV_SSPRK3"]) == gpu.ADV_SSPRK3
+    assert num(vals["EU3D_DIFF_WENO"]) == gpu.DIFF_WENO
     text = open(os.path.join(ROOT, "include", "eu3d_gpu.h")).read()
     parts = dict(re.findall(r"#define (EU3D_PART_\w+) (\d+)", text))
     assert {k: int(v) for k, v in parts.items()} == {"EU3D_PART_STAGE1": gpu.PART_STAGE1, "EU3D_PART_STAGE2":

@@ -80,7 +80,7 @@ def test_wedge_parity(mech):
         assert rel_err(d.download(n), o.view(n)) < TOL_FN, n
 
 
-@pytest.mark.parametrize("diff", [gpu.DIFF_MUSCL1, gpu.DIFF_MUSCL2], ids=["muscl1", "muscl2"])
+@pytest.mark.parametrize("diff", [gpu.DIFF_MUSCL1, gpu.DIFF_MUSCL2, gpu.DIFF_WENO], ids=["muscl1", "muscl2", "weno"])
 @pytest.mark.parametrize("quirks", [QUIRKS_FIXED, QUIRKS_REF], ids=["fixed", "ref"])
 def test_advection_parity(mech, quirks, diff):
     o, g = make_oracle(mech, seed=4, quirks=quirks, **policy(quirks))
@@ -225,16 +225,34 @@ def test_gpu_reproduces_reference_fixture(mech, case_idx):
         assert rel_err(interior(d.download(f)), ref) < TOL_STEP, f
 
 
-def test_fp32_flux_error_bound(mech):
+@pytest.mark.parametrize("diff", [gpu.DIFF_MUSCL2, gpu.DIFF_WENO], ids=["muscl2", "weno"])
+def test_fp32_flux_error_bound(mech, diff):
     """Mixed precision (FP32 reconstruction/AUSM, FP64 state) against the
     all-FP64 oracle: stated bound 5e-5 field-normalised after 3 steps."""
     o, g = make_oracle(mech, seed=14, quirks=QUIRKS_FIXED, **HOT)
     d = to_gpu(o, g, QUIRKS_FIXED, flux_bits=32)
     for _ in range(3):
-        o.step(1, 0, 0, 1, 0.3, 1.0, gpu.BC_RSBI)
-        d.step(react=1, bc_kind=gpu.BC_RSBI, cfl=0.3)
+        o.step(1, 0, 0, diff, 0.3, 1.0, gpu.BC_RSBI)
+        d.step(react=1, diff=diff, bc_kind=gpu.BC_RSBI, cfl=0.3)
     e, errs = worst(d, o, names=["CS", "T", "P", "D"])
     assert e < 5e-5, errs
+
+
+@pytest.mark.parametrize("gname", list(GRIDS))
+@pytest.mark.parametrize("quirks", [QUIRKS_FIXED, QUIRKS_REF], ids=["fixed", "ref"])
+def test_weno_rk3_steps_parity(mech, quirks, gname):
+    """The WENO reconstruction with the three-stage SSP Runge-Kutta scheme
+    (both new) through eu3d_step: four CFL-limited IMEX steps, 1e-10."""
+    st = policy(quirks)
+    g = small_grid(fixed_ghosts=(quirks == QUIRKS_FIXED), **GRIDS[gname])
+    o, g = make_oracle(mech, seed=15, quirks=quirks, grid=g, **st)
+    d = to_gpu(o, g, quirks)
+    for _ in range(4):
+        o.step(gpu.REACT_IMEX, 0, gpu.ADV_SSPRK3, gpu.DIFF_WENO, 0.3, 1.0, gpu.BC_RSBI)
+        d.step(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK3, diff=gpu.DIFF_WENO, bc_kind=gpu.BC_RSBI, cfl=0.3)
+    assert np.isfinite(interior(o.view("T"))).all()
+    e, errs = worst(d, o)
+    assert e < TOL_STEP, errs
 
 
 def test_nonfinite_state_is_reported_not_faulted(mech):

@@ -60,12 +60,14 @@ def test_autotune_restores_state_and_sets_best(mech):
                                                  ((33, 9, 4), 4, gpu.DIFF_MUSCL2, QUIRKS_FIXED),
                                                  ((70, 19, 9), 1, gpu.DIFF_MUSCL2, QUIRKS_REF),
                                                  ((40, 17, 7), 16, gpu.DIFF_MUSCL1, QUIRKS_REF),
-                                                 ((96, 24, 12), 5, gpu.DIFF_MUSCL2, QUIRKS_FIXED)])
+                                                 ((96, 24, 12), 5, gpu.DIFF_MUSCL2, QUIRKS_FIXED),
+                                                 ((70, 19, 9), 4, gpu.DIFF_WENO, QUIRKS_FIXED),
+                                                 ((40, 17, 7), 16, gpu.DIFF_WENO, QUIRKS_REF)])
 def test_flux_staged_equals_l1_path(mech, dims, kz, diff, quirks):
     """The three FP32 flux kernels -- primitives read through L1 (0), staged
     into shared memory by loads (1), brought into a shared-memory ring by
     TMA (2) -- give the same residual bit for bit, over ragged tiles, blocks
-    of one to many z planes, both reconstructions and the species-face quirk."""
+    of one to many z planes, the three reconstructions and the species-face quirk."""
     g = small_grid(*dims)
     o = Oracle(mech, g, quirks)
     fill_state(o, 5, 1100.0, 2600.0)
