@@ -519,6 +519,7 @@ constexpr int QBINS = 32;
 struct ChemQueue {
     int *list;   // interior cells in bin order
     int *bins;   // [0, 32) counts, [32, 64) start offsets, [64, 96) fill cursors, [96] work cursor, [97] total
+    long long away_lo = 0, away_hi = 0;  // interior rows (k nj + j) integrated on another rank
 };
 
 __device__ __forceinline__ int nchem_bin(int n) { return 31 - __clz(max(n, 1)); }
@@ -774,6 +775,8 @@ __global__ void k_queue_scatter(CellArgs a, ChemQueue qu)
     const int k = L.bc + blockIdx.z;
     if (i >= L.ni + L.bc) return;
     if (solid_cell(a, i, j)) return;
+    const long long row = (long long)blockIdx.z * L.nj + blockIdx.y;
+    if (row >= qu.away_lo && row < qu.away_hi) return;
     const long long c = L.at(i, j, k);
     const int b = nchem_bin(a.nchem[c]);
     const unsigned act = __activemask();

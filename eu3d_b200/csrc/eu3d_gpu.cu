@@ -23,6 +23,7 @@
 #include "mlp.cuh"
 #include "surrogate.cuh"
 #include "tecplot.cuh"
+#include "dlb.cuh"
 
 using namespace eu3d;
 
@@ -116,6 +117,16 @@ struct eu3d_handle {
     std::vector<double> tp_nodes;  // ghosted x, y, z node coordinates
     std::thread writer;
     std::string writer_err;
+    // dynamic load balancing of the adaptive trapezoid (eu3d_chem_load, eu3d_dlb_*)
+    long long *dlb_rowload = nullptr;  // per interior row, device
+    std::vector<long long> dlb_rows;   // host copy of the last eu3d_chem_load
+    DlbSegs dlb_segs{};                // the transfers this rank sends (rows, offsets in DLB_OUT fields)
+    long long away_lo = 0, away_hi = 0;  // rows the next queue pass leaves to other ranks
+    // guest store: cells received from other ranks, field stride g_cap
+    long long g_cap = 0;
+    double *g_cs = nullptr, *g_T = nullptr, *g_E = nullptr;
+    int *g_nchem = nullptr, *g_list = nullptr, *g_bins = nullptr;
+    void *g_prim = nullptr;
 };
 
 namespace {
@@ -217,28 +228,59 @@ int queue_grid(const eu3d_handle *h)
     return sms * h->queue_blocks;
 }
 
-// Adaptive trapezoid on the work queue: predict + bin, offsets, list, workers.
+// Adaptive trapezoid on the work queue: predict + bin, then offsets, list,
+// workers.  Between the two a multi-rank driver may hand rows to other ranks
+// (eu3d_dlb_pack), which the list then leaves out.
 template <class P, bool SPEC>
-void launch_trap1_queue(eu3d_handle *h)
+void trap1_predict(eu3d_handle *h)
 {
     CellArgs a = cell_args(h);
-    P *q = (P *)h->prim;
-    dim3 g = cell_grid(h->L, 128);
-    ChemQueue qu{h->qlist, h->qbins};
     cudaMemsetAsync(h->qbins, 0, QBINS * sizeof(int), h->st);
-    {
-        ProfScope ps(h, "trap1_predict");
-        k_cell<P, M_TRAP1_PREDICT, SPEC><<<g, 128, 0, h->st>>>(a, q);
-    }
+    h->away_lo = h->away_hi = 0;
+    h->dlb_segs.n = 0;  // a new prediction: no rows selected yet
+    ProfScope ps(h, "trap1_predict");
+    k_cell<P, M_TRAP1_PREDICT, SPEC><<<cell_grid(h->L, 128), 128, 0, h->st>>>(a, (P *)h->prim);
+}
+
+template <class P, bool SPEC>
+void trap1_work(eu3d_handle *h)
+{
+    CellArgs a = cell_args(h);
+    ChemQueue qu{h->qlist, h->qbins, h->away_lo, h->away_hi};
     {
         ProfScope ps(h, "trap1_list");
         k_queue_scan<<<1, 32, 0, h->st>>>(qu);
-        k_queue_scatter<<<g, 128, 0, h->st>>>(a, qu);
+        k_queue_scatter<<<cell_grid(h->L, 128), 128, 0, h->st>>>(a, qu);
     }
     {
         ProfScope ps(h, "trap1_work");
-        k_trap1_work<P, SPEC><<<queue_grid(h), 128, 0, h->st>>>(a, q, qu);
+        k_trap1_work<P, SPEC><<<queue_grid(h), 128, 0, h->st>>>(a, (P *)h->prim, qu);
     }
+}
+
+template <class P, bool SPEC>
+void launch_trap1_queue(eu3d_handle *h)
+{
+    trap1_predict<P, SPEC>(h);
+    trap1_work<P, SPEC>(h);
+}
+
+// one half of the queued adaptive trapezoid: 0 predict, 1 work
+int trap1_part(eu3d_handle *h, int half)
+{
+    if (h->flux_bits == 64) {
+        if (h->spec)
+            half ? trap1_work<double, true>(h) : trap1_predict<double, true>(h);
+        else
+            half ? trap1_work<double, false>(h) : trap1_predict<double, false>(h);
+    } else {
+        if (h->spec)
+            half ? trap1_work<float, true>(h) : trap1_predict<float, true>(h);
+        else
+            half ? trap1_work<float, false>(h) : trap1_predict<float, false>(h);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
 }
 
 template <class P>
@@ -654,7 +696,8 @@ void free_handle(eu3d_handle *h)
     void *ptrs[] = {h->cs,      h->rhs,    h->cs0,    h->T,       h->E,         h->prim,
                     h->nchem,   h->xn,     h->yn,     h->zn,      h->scal,      h->partial,
                     h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
-                    h->sur_audit, h->qlist,   h->qbins,  h->wedge_band};
+                    h->sur_audit, h->qlist,   h->qbins,  h->wedge_band, h->dlb_rowload, h->g_cs,
+                    h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->writer.joinable()) h->writer.join();
@@ -1312,8 +1355,226 @@ int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part)
         if (s->timeadv != EU3D_ADV_SSPRK3) return fail(EU3D_ERR_ARG, "stage 3 exists for SSP-RK3 only");
         return stage_op(h, s, 3);
     case EU3D_PART_REACT: return react_op(h, s);
+    case EU3D_PART_CHEM_PREDICT:
+    case EU3D_PART_CHEM_WORK:
+        if (s->react != EU3D_REACT_TRAPEZOID || s->type != 1)
+            return fail(EU3D_ERR_ARG, "the chemistry halves exist for the adaptive trapezoid (type 1) only");
+        if (!h->chem_queue || !h->qlist) return fail(EU3D_ERR_STATE, "the chemistry halves need the work queue");
+        return trap1_part(h, part == EU3D_PART_CHEM_WORK ? 1 : 0);
     default: return fail(EU3D_ERR_ARG, "unknown step part");
     }
+}
+
+// ---------------------------------------------------------------------------
+// Dynamic load balancing of the adaptive trapezoid across ranks
+// (DynamicLoadBalancer, src/LoadBalance.cpp; Euler::Trapezoid type 1,
+// src/Euler.cpp:380-700).
+
+static_assert(EU3D_DLB_OUT_FIELDS == DLB_OUT && EU3D_DLB_BACK_FIELDS == DLB_BACK &&
+                  EU3D_DLB_MAX_TRANSFERS == DLB_MAXSEG,
+              "packet constants of the C ABI");
+
+int eu3d_dlb_plan(const long long *loads, int nranks, int cap, int *sender, int *receiver, long long *amount,
+                  int *ntransfers)
+{
+    if (!loads || !ntransfers || nranks < 1) return fail(EU3D_ERR_ARG, "bad arguments");
+    std::vector<int> s, r;
+    std::vector<long long> a;
+    dlb::plan(loads, nranks, s, r, a);
+    *ntransfers = (int)s.size();
+    if ((int)s.size() > cap || ((!sender || !receiver || !amount) && !s.empty()))
+        return fail(EU3D_ERR_ARG, "transfer arrays too small");
+    for (size_t t = 0; t < s.size(); t++) {
+        sender[t] = s[t];
+        receiver[t] = r[t];
+        amount[t] = a[t];
+    }
+    return EU3D_OK;
+}
+
+int eu3d_dlb_select_rows(const long long *rowload, long long nrows, int npacks, const long long *amount,
+                         long long *bounds, long long *moved)
+{
+    if (!rowload || nrows < 0 || npacks < 0 || (npacks && (!amount || !moved)) || !bounds)
+        return fail(EU3D_ERR_ARG, "bad arguments");
+    dlb::select_rows(rowload, nrows, npacks, amount, bounds, moved);
+    return EU3D_OK;
+}
+
+int eu3d_chem_load(eu3d_handle *h, long long *load)
+{
+    if (!h || !load) return fail(EU3D_ERR_ARG, "null argument");
+    if (!h->qlist) return fail(EU3D_ERR_STATE, "no queued chemistry prediction on this handle");
+    CK(cudaSetDevice(h->dev));
+    const Layout &L = h->L;
+    const long long nrows = (long long)L.nj * L.nk;
+    if (!h->dlb_rowload) CK(cudaMalloc(&h->dlb_rowload, (size_t)nrows * sizeof(long long)));
+    const int blocks = (int)std::min<long long>((nrows * 32 + 255) / 256, 148 * 16);
+    k_dlb_rowload<<<blocks, 256, 0, h->st>>>(cell_args(h), h->dlb_rowload);
+    CK(cudaGetLastError());
+    h->dlb_rows.resize((size_t)nrows);
+    CK(cudaMemcpyAsync(h->dlb_rows.data(), h->dlb_rowload, (size_t)nrows * sizeof(long long), cudaMemcpyDeviceToHost,
+                       h->st));
+    CK(cudaStreamSynchronize(h->st));
+    long long s = 0;
+    for (long long v : h->dlb_rows) s += v;
+    *load = s;
+    return EU3D_OK;
+}
+
+int eu3d_dlb_select(eu3d_handle *h, int ntransfers, const long long *amount, long long *cells, long long *moved)
+{
+    if (!h || ntransfers < 0 || ntransfers > DLB_MAXSEG || (ntransfers && (!amount || !cells || !moved)))
+        return fail(EU3D_ERR_ARG, "bad arguments");
+    const Layout &L = h->L;
+    const long long nrows = (long long)L.nj * L.nk;
+    if ((long long)h->dlb_rows.size() != nrows) return fail(EU3D_ERR_STATE, "eu3d_chem_load first");
+    long long bounds[DLB_MAXSEG + 1];
+    long long mv[DLB_MAXSEG];
+    dlb::select_rows(h->dlb_rows.data(), nrows, ntransfers, amount, bounds, mv);
+    DlbSegs &sg = h->dlb_segs;
+    sg.n = ntransfers;
+    long long off = 0;
+    for (int p = 0; p <= ntransfers; p++) sg.row[p] = bounds[p];
+    for (int p = 0; p < ntransfers; p++) {
+        cells[p] = (bounds[p + 1] - bounds[p]) * L.ni;
+        moved[p] = mv[p];
+        sg.off[p] = off;
+        off += DLB_OUT * cells[p];
+    }
+    return EU3D_OK;
+}
+
+int eu3d_dlb_pack(eu3d_handle *h, double *buf)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    const DlbSegs &sg = h->dlb_segs;
+    if (sg.n == 0 || sg.row[sg.n] == sg.row[0]) return EU3D_OK;
+    if (!buf) return fail(EU3D_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(h->dev));
+    const long long total = (sg.row[sg.n] - sg.row[0]) * h->L.ni;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    {
+        ProfScope ps(h, "dlb_pack");
+        k_dlb_pack<<<blocks, 256, 0, h->st>>>(cell_args(h), sg, buf, h->qbins);
+    }
+    CK(cudaGetLastError());
+    h->away_lo = sg.row[0];
+    h->away_hi = sg.row[sg.n];
+    return EU3D_OK;
+}
+
+extern "C++" {
+namespace {
+int ensure_guest(eu3d_handle *h, long long cells)
+{
+    if (cells <= h->g_cap) return EU3D_OK;
+    const long long cap = std::max<long long>(cells, 2 * h->g_cap);
+    void *old[] = {h->g_cs, h->g_T, h->g_E, h->g_nchem, h->g_list, h->g_prim};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    h->g_cs = h->g_T = h->g_E = nullptr;
+    h->g_nchem = h->g_list = nullptr;
+    h->g_prim = nullptr;
+    h->g_cap = 0;
+    CK(cudaMalloc(&h->g_cs, (size_t)NV * cap * sizeof(double)));
+    CK(cudaMalloc(&h->g_T, (size_t)cap * sizeof(double)));
+    CK(cudaMalloc(&h->g_E, (size_t)cap * sizeof(double)));
+    CK(cudaMalloc(&h->g_nchem, (size_t)cap * sizeof(int)));
+    CK(cudaMalloc(&h->g_list, (size_t)cap * sizeof(int)));
+    CK(cudaMalloc(&h->g_prim, (size_t)NPRIM * cap * prim_bytes(h)));
+    if (!h->g_bins) CK(cudaMalloc(&h->g_bins, (3 * QBINS + 2) * sizeof(int)));
+    h->g_cap = cap;
+    return EU3D_OK;
+}
+
+template <class P, bool SPEC>
+void guest_work(eu3d_handle *h, const DlbGuestSegs &sg, const double *in, double *out)
+{
+    const long long total = sg.first[sg.n];
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    ChemQueue qu{h->g_list, h->g_bins};
+    cudaMemsetAsync(h->g_bins, 0, (3 * QBINS + 2) * sizeof(int), h->st);
+    k_dlb_guest_in<<<blocks, 256, 0, h->st>>>(sg, in, h->g_cap, h->g_cs, h->g_T, h->g_nchem, h->g_bins);
+    k_queue_scan<<<1, 32, 0, h->st>>>(qu);
+    k_dlb_guest_list<<<blocks, 256, 0, h->st>>>(h->g_nchem, total, qu);
+    // the store as a field of g_cap cells: trap1_cell reads only the field
+    // stride of the layout
+    CellArgs a = cell_args(h);
+    a.L.fs = h->g_cap;
+    a.cs = h->g_cs;
+    a.T = h->g_T;
+    a.E = h->g_E;
+    a.nchem = h->g_nchem;
+    a.rhs = nullptr;
+    a.cs0 = nullptr;
+    a.wedge_on = 0;
+    {
+        ProfScope ps(h, "dlb_guest_work");
+        k_trap1_work<P, SPEC><<<queue_grid(h), 128, 0, h->st>>>(a, (P *)h->g_prim, qu);
+    }
+    k_dlb_guest_out<P><<<blocks, 256, 0, h->st>>>(sg, h->g_cap, h->g_cs, h->g_T, h->g_E, (const P *)h->g_prim,
+                                                  h->g_nchem, out);
+}
+}  // namespace
+}  // extern "C++"
+
+int eu3d_dlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *in, double *out)
+{
+    if (!h || nseg < 0 || nseg > DLB_MAXSEG || (nseg && !seg_cells)) return fail(EU3D_ERR_ARG, "bad arguments");
+    DlbGuestSegs sg{};
+    sg.n = nseg;
+    sg.first[0] = 0;
+    for (int s = 0; s < nseg; s++) {
+        if (seg_cells[s] < 0) return fail(EU3D_ERR_ARG, "negative segment size");
+        sg.off_in[s] = DLB_OUT * sg.first[s];
+        sg.off_out[s] = DLB_BACK * sg.first[s];
+        sg.first[s + 1] = sg.first[s] + seg_cells[s];
+    }
+    const long long total = sg.first[nseg];
+    if (total == 0) return EU3D_OK;
+    if (!in || !out) return fail(EU3D_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(h->dev));
+    int rc = ensure_guest(h, total);
+    if (rc) return rc;
+    if (h->flux_bits == 64) {
+        if (h->spec)
+            guest_work<double, true>(h, sg, in, out);
+        else
+            guest_work<double, false>(h, sg, in, out);
+    } else {
+        if (h->spec)
+            guest_work<float, true>(h, sg, in, out);
+        else
+            guest_work<float, false>(h, sg, in, out);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+int eu3d_dlb_unpack(eu3d_handle *h, const double *back)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    DlbSegs sg = h->dlb_segs;
+    if (sg.n == 0 || sg.row[sg.n] == sg.row[0]) return EU3D_OK;
+    if (!back) return fail(EU3D_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(h->dev));
+    long long off = 0;
+    for (int p = 0; p < sg.n; p++) {
+        sg.off[p] = off;
+        off += DLB_BACK * (sg.row[p + 1] - sg.row[p]) * h->L.ni;
+    }
+    const long long total = (sg.row[sg.n] - sg.row[0]) * h->L.ni;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    {
+        ProfScope ps(h, "dlb_unpack");
+        if (h->flux_bits == 64)
+            k_dlb_unpack<double><<<blocks, 256, 0, h->st>>>(cell_args(h), sg, back, (double *)h->prim);
+        else
+            k_dlb_unpack<float><<<blocks, 256, 0, h->st>>>(cell_args(h), sg, back, (float *)h->prim);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
 }
 
 int eu3d_boundary(eu3d_handle *h, int kind)

@@ -42,9 +42,12 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune",
            "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive", "eu3d_halo_bytes", "eu3d_halo_pack",
            "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
-           "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host"]
+           "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host", "eu3d_dlb_plan",
+           "eu3d_dlb_select_rows", "eu3d_chem_load", "eu3d_dlb_select", "eu3d_dlb_pack", "eu3d_dlb_guest",
+           "eu3d_dlb_unpack"]
 
-PART_STAGE1, PART_STAGE2, PART_REACT, PART_STAGE3 = 0, 1, 2, 3
+PART_STAGE1, PART_STAGE2, PART_REACT, PART_STAGE3, PART_CHEM_PREDICT, PART_CHEM_WORK = 0, 1, 2, 3, 4, 5
+DLB_OUT_FIELDS, DLB_BACK_FIELDS, DLB_MAX_TRANSFERS = 15, 32, 64
 
 SUR_NPARAM = 37264
 SUR_NORM_LEN = 80
@@ -166,6 +169,15 @@ def load_library(path: Optional[str] = None):
     L.eu3d_write_wait.argtypes = h
     L.eu3d_tecplot_write_host.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
                                           C.POINTER(C.c_int), C.c_double]
+    _lp = C.POINTER(C.c_longlong)
+    _ip = C.POINTER(C.c_int)
+    L.eu3d_dlb_plan.argtypes = [_lp, C.c_int, C.c_int, _ip, _ip, _lp, _ip]
+    L.eu3d_dlb_select_rows.argtypes = [_lp, C.c_longlong, C.c_int, _lp, _lp, _lp]
+    L.eu3d_chem_load.argtypes = h + [_lp]
+    L.eu3d_dlb_select.argtypes = h + [C.c_int, _lp, _lp, _lp]
+    L.eu3d_dlb_pack.argtypes = h + [C.c_void_p]
+    L.eu3d_dlb_guest.argtypes = h + [C.c_int, _lp, C.c_void_p, C.c_void_p]
+    L.eu3d_dlb_unpack.argtypes = h + [C.c_void_p]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]
@@ -361,6 +373,34 @@ class DeviceFlowfield:
     def halo_unpack(self, side: int, src_ptr: int):
         """Fill the two ghost planes of face `side` from the device buffer at src_ptr."""
         _check(self.L.eu3d_halo_unpack(self.h, side, C.c_void_p(src_ptr)))
+
+    # ---- load balancing of the adaptive trapezoid across ranks (eu3d_b200.slabs drives it)
+    def chem_load(self) -> int:
+        v = C.c_longlong()
+        _check(self.L.eu3d_chem_load(self.h, C.byref(v)))
+        return v.value
+
+    def dlb_select(self, amounts):
+        """Rows for this rank's transfers: (cells, moved load) per transfer."""
+        n = len(amounts)
+        a = np.ascontiguousarray(amounts, dtype=np.int64)
+        cells = np.zeros(n, dtype=np.int64)
+        moved = np.zeros(n, dtype=np.int64)
+        lp = C.POINTER(C.c_longlong)
+        _check(self.L.eu3d_dlb_select(self.h, n, a.ctypes.data_as(lp), cells.ctypes.data_as(lp),
+                                      moved.ctypes.data_as(lp)))
+        return cells, moved
+
+    def dlb_pack(self, dst_ptr: int):
+        _check(self.L.eu3d_dlb_pack(self.h, C.c_void_p(dst_ptr)))
+
+    def dlb_guest(self, seg_cells, src_ptr: int, dst_ptr: int):
+        s = np.ascontiguousarray(seg_cells, dtype=np.int64)
+        _check(self.L.eu3d_dlb_guest(self.h, len(s), s.ctypes.data_as(C.POINTER(C.c_longlong)), C.c_void_p(src_ptr),
+                                     C.c_void_p(dst_ptr)))
+
+    def dlb_unpack(self, src_ptr: int):
+        _check(self.L.eu3d_dlb_unpack(self.h, C.c_void_p(src_ptr)))
 
     def cfl_local(self, cfl: float, final_time: float):
         """This rank's CFL dt into the device scalar (time not advanced)."""
@@ -569,3 +609,41 @@ def write_tecplot_host(path: str, grid, cols, lcol, wait_time: float = 0.0):
     _check(L.eu3d_tecplot_write_host(path.encode(), grid.ni, grid.nj, grid.nk, grid.bc,
                                      *(a.ctypes.data_as(_dp) for a in xs), c.ctypes.data_as(_dp),
                                      lc.ctypes.data_as(C.POINTER(C.c_int)), wait_time))
+
+
+def dlb_plan(loads):
+    """DynamicLoadBalancer::DLBPriorityQueue (src/LoadBalance.cpp:8-59) through
+    the library: [(sender, receiver, amount)] in the reference's order."""
+    L = load_library()
+    a = np.ascontiguousarray(loads, dtype=np.int64)
+    n = len(a)
+    cap = max(1, n * n)
+    snd = np.zeros(cap, dtype=np.int32)
+    rcv = np.zeros(cap, dtype=np.int32)
+    amt = np.zeros(cap, dtype=np.int64)
+    m = C.c_int()
+    lp, ip = C.POINTER(C.c_longlong), C.POINTER(C.c_int)
+    _check(L.eu3d_dlb_plan(a.ctypes.data_as(lp), n, cap, snd.ctypes.data_as(ip), rcv.ctypes.data_as(ip),
+                           amt.ctypes.data_as(lp), C.byref(m)))
+    return [(int(snd[t]), int(rcv[t]), int(amt[t])) for t in range(m.value)]
+
+
+def load_degree(loads) -> float:
+    """(max - mean) / max of the loads, the mean an integer one as the
+    reference's Array::AveValue (src/Euler.cpp:394)."""
+    a = [int(v) for v in loads]
+    mx = max(a)
+    return 0.0 if mx <= 0 else (mx - sum(a) // len(a)) / mx
+
+
+def dlb_select_rows(rowload, amounts):
+    """The row picker of eu3d_dlb_select: (row bounds, moved load per transfer)."""
+    L = load_library()
+    r = np.ascontiguousarray(rowload, dtype=np.int64)
+    a = np.ascontiguousarray(amounts, dtype=np.int64)
+    bounds = np.zeros(len(a) + 1, dtype=np.int64)
+    moved = np.zeros(len(a), dtype=np.int64)
+    lp = C.POINTER(C.c_longlong)
+    _check(L.eu3d_dlb_select_rows(r.ctypes.data_as(lp), len(r), len(a), a.ctypes.data_as(lp),
+                                  bounds.ctypes.data_as(lp), moved.ctypes.data_as(lp)))
+    return bounds, moved

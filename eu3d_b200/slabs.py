@@ -22,6 +22,17 @@ With an immersed wedge the band is filled again after the first exchange (its
 mirror sources near a slab face are the neighbour's cells) and a second
 exchange hands the refilled solid cells to the neighbours.
 
+With `dlb` set and the adaptive trapezoid (react TRAPEZOID, type 1), the
+chemistry is load balanced across the slabs as the reference's
+DynamicLoadBalancer does it (src/LoadBalance.cpp:8-159, src/Euler.cpp:380-700):
+
+    predict -> all-gather the loads -> plan (same on every rank; skipped while
+    the load degree (max - mean) / max is at most dlb_tol) -> rows selected ->
+    all-reduce the cells per transfer -> packets to the receivers -> own cells
+    -> received cells -> results back to the senders -> unpacked
+
+The result equals the unbalanced step bit for bit.
+
 Layouts: "partition" gives every interior cell to one rank; "reference"
 reproduces the reference's mesh blocks (src/Mesh.cpp:77-93), where
 neighbouring slabs share their end node and the exchange skips it.
@@ -80,9 +91,16 @@ class StepSpec:
     bc_kind: int = gpu.BC_RSBI
     cfl: float = 0.0
     final_time: float = 1.0
+    dlb: bool = False       # balance the adaptive trapezoid across ranks
+    dlb_tol: float = 0.0    # ... when the load degree exceeds this
 
     def kw(self) -> dict:
-        return dataclasses.asdict(self)
+        d = dataclasses.asdict(self)
+        del d["dlb"], d["dlb_tol"]
+        return d
+
+    def balanced(self) -> bool:
+        return self.dlb and self.react == gpu.REACT_TRAPEZOID and self.type_ == 1
 
 
 class Slab:
@@ -113,6 +131,15 @@ class Slab:
     def recv_buffer(self, side): raise NotImplementedError
     def unpack(self, side): raise NotImplementedError
     def part(self, part, spec: StepSpec): raise NotImplementedError
+    # load balancing: chem_load() -> int; dlb_select(amounts) -> cells per
+    # transfer; dlb_pack(); dlb_guest(seg_cells); dlb_unpack(); and the packet
+    # segments out_seg(t) / in_seg(t) / guest_seg(t) / back_seg(t) of transfer t
+    def chem_load(self): raise NotImplementedError
+    def dlb_select(self, amounts): raise NotImplementedError
+    def dlb_alloc(self, n_out, n_in): raise NotImplementedError
+    def dlb_pack(self): raise NotImplementedError
+    def dlb_guest(self, seg_cells): raise NotImplementedError
+    def dlb_unpack(self): raise NotImplementedError
 
     def step(self, spec: StepSpec):
         """One step as a generator; it yields at the collective points."""
@@ -128,7 +155,44 @@ class Slab:
         if spec.timeadv == gpu.ADV_SSPRK3:
             yield from self._fill(spec.bc_kind)
             self.part(gpu.PART_STAGE3, spec)
-        self.part(gpu.PART_REACT, spec)
+        if spec.balanced():
+            yield from self._balanced_chemistry(spec)
+        else:
+            self.part(gpu.PART_REACT, spec)
+
+    def _balanced_chemistry(self, spec):
+        self.part(gpu.PART_CHEM_PREDICT, spec)
+        self.load = int(self.chem_load())
+        yield "loads"  # -> self.loads, every rank's load in rank order
+        plan = gpu.dlb_plan(self.loads) if gpu.load_degree(self.loads) > spec.dlb_tol else []
+        self.plan = plan
+        self.last_plan = plan
+        if not plan:
+            self.part(gpu.PART_CHEM_WORK, spec)
+            return
+        self.mine = [t for t, (s, _, _) in enumerate(plan) if s == self.rank]
+        self.theirs = [t for t, (_, r, _) in enumerate(plan) if r == self.rank]
+        cells = self.dlb_select([plan[t][2] for t in self.mine])
+        self.sent = {t: int(c) for t, c in zip(self.mine, cells)}
+        yield "dlb_counts"  # -> self.counts: cells of every transfer, in plan order
+        c = self.counts
+        self.dlb_alloc(sum(c[t] for t in self.mine), sum(c[t] for t in self.theirs))
+        self.dlb_pack()
+        yield "dlb_out"
+        self.part(gpu.PART_CHEM_WORK, spec)
+        self.dlb_guest([c[t] for t in self.theirs])
+        yield "dlb_back"
+        self.dlb_unpack()
+
+    def _offsets(self, ts, fields):
+        """{transfer: (start, end)} of the segments of transfers ts, concatenated
+        in that order, `fields` values per cell"""
+        out, o = {}, 0
+        for t in ts:
+            n = self.counts[t] * fields
+            out[t] = (o, o + n)
+            o += n
+        return out
 
     def _fill(self, kind):
         self.boundary(kind)
@@ -188,6 +252,50 @@ class DeviceSlab(Slab):
     def part(self, part, spec):
         self.d.step_part(part, **spec.kw())
 
+    # load balancing: packets are torch CUDA tensors of doubles
+    def chem_load(self):
+        return self.d.chem_load()
+
+    def dlb_select(self, amounts):
+        cells, _ = self.d.dlb_select(amounts)
+        return cells
+
+    def dlb_alloc(self, n_out, n_in):
+        dev, f64 = f"cuda:{self.d.device}", self.torch.float64
+        self._out = self.torch.empty(max(1, n_out * gpu.DLB_OUT_FIELDS), dtype=f64, device=dev)
+        self._back_in = self.torch.empty(max(1, n_out * gpu.DLB_BACK_FIELDS), dtype=f64, device=dev)
+        self._in = self.torch.empty(max(1, n_in * gpu.DLB_OUT_FIELDS), dtype=f64, device=dev)
+        self._guest = self.torch.empty(max(1, n_in * gpu.DLB_BACK_FIELDS), dtype=f64, device=dev)
+        self._o_out = self._offsets(self.mine, gpu.DLB_OUT_FIELDS)
+        self._o_back = self._offsets(self.mine, gpu.DLB_BACK_FIELDS)
+        self._o_in = self._offsets(self.theirs, gpu.DLB_OUT_FIELDS)
+        self._o_guest = self._offsets(self.theirs, gpu.DLB_BACK_FIELDS)
+
+    def dlb_pack(self):
+        self.d.dlb_pack(self._out.data_ptr())
+
+    def dlb_guest(self, seg_cells):
+        self.d.dlb_guest(seg_cells, self._in.data_ptr(), self._guest.data_ptr())
+
+    def dlb_unpack(self):
+        self.d.dlb_unpack(self._back_in.data_ptr())
+
+    def out_seg(self, t):
+        a, b = self._o_out[t]
+        return self._out[a:b]
+
+    def back_seg(self, t):
+        a, b = self._o_back[t]
+        return self._back_in[a:b]
+
+    def in_seg(self, t):
+        a, b = self._o_in[t]
+        return self._in[a:b]
+
+    def guest_seg(self, t):
+        a, b = self._o_guest[t]
+        return self._guest[a:b]
+
 
 class LoopbackTransport:
     """All ranks' slabs live in this process (tests, one GPU): buffers are
@@ -218,6 +326,39 @@ class LoopbackTransport:
         for s in slabs:
             for side in s.sides():
                 s.unpack(side)
+
+    def loads(self, slabs):
+        allv = [s.load for s in sorted(slabs, key=lambda s: s.rank)]
+        for s in slabs:
+            s.loads = allv
+
+    def dlb_counts(self, slabs):
+        plan = slabs[0].plan
+        counts = [0] * len(plan)
+        for s in slabs:
+            for t, c in s.sent.items():
+                counts[t] = c
+        for s in slabs:
+            s.counts = counts
+
+    def _by_rank(self, slabs):
+        return {s.rank: s for s in slabs}
+
+    def dlb_out(self, slabs):
+        self._sync(slabs)
+        by = self._by_rank(slabs)
+        for t, (snd, rcv, _) in enumerate(slabs[0].plan):
+            if by[rcv].counts[t]:
+                by[rcv].in_seg(t).copy_(by[snd].out_seg(t))
+        self._sync(slabs)
+
+    def dlb_back(self, slabs):
+        self._sync(slabs)
+        by = self._by_rank(slabs)
+        for t, (snd, rcv, _) in enumerate(slabs[0].plan):
+            if by[rcv].counts[t]:
+                by[snd].back_seg(t).copy_(by[rcv].guest_seg(t))
+        self._sync(slabs)
 
 
 class TorchTransport:
@@ -254,6 +395,52 @@ class TorchTransport:
                     req.wait()
             for side in s.sides():
                 s.unpack(side)
+
+    def _vec(self, s, values):
+        import torch
+        dev = f"cuda:{s.d.device}" if isinstance(s, DeviceSlab) else "cpu"
+        return torch.tensor(values, dtype=torch.int64, device=dev)
+
+    def loads(self, slabs):
+        (s,) = slabs
+        with self._ctx(s):
+            mine = self._vec(s, [s.load])
+            allv = [self._vec(s, [0]) for _ in range(self.dist.get_world_size(self.group))]
+            self.dist.all_gather(allv, mine, group=self.group)
+        s.loads = [int(v.item()) for v in allv]
+
+    def dlb_counts(self, slabs):
+        (s,) = slabs
+        counts = [0] * len(s.plan)
+        for t, c in s.sent.items():
+            counts[t] = c
+        with self._ctx(s):
+            v = self._vec(s, counts)
+            self.dist.all_reduce(v, op=self.dist.ReduceOp.SUM, group=self.group)
+        s.counts = [int(x) for x in v.tolist()]
+
+    def _p2p(self, s, sends, recvs):
+        dist = self.dist
+        with self._ctx(s):
+            ops = [dist.P2POp(dist.isend, buf, peer, group=self.group) for buf, peer in sends]
+            ops += [dist.P2POp(dist.irecv, buf, peer, group=self.group) for buf, peer in recvs]
+            if ops:
+                for req in dist.batch_isend_irecv(ops):
+                    req.wait()
+
+    def dlb_out(self, slabs):
+        (s,) = slabs
+        plan = s.plan
+        sends = [(s.out_seg(t), plan[t][1]) for t in s.mine if s.counts[t]]
+        recvs = [(s.in_seg(t), plan[t][0]) for t in s.theirs if s.counts[t]]
+        self._p2p(s, sends, recvs)
+
+    def dlb_back(self, slabs):
+        (s,) = slabs
+        plan = s.plan
+        sends = [(s.guest_seg(t), plan[t][0]) for t in s.theirs if s.counts[t]]
+        recvs = [(s.back_seg(t), plan[t][1]) for t in s.mine if s.counts[t]]
+        self._p2p(s, sends, recvs)
 
 
 class SlabRun:

@@ -208,7 +208,53 @@ int eu3d_wedge_fill(eu3d_handle *h);
 #define EU3D_PART_STAGE2 1 /* SSP-RK2/RK3 stage 2: advection, update, decode */
 #define EU3D_PART_REACT 2  /* chemistry */
 #define EU3D_PART_STAGE3 3 /* SSP-RK3 stage 3: advection, update, decode */
+/* the adaptive trapezoid (react TRAPEZOID, type 1, work queue on) in two halves, for load
+   balancing between them: PREDICT = Update_after_Adv + TrapezoidPrediction, counts binned;
+   WORK = the substeps of every cell not packed away (eu3d_dlb_pack) since PREDICT.
+   PREDICT then WORK equals REACT. */
+#define EU3D_PART_CHEM_PREDICT 4
+#define EU3D_PART_CHEM_WORK 5
 int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
+
+/* Dynamic load balancing of the adaptive trapezoid across ranks (replaces the reference's
+   DynamicLoadBalancer, include/LoadBalance.hpp:10-47, src/LoadBalance.cpp:8-159, and its use in
+   Euler::Trapezoid, src/Euler.cpp:380-700).  A rank's load is the sum of its cells' predicted
+   substep counts (React.Nchem.SumNoBoundary, src/Euler.cpp:392).  Per step, on every rank:
+     eu3d_step_part(CHEM_PREDICT); eu3d_chem_load -> all-gather the loads;
+     eu3d_dlb_plan (same result on every rank); the transfers whose sender is this rank:
+     eu3d_dlb_select -> cells per transfer (tell each receiver its count);
+     eu3d_dlb_pack into a device buffer of EU3D_DLB_OUT_FIELDS doubles per cell, one segment per
+     transfer in plan order; send each segment to its receiver;
+     eu3d_step_part(CHEM_WORK);
+     receivers: eu3d_dlb_guest on the received segments (in plan order) -> results, sent back;
+     senders: eu3d_dlb_unpack of the returned segments (same order and sizes, EU3D_DLB_BACK_FIELDS
+     doubles per cell).
+   The result equals the step without balancing bit for bit.  Packets are field-major per
+   segment: out CS[13], T, count; back CS[13], T, E, the 16 primitives, count (-1: a solid cell,
+   carried but not integrated).  All buffers are device memory; the calls run on the handle's
+   stream, eu3d_chem_load synchronises it. */
+#define EU3D_DLB_OUT_FIELDS 15
+#define EU3D_DLB_BACK_FIELDS 32
+#define EU3D_DLB_MAX_TRANSFERS 64 /* per rank and direction */
+/* DynamicLoadBalancer::DLBPriorityQueue (src/LoadBalance.cpp:8-59): transfers (sender,
+   receiver, amount) in the reference's order; *ntransfers is set even when cap is too small
+   (EU3D_ERR_ARG).  Host only. */
+int eu3d_dlb_plan(const long long *loads, int nranks, int cap, int *sender, int *receiver, long long *amount,
+                  int *ntransfers);
+/* the row picker of eu3d_dlb_select on host arrays: from row 0, each transfer takes
+   consecutive rows while their summed load stays within its amount; bounds: npacks + 1 row
+   boundaries, moved: the load each transfer takes.  Host only. */
+int eu3d_dlb_select_rows(const long long *rowload, long long nrows, int npacks, const long long *amount,
+                         long long *bounds, long long *moved);
+/* sum of the predicted substep counts of the handle's fluid cells (after CHEM_PREDICT) */
+int eu3d_chem_load(eu3d_handle *h, long long *load);
+/* picks the rows of this rank's transfers (amounts in plan order); cells and moved per transfer */
+int eu3d_dlb_select(eu3d_handle *h, int ntransfers, const long long *amount, long long *cells, long long *moved);
+int eu3d_dlb_pack(eu3d_handle *h, double *dev_out);
+/* integrates received cells: nseg segments of seg_cells[s] cells each, concatenated in dev_in;
+   writes the return segments, concatenated in the same order, to dev_back */
+int eu3d_dlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *dev_in, double *dev_back);
+int eu3d_dlb_unpack(eu3d_handle *h, const double *dev_back);
 
 /* Launch settings picked per handle (new): z planes walked by one flux block
    (default: 64, halved while the flux grid has fewer than four waves),

@@ -1,6 +1,6 @@
 // Function-level harness around the reference EU3D sources (test
 // infrastructure only).  It is compiled together with the reference's own
-// src/{Flowfield,Reaction,Mesh,TimeAdv,Function,FileReader,Global}.cpp, left
+// src/{Flowfield,Reaction,Mesh,TimeAdv,Function,FileReader,Global,LoadBalance}.cpp, left
 // unmodified, into oracle/_ref/libeu3d_ref.so.  The reference's driver class
 // `Euler` is a friend of Flowfield, Reaction and Mesh
 // (include/Flowfield.hpp:139, include/Reaction.hpp:140, include/Mesh.hpp:57);
@@ -20,7 +20,9 @@
 //    (src/Euler.cpp:375), a use-after-free on the next call.  The harness keeps
 //    the returned shallow copy alive, so each call computes what the
 //    reference computes when memory is not reused.
-//  * dynamic load balancing is a no-op on one rank and is not run.
+//  * dynamic load balancing is a no-op on one rank and is not run as part of a
+//    step; its planner (DynamicLoadBalancer::DLBPriorityQueue) is exported on
+//    its own (ref_dlb_plan) so the transfer plan can be compared.
 #include <cstring>
 #include <cstdint>
 #include <string>
@@ -31,6 +33,7 @@
 #include "Flowfield.hpp"
 #include "Reaction.hpp"
 #include "Global.hpp"
+#include "LoadBalance.hpp"
 
 namespace {
 struct RefCase {
@@ -307,5 +310,22 @@ int ref_read_mechanism(const char *mech, const char *thermo, int *ns_nr_tb, doub
 {
     return Euler::read_mechanism(mech, thermo, ns_nr_tb, stoi_f, stoi_b, react_tb, af, bf, eaf, c0, c1, mw, cap_ns,
                                  cap_nr);
+}
+// DynamicLoadBalancer::DLBPriorityQueue (src/LoadBalance.cpp:8-59) on per-rank
+// loads; out receives (sender, receiver, amount) triples, at most cap of them.
+// Returns the number of transfers.
+int ref_dlb_plan(const int *loads, int n, int *out, int cap)
+{
+    Array<int, 1> arr(n);
+    for (int i = 0; i < n; i++) arr(i) = loads[i];
+    DynamicLoadBalancer dlb;
+    dlb.DLBPriorityQueue(arr);
+    const int m = (int)dlb.transferNchem.size();
+    for (int t = 0; t < m && t < cap; t++) {
+        out[3 * t] = std::get<0>(dlb.transferNchem[t]);
+        out[3 * t + 1] = std::get<1>(dlb.transferNchem[t]);
+        out[3 * t + 2] = std::get<2>(dlb.transferNchem[t]);
+    }
+    return m;
 }
 }

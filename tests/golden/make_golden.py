@@ -16,7 +16,12 @@
    reference's Euler::Output file of rank 0), zlib-compressed, to pin the
    result-file writer's format.
 
+4. dlb_plans.npz -- transfer plans of the reference's load-balancing planner
+   (DynamicLoadBalancer::DLBPriorityQueue, compiled into oracle/_ref) for
+   seeded per-rank loads on 1 to 12 ranks and a few edge cases.
+
     python tests/golden/make_golden.py --text    (3. only)
+    python tests/golden/make_golden.py --dlb     (4. only)
 """
 from __future__ import annotations
 
@@ -107,8 +112,35 @@ def text_fixture():
     print("wrote", os.path.join(HERE, "rsbi_t0_text.npz"), len(raw), "bytes of text")
 
 
+def dlb_cases():
+    """Per-rank load vectors: seeded random ones (spread and skewed) and edge cases."""
+    rng = np.random.default_rng(2024)
+    cases = [[7], [0, 0], [5, 5, 5, 5], [100, 0, 0, 0], [0, 0, 0, 100], [1, 2], [3, 0, 1],
+             [100, 0, 0, 50, 1, 80, 3, 2], [2 ** 20, 3, 2 ** 19, 7, 11, 2 ** 18]]
+    for n in range(1, 13):
+        for _ in range(6):
+            cases.append([int(v) for v in rng.integers(0, 5000, n)])
+            cases.append([int(v) for v in (rng.pareto(1.2, n) * 300).astype(np.int64)])
+    return cases
+
+
+def dlb_fixture():
+    import ctypes as C
+    L = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libeu3d_ref.so"))
+    out = {}
+    for t, loads in enumerate(dlb_cases()):
+        a = (C.c_int * len(loads))(*loads)
+        buf = (C.c_int * (3 * 200))()
+        m = L.ref_dlb_plan(a, len(loads), buf, 200)
+        out[f"loads{t}"] = np.array(loads, dtype=np.int64)
+        out[f"plan{t}"] = np.array(buf[:3 * m], dtype=np.int64).reshape(m, 3)
+    np.savez_compressed(os.path.join(HERE, "dlb_plans.npz"), **out)
+    print("wrote", os.path.join(HERE, "dlb_plans.npz"), len(out) // 2, "plans")
+
+
 def main():
     text_fixture()
+    dlb_fixture()
     mech = load_h2_ja919()
     out = {}
     for c in CASES:
@@ -138,5 +170,7 @@ def main():
 if __name__ == "__main__":
     if "--text" in sys.argv:
         text_fixture()
+    elif "--dlb" in sys.argv:
+        dlb_fixture()
     else:
         main()

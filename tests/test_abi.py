@@ -59,9 +59,13 @@ def test_constants_match_quirk_header():
     assert num(vals["EU3D_DIFF_WENO"]) == gpu.DIFF_WENO
     text = open(os.path.join(ROOT, "include", "eu3d_gpu.h")).read()
     parts = dict(re.findall(r"#define (EU3D_PART_\w+) (\d+)", text))
-    assert {k: int(v) for k, v in parts.items()} == {"EU3D_PART_STAGE1": gpu.PART_STAGE1, "EU3D_PART_STAGE2":
-                                                     gpu.PART_STAGE2, "EU3D_PART_REACT": gpu.PART_REACT,
-                                                     "EU3D_PART_STAGE3": gpu.PART_STAGE3}
+    assert {k: int(v) for k, v in parts.items()} == {
+        "EU3D_PART_STAGE1": gpu.PART_STAGE1, "EU3D_PART_STAGE2": gpu.PART_STAGE2, "EU3D_PART_REACT": gpu.PART_REACT,
+        "EU3D_PART_STAGE3": gpu.PART_STAGE3, "EU3D_PART_CHEM_PREDICT": gpu.PART_CHEM_PREDICT,
+        "EU3D_PART_CHEM_WORK": gpu.PART_CHEM_WORK}
+    dlb = dict(re.findall(r"#define (EU3D_DLB_\w+) (\d+)", text))
+    assert (int(dlb["EU3D_DLB_OUT_FIELDS"]), int(dlb["EU3D_DLB_BACK_FIELDS"]), int(dlb["EU3D_DLB_MAX_TRANSFERS"])) == \
+        (gpu.DLB_OUT_FIELDS, gpu.DLB_BACK_FIELDS, gpu.DLB_MAX_TRANSFERS)
 
 
 def test_null_arguments_are_rejected_without_a_device(lib):

@@ -137,3 +137,68 @@ def test_halo_pack_unpack_roundtrip(mech):
         a.close()
     with pytest.raises(gpu.Eu3dError):
         gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED).halo_pack(2, buf.data_ptr())
+
+
+def _dlb_run(full, pieces, spec, steps, wedge=False):
+    slabs = [DeviceSlab(d, r, len(pieces), wedge=wedge) for r, (_, _, d) in enumerate(pieces)]
+    run = SlabRun(slabs, LoopbackTransport())
+    plans = []
+    for _ in range(steps):
+        full.step(**spec.kw())
+        run.step(spec)
+        plans.append(slabs[0].last_plan)
+    full.synchronize()
+    for _, _, d in pieces:
+        d.synchronize()
+    return slabs, plans
+
+
+@pytest.mark.parametrize("flux_bits", [64, 32])
+def test_dlb_trapezoid_slabs_equal_single_domain(mech, flux_bits):
+    """The adaptive trapezoid balanced across three slabs (the most loaded
+    slab hands rows to the others: packets out, substeps on the receivers,
+    results back) gives the unbalanced single domain bit for bit, counts
+    included; the substeps counted over the slabs equal the single domain's.
+    (The state stays finite under this trapezoid form for the two steps, as
+    the oracle shows; hotter ones do not.)"""
+    from _cases import fill_state
+    from pyoracle import Oracle
+    g = dyadic_grid(96, 20, 9)
+    o = Oracle(mech, g, gpu.QUIRKS_FIXED)
+    fill_state(o, 7, 1200.0, 1800.0, radicals=1e-5)
+    o.view("T")[:36] += 200.0  # more substeps in the first slab
+    o.prims_from_state()
+    full = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+    full.upload_state(o)
+    full.dt = 1e-8
+    pieces = _cut(full, mech, g, 3, "partition", flux_bits)
+    spec = StepSpec(react=gpu.REACT_TRAPEZOID, type_=1, bc_kind=gpu.BC_RSBI, cfl=0.0, final_time=1.0, dlb=True)
+    full.reset_status()
+    for _, _, d in pieces:
+        d.reset_status()
+    slabs, plans = _dlb_run(full, pieces, spec, 2)
+    _compare(full, pieces, names=("CS", "T", "P", "Yi", "Nchem", "E"))
+    # step 1 predicts one substep everywhere (balanced); step 2 balances
+    assert plans[0] == [] and plans[1] and plans[1][0][0] == 0, plans
+    assert sum(slabs[0].counts[t] for t in slabs[0].mine) > 0
+    assert sum(d.status()["substeps"] for _, _, d in pieces) == full.status()["substeps"]
+    assert all(d.status()["wait_timeouts"] == 0 for _, _, d in pieces)
+
+
+def test_dlb_odw_wedge_slabs_equal_single_domain(mech):
+    """Balancing with the immersed wedge: solid cells travel in the packets
+    unintegrated and are left untouched on return."""
+    case = odw_case(mech, 128, 48, 6, L=0.05)
+    full = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=32)
+    setup_odw(full, case)
+    full.dt = 4e-8
+    warm = StepSpec(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0, final_time=1.0)
+    for _ in range(30):
+        full.step(**warm.kw())
+    full.synchronize()
+    pieces = _cut(full, mech, case.grid, 3, "partition", 32, lambda d: setup_odw(d, case))
+    spec = StepSpec(react=gpu.REACT_TRAPEZOID, type_=1, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0,
+                    final_time=1.0, dlb=True)
+    _, plans = _dlb_run(full, pieces, spec, 2, wedge=True)
+    _compare(full, pieces, names=("CS", "T", "P", "Yi", "Nchem"))
+    assert any(plans), plans
