@@ -282,15 +282,17 @@ def roofline(prof, cells, hbm, tflops, src):
         return {"bound": "hbm", "kernel": k, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
                 "traffic_note": "ncu DRAM bytes of one launch on a 2.10 M-cell case, scaled by cells",
-                "per_cell": f"{work} B", "avg_ms": avg_ms,
-                "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; peak {src} "
-                        f"(MEASURED_PEAKS.json hbm_gbs)"}
+                "per_cell": f"{work} B", "avg_ms": avg_ms, "peak_source": src,
+                "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; frac of {src} peak "
+                        + ("(MEASURED_PEAKS.json hbm_gbs)" if src == "measured"
+                           else "(MEASURED_PEAKS.json absent: the pool's earlier copy measurement, 6650 GB/s)")}
     ach = work * cells / (avg_ms * 1e-3) / 1e12
     return {"bound": "tensor", "kernel": k, "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops,
             "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
-            "per_cell": f"{work} FLOP", "avg_ms": avg_ms,
-            "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; peak {src} "
-                    f"(MEASURED_PEAKS.json bf16_tflops)"}
+            "per_cell": f"{work} FLOP", "avg_ms": avg_ms, "peak_source": src,
+            "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; frac of {src} peak "
+                    + ("(MEASURED_PEAKS.json bf16_tflops)" if src == "measured"
+                       else "(MEASURED_PEAKS.json absent: the pool's earlier cuBLAS measurement, 1590 TFLOP/s)")}
 
 
 # DRAM bytes per cell of a launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
