@@ -371,11 +371,14 @@ def evaluate(sur: gpu.DeviceSurrogate, X, Lb, norm) -> dict:
 
 
 def select_model(mech, dev: gpu.DeviceFlowfield, recipe: Recipe, candidates: int, log=print,
-                 val_steps: int = 2000):
+                 val_steps: int = 2000, by: str = "accuracy", front_max: float = 0.5, peak_max: float = 0.005):
     """Train `candidates` networks (seeds recipe.seed, +1, ...) on one
     training set and keep the one whose coupled 2D ODW run (the benchmark's
     cells, `val_steps` steps) is closest to the FP64 adaptive run: smallest
-    median front offset, then peak-T error."""
+    median front offset, then peak-T error.  by="fallback": among the
+    candidates within front_max cells (median) and peak_max (peak-T error),
+    the one whose predictions fall back least; the accuracy order when none
+    qualifies."""
     from .validate import accuracy_2d
     sur = build_dataset(mech, dev, recipe, log)
     best, best_key = None, None
@@ -385,8 +388,13 @@ def select_model(mech, dev: gpu.DeviceFlowfield, recipe: Recipe, candidates: int
         acc = accuracy_2d(mech, model, val_steps)["surrogate"]
         key = (acc["front_abs_diff_cells_median"] if acc["front_abs_diff_cells_median"] is not None else 1e9,
                acc["peak_T_rel_err_vs_adaptive"])
+        if by == "fallback":
+            within = key[0] <= front_max and key[1] <= peak_max
+            key = (0 if within else 1, acc["fallback_frac"] if within else 0.0) + key
         model.meta["validation"] = acc
-        log(f"[surrogate] candidate {c}: front median {key[0]:.2f} cells, peak T error {key[1]:.4f}")
+        log(f"[surrogate] candidate {c} (seed {rec.seed}): front median "
+            f"{acc['front_abs_diff_cells_median']} cells, peak T error {acc['peak_T_rel_err_vs_adaptive']:.4f}, "
+            f"fallback {acc['fallback_frac']:.4f}")
         if best_key is None or key < best_key:
             best, best_key = model, key
     return best
@@ -403,13 +411,15 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=Recipe.batch)
     ap.add_argument("--seed", type=int, default=Recipe.seed)
     ap.add_argument("--candidates", type=int, default=1, help="networks to train; the best coupled run is kept")
+    ap.add_argument("--select", choices=["accuracy", "fallback"], default="accuracy",
+                    help="accuracy: closest coupled run; fallback: fewest fallbacks among accurate ones")
     a = ap.parse_args(argv)
     mech = load_h2_ja919()
     g = make_grid(8, 0.0, 1.0, 4, 0.0, 1.0, 2, 0.0, 1.0, 2, fixed_ghosts=True)
     dev = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=32)
     rec = Recipe(n_total=a.samples, steps=a.steps, batch=a.batch, seed=a.seed)
     if a.candidates > 1:
-        model = select_model(mech, dev, rec, a.candidates)
+        model = select_model(mech, dev, rec, a.candidates, by=a.select)
     else:
         model, _, _ = train_model(mech, dev, rec)
     model.save(a.out)
