@@ -145,3 +145,28 @@ def test_three_gloo_ranks_equal_unbalanced(tmp_path):
         assert np.array_equal(res[r]["vals"], want), r
     assert len(res[0]["plan"]) > 0
     assert all(np.array_equal(res[0]["plan"], x["plan"]) for x in res)
+
+
+def test_entry_points_reject_bad_arguments():
+    _library_or_skip()
+    L = gpu.load_library()
+    lp, ip = C.POINTER(C.c_longlong), C.POINTER(C.c_int)
+    loads = np.array([100, 0, 0, 0], dtype=np.int64)
+    m = C.c_int()
+    snd = np.zeros(1, dtype=np.int32)
+    rcv = np.zeros(1, dtype=np.int32)
+    amt = np.zeros(1, dtype=np.int64)
+    # three transfers do not fit a capacity of one; the count is still reported
+    rc = L.eu3d_dlb_plan(loads.ctypes.data_as(lp), 4, 1, snd.ctypes.data_as(ip), rcv.ctypes.data_as(ip),
+                         amt.ctypes.data_as(lp), C.byref(m))
+    assert rc == -1 and m.value == 3
+    assert L.eu3d_dlb_plan(None, 4, 1, None, None, None, C.byref(m)) == -1
+    assert L.eu3d_dlb_plan(loads.ctypes.data_as(lp), 0, 1, None, None, None, C.byref(m)) == -1
+    b = np.zeros(2, dtype=np.int64)
+    assert L.eu3d_dlb_select_rows(None, 3, 1, None, b.ctypes.data_as(lp), None) == -1
+    assert L.eu3d_dlb_select_rows(loads.ctypes.data_as(lp), 4, -1, None, b.ctypes.data_as(lp), None) == -1
+    for fn in ("eu3d_chem_load", "eu3d_dlb_pack", "eu3d_dlb_unpack"):
+        assert getattr(L, fn)(None, None) == -1, fn
+    assert L.eu3d_dlb_select(None, 0, None, None, None) == -1
+    assert L.eu3d_dlb_guest(None, 0, None, None, None) == -1
+    assert b"null" in L.eu3d_last_error() or b"bad" in L.eu3d_last_error()
