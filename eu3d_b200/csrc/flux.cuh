@@ -204,6 +204,27 @@ __device__ __forceinline__ void face_flux_src(const Src &src, bool zspec, float 
     out[NS + 3] = __fmul_rn(VI, __fmaf_rn(__fmul_rn(0.5f, Ds), q2, __fmul_rn(Ds, Hs)));
 }
 
+// TimeAdv::EE's residual of one conserved variable (src/TimeAdv.cpp:29-43:
+// RHS = -dt (dF/dx + dG/dy + dQ/dz)) from the face fluxes of the cell, with
+// ax = -dt/dx, by = dt/dy, cz = dt/dz.  FP64 fluxes: FP64 in the
+// reference's order.  FP32 fluxes: the three differences and the sum in
+// FP32, each operation rounded explicitly so that every FP32 kernel forms
+// the same bits, converted once for the FP64 store -- its rounding (2^-24
+// of the residual) is below the error the FP32 fluxes carry already.
+__device__ __forceinline__ double residual(double ax, double by, double cz, double xr, double xl, double yt, double yb,
+                                           double za, double zb)
+{
+    const double r = ax * (xr - xl);
+    return (r - by * (yt - yb)) - cz * (za - zb);
+}
+
+__device__ __forceinline__ double residual(float ax, float by, float cz, float xr, float xl, float yt, float yb,
+                                           float za, float zb)
+{
+    const float r = __fmaf_rn(-by, __fsub_rn(yt, yb), __fmul_rn(ax, __fsub_rn(xr, xl)));
+    return (double)__fmaf_rn(-cz, __fsub_rn(za, zb), r);
+}
+
 // Cells a-1 .. a+2 at element step st from qc (cell a-1 of field 0), fields
 // fs elements apart; global memory through the read-only path (LDG) or
 // shared memory.
@@ -340,8 +361,8 @@ __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
     P qb[NV], qa[NV];
-    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
-    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    const P ax = (P)(act ? -dt / (xn[i] - xn[i - 1]) : 0.0);
+    const P by = (P)(act ? dt / (yn[j] - yn[j - 1]) : 0.0);
     if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
     for (int k = kb, it = 0; k < ke; k++, it ^= 1) {
         // x faces of row r: face f sits between a = i0+f-1 and a+1 and is
@@ -364,13 +385,12 @@ __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
         if (act) face_flux_up<P, 3, DIFF>(q + L.at(i, j, k) - sz, fs, sz, zs_cell, qa);
         __syncthreads();
         if (act) {
-            const double cz = dt / (zn[k] - zn[k - 1]);
+            const P cz = (P)(dt / (zn[k] - zn[k - 1]));
             const long long c = L.at(i, j, k);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
-                double r = ax * ((double)fx[it][ty][tx + 1][v] - (double)fx[it][ty][tx][v]);
-                r = r - by * ((double)fy[it][ty + 1][tx][v] - (double)fy[it][ty][tx][v]);
-                rhs[v * L.fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
+                rhs[v * L.fs + c] = residual(ax, by, cz, fx[it][ty][tx + 1][v], fx[it][ty][tx][v], fy[it][ty + 1][tx][v],
+                                             fy[it][ty][tx][v], qa[v], qb[v]);
                 qb[v] = qa[v];
             }
         }
@@ -414,8 +434,8 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
     float qb[NV], qa[NV];
-    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
-    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    const float ax = (float)(act ? -dt / (xn[i] - xn[i - 1]) : 0.0);
+    const float by = (float)(act ? dt / (yn[j] - yn[j - 1]) : 0.0);
     if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
     for (int k = kb; k < ke; k++) {
         // stage cells x in [i0 - 2, i0 + 34), y in [j0 - 2, j0 + TY + 2) of plane k
@@ -446,13 +466,12 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
         if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, k) - sz, fs, sz, zs_cell, qa);
         __syncthreads();
         if (act) {
-            const double cz = dt / (zn[k] - zn[k - 1]);
+            const float cz = (float)(dt / (zn[k] - zn[k - 1]));
             const long long c = L.at(i, j, k);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
-                double r = ax * ((double)fx[ty][tx + 1][v] - (double)fx[ty][tx][v]);
-                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
-                rhs[v * L.fs + c] = r - cz * ((double)qa[v] - (double)qb[v]);
+                rhs[v * L.fs + c] = residual(ax, by, cz, fx[ty][tx + 1][v], fx[ty][tx][v], fy[ty + 1][tx][v],
+                                             fy[ty][tx][v], qa[v], qb[v]);
                 qb[v] = qa[v];
             }
         }
@@ -543,8 +562,8 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         for (int p = 0; p < issued; p++) issue(p);
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
-    const double ax = act ? -dt / (xn[i] - xn[i - 1]) : 0.0;
-    const double by = act ? dt / (yn[j] - yn[j - 1]) : 0.0;
+    const float ax = (float)(act ? -dt / (xn[i] - xn[i - 1]) : 0.0);
+    const float by = (float)(act ? dt / (yn[j] - yn[j - 1]) : 0.0);
     float qb[NV], qa[NV], fo[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) qb[v] = qa[v] = fo[v] = 0.f;
@@ -590,16 +609,14 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
             // that are never stored): only the stores are predicated
             // The right x face comes from the next lane; lane 31's (face 32
             // of the row) is sent by lane 0 from the face warp's slot.
-            const double cz = dt / (zn[k] - zn[k - 1]);
+            const float cz = (float)(dt / (zn[k] - zn[k - 1]));
             double *out = rhs + L.at(min(i, ilast), min(j, jlast), k);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 float send = fo[v];
                 if (tx == 0) send = fxe[ty][v];
                 const float fr = __shfl_sync(0xffffffffu, send, (tx + 1) & (FT_X - 1));
-                double r = ax * ((double)fr - (double)fo[v]);
-                r = r - by * ((double)fy[ty + 1][tx][v] - (double)fy[ty][tx][v]);
-                const double val = r - cz * ((double)qa[v] - (double)qb[v]);
+                const double val = residual(ax, by, cz, fr, fo[v], fy[ty + 1][tx][v], fy[ty][tx][v], qa[v], qb[v]);
                 if (act) out[v * L.fs] = val;
                 qb[v] = qa[v];
             }
