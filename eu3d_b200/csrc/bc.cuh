@@ -189,6 +189,27 @@ __global__ void k_wedge_band(GhostArgs a, P *q, const int4 *__restrict__ band, i
 // once.  A cell whose x time is NaN is skipped, as the reference's
 // comparisons skip it; NaN y or z times drop out of fmax as they drop out of
 // the reference's min.  One warp walks one (j, k) row of interior cells.
+// FP64 primitives: the reference's FP64 arithmetic (C = sqrt(gamma p / rho),
+// src/Flowfield.cpp:1281).  FP32 primitives: the same speeds in FP32 (the
+// inputs carry FP32 precision already), widened exactly for the maxima.
+__device__ __forceinline__ void cfl_speeds(double D, double Pp, double G, double U, double V, double W, double &ax,
+                                           double &ay, double &az)
+{
+    const double C = sqrt(G * Pp / D);
+    ax = fabs(U) + C;
+    ay = fabs(V) + C;
+    az = fabs(W) + C;
+}
+
+__device__ __forceinline__ void cfl_speeds(float D, float Pp, float G, float U, float V, float W, double &ax,
+                                           double &ay, double &az)
+{
+    const float C = sqrtf(__fdividef(__fmul_rn(G, Pp), D));
+    ax = (double)__fadd_rn(fabsf(U), C);
+    ay = (double)__fadd_rn(fabsf(V), C);
+    az = (double)__fadd_rn(fabsf(W), C);
+}
+
 template <class P>
 __global__ void k_cfl_partial(Layout L, const P *__restrict__ q, int use_z, const double *__restrict__ xn,
                               const double *__restrict__ yn, double x0, double y0, double tn, int wedge_on,
@@ -208,13 +229,13 @@ __global__ void k_cfl_partial(Layout L, const P *__restrict__ q, int use_z, cons
                 if (x > x0 && (y - y0) < (x - x0) * tn) continue;
             }
             const long long c = base + i;
-            const double D = (double)q[PD * fs + c], Pp = (double)q[PP * fs + c], G = (double)q[PG * fs + c];
-            const double C = sqrt(G * Pp / D);
-            const double ax = fabs((double)q[PU * fs + c]) + C;
+            double ax, ay, az;
+            cfl_speeds(q[PD * fs + c], q[PP * fs + c], q[PG * fs + c], q[PU * fs + c], q[PV * fs + c],
+                       q[PW * fs + c], ax, ay, az);
             if (isnan(ax)) continue;
             sx = fmax(sx, ax);
-            sy = fmax(sy, fabs((double)q[PV * fs + c]) + C);
-            if (use_z) sz = fmax(sz, fabs((double)q[PW * fs + c]) + C);
+            sy = fmax(sy, ay);
+            if (use_z) sz = fmax(sz, az);
         }
     }
     __shared__ double sm[3][32];
