@@ -76,9 +76,13 @@ __global__ void k_ghost_x(GhostArgs a, P *q)
     const int g = 2 * L.bc;
     const int n = g * L.nj * L.nk;
     if (t >= n) return;
-    const int gi = t % g, j = L.bc + (t / g) % L.nj, k = L.bc + t / (g * L.nj);
-    const bool lower = gi < L.bc;
-    const int i = lower ? gi : L.ni + L.bc + (gi - L.bc);
+    // a warp covers the bc ghost cells of consecutive rows j on one face:
+    // neighbouring lanes write neighbouring cells, the face is uniform across
+    // the warp, and the inflow planes (j fastest on the device) are read in order
+    const int gi = t % L.bc, j = L.bc + (t / L.bc) % L.nj;
+    const bool lower = (t / (L.bc * L.nj)) % 2 == 0;
+    const int k = L.bc + t / (g * L.nj);
+    const int i = lower ? gi : L.ni + L.bc + gi;
     const long long d = L.at(i, j, k);
     if (a.kind == EU3D_BC_RSBI) {
         const int si = lower ? 2 * L.bc - 1 - i : 2 * (L.ni + L.bc) - 1 - i;
@@ -88,7 +92,7 @@ __global__ void k_ghost_x(GhostArgs a, P *q)
         ghost_copy(a, q, d, L.at(si, j, k));
     } else if (a.kind == EU3D_BC_ODM) {
         if (lower) {
-            const long long p = (long long)(j - L.bc) * L.nk + (k - L.bc), pl = (long long)L.nj * L.nk;
+            const long long p = (long long)(k - L.bc) * L.nj + (j - L.bc), pl = (long long)L.nj * L.nk;
             const long long fs = L.fs;
             q[PU * fs + d] = (P)a.inflow[0 * pl + p];
             q[PV * fs + d] = (P)a.inflow[1 * pl + p];

@@ -1148,20 +1148,23 @@ int eu3d_set_inflow(eu3d_handle *h, const double *U, const double *V, const doub
         CK(cudaMalloc(&h->inflow, (9 + NS) * pl * sizeof(double)));
         CK(cudaMemsetAsync(h->inflow, 0, (9 + NS) * pl * sizeof(double), h->st));
     }
+    // host planes are (nj, nk) with k fastest (Yint (nj, nk, NS)); the device
+    // planes are field-major with j fastest, the order the x-face ghost fill
+    // reads them in
+    const int nj = h->L.nj, nk = h->L.nk;
+    std::vector<double> tmp((9 + NS) * pl);
     const double *src[9] = {U, V, W, Pp, D, T, H, E, G};
-    for (int f = 0; f < 9; f++)
-        if (src[f]) CK(cudaMemcpyAsync(h->inflow + f * pl, src[f], pl * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    if (Y) {
-        // host Yint is (nj, nk, NS); device planes are species-major
-        double *tmp = (double *)malloc(NS * pl * sizeof(double));
-        if (!tmp) return fail(EU3D_ERR_NOMEM, "host allocation failed");
-        for (size_t p = 0; p < pl; p++)
-            for (int s = 0; s < NS; s++) tmp[s * pl + p] = Y[p * NS + s];
-        cudaError_t e = cudaMemcpy(h->inflow + 9 * pl, tmp, NS * pl * sizeof(double), cudaMemcpyHostToDevice);
-        free(tmp);
-        if (e != cudaSuccess) return fail(EU3D_ERR_CUDA, cudaGetErrorString(e));
-    }
     CK(cudaStreamSynchronize(h->st));
+    for (int f = 0; f < 9 + NS; f++) {
+        if (f < 9 ? !src[f] : !Y) continue;
+        double *dst = tmp.data() + f * pl;
+        for (int j = 0; j < nj; j++)
+            for (int k = 0; k < nk; k++) {
+                const size_t p = (size_t)j * nk + k;
+                dst[(size_t)k * nj + j] = f < 9 ? src[f][p] : Y[p * NS + (f - 9)];
+            }
+        CK(cudaMemcpy(h->inflow + f * pl, dst, pl * sizeof(double), cudaMemcpyHostToDevice));
+    }
     return EU3D_OK;
 }
 
