@@ -508,30 +508,53 @@ int cfl_op(eu3d_handle *h, double cfl, double final_time, const Spacing &sp, int
 }
 
 // host reference layout <-> device SoA layout
+// Host arrays are the reference's (i, j, k[, field]) order -- field fastest,
+// then k -- and the device fields are x-fastest planes, so an upload or a
+// download is a transpose.  One block moves a tile of 32 cells in x by 8
+// planes in z of one row j, every field, through shared memory: the host
+// side is read (written) in runs of 8 n contiguous values per x cell, the
+// device side in 32-cell rows.
+constexpr int XFER_XT = 32, XFER_KT = 8;
+
 template <class D>
-__global__ void k_h2d(Layout L, const double *__restrict__ stage, int n, D *__restrict__ dst, long long dfs)
+__global__ void __launch_bounds__(256) k_h2d(Layout L, const double *__restrict__ stage, int n, D *__restrict__ dst,
+                                             long long dfs)
 {
-    const long long cells = (long long)L.NI * L.NJ * L.NK;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long hc = t / n;
-        const int s = (int)(t % n);
-        const int k = (int)(hc % L.NK), j = (int)((hc / L.NK) % L.NJ), i = (int)(hc / ((long long)L.NK * L.NJ));
-        dst[s * dfs + L.at(i, j, k)] = (D)stage[t];
+    __shared__ double tile[NV][XFER_KT][XFER_XT + 1];
+    const int i0 = blockIdx.x * XFER_XT, j = blockIdx.y, k0 = blockIdx.z * XFER_KT;
+    const int ni = min(XFER_XT, L.NI - i0), nk = min(XFER_KT, L.NK - k0), run = nk * n;
+    for (int e = threadIdx.x; e < ni * run; e += blockDim.x) {
+        const int il = e / run, r = e - il * run, kl = r / n, s = r - kl * n;
+        tile[s][kl][il] = stage[(((long long)(i0 + il) * L.NJ + j) * L.NK + k0) * n + r];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < XFER_XT * XFER_KT * n; e += blockDim.x) {
+        const int il = e % XFER_XT, r = e / XFER_XT, kl = r % XFER_KT, s = r / XFER_KT;
+        if (il < ni && kl < nk) dst[s * dfs + L.at(i0 + il, j, k0 + kl)] = (D)tile[s][kl][il];
     }
 }
 
 template <class S>
-__global__ void k_d2h(Layout L, const S *__restrict__ src, long long sfs, int n, double *__restrict__ stage)
+__global__ void __launch_bounds__(256) k_d2h(Layout L, const S *__restrict__ src, long long sfs, int n,
+                                             double *__restrict__ stage)
 {
-    const long long cells = (long long)L.NI * L.NJ * L.NK;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < cells * n;
-         t += (long long)gridDim.x * blockDim.x) {
-        const long long hc = t / n;
-        const int s = (int)(t % n);
-        const int k = (int)(hc % L.NK), j = (int)((hc / L.NK) % L.NJ), i = (int)(hc / ((long long)L.NK * L.NJ));
-        stage[t] = (double)src[s * sfs + L.at(i, j, k)];
+    __shared__ double tile[NV][XFER_KT][XFER_XT + 1];
+    const int i0 = blockIdx.x * XFER_XT, j = blockIdx.y, k0 = blockIdx.z * XFER_KT;
+    const int ni = min(XFER_XT, L.NI - i0), nk = min(XFER_KT, L.NK - k0), run = nk * n;
+    for (int e = threadIdx.x; e < XFER_XT * XFER_KT * n; e += blockDim.x) {
+        const int il = e % XFER_XT, r = e / XFER_XT, kl = r % XFER_KT, s = r / XFER_KT;
+        if (il < ni && kl < nk) tile[s][kl][il] = (double)src[s * sfs + L.at(i0 + il, j, k0 + kl)];
     }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ni * run; e += blockDim.x) {
+        const int il = e / run, r = e - il * run, kl = r / n, s = r - kl * n;
+        stage[(((long long)(i0 + il) * L.NJ + j) * L.NK + k0) * n + r] = tile[s][kl][il];
+    }
+}
+
+dim3 xfer_grid(const Layout &L)
+{
+    return dim3((L.NI + XFER_XT - 1) / XFER_XT, L.NJ, (L.NK + XFER_KT - 1) / XFER_KT);
 }
 
 // derived download fields: C = sqrt(G P / D); Mc = CS_s / Mw * 1000; Di = CS_s
@@ -1087,16 +1110,16 @@ int eu3d_upload_field(eu3d_handle *h, int field, const double *host)
     int rc = ensure_stage(h, bytes);
     if (rc) return rc;
     CK(cudaMemcpyAsync(h->stage, host, bytes, cudaMemcpyHostToDevice, h->st));
-    const int gb = grid_blocks(cells * n);
+    const dim3 xg = xfer_grid(L);
     const int pi = prim_index(field);
     if (pi >= 0) {
         if (h->flux_bits == 64)
-            k_h2d<double><<<gb, 256, 0, h->st>>>(L, h->stage, n, (double *)h->prim + pi * L.fs, L.fs);
+            k_h2d<double><<<xg, 256, 0, h->st>>>(L, h->stage, n, (double *)h->prim + pi * L.fs, L.fs);
         else
-            k_h2d<float><<<gb, 256, 0, h->st>>>(L, h->stage, n, (float *)h->prim + pi * L.fs, L.fs);
+            k_h2d<float><<<xg, 256, 0, h->st>>>(L, h->stage, n, (float *)h->prim + pi * L.fs, L.fs);
     } else {
         double *dst = field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
-        k_h2d<double><<<gb, 256, 0, h->st>>>(L, h->stage, n, dst, L.fs);
+        k_h2d<double><<<xg, 256, 0, h->st>>>(L, h->stage, n, dst, L.fs);
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->st));
@@ -1114,23 +1137,24 @@ int eu3d_download_field(eu3d_handle *h, int field, double *host)
     int rc = ensure_stage(h, bytes);
     if (rc) return rc;
     const int gb = grid_blocks(cells * n);
+    const dim3 xg = xfer_grid(L);
     const int pi = prim_index(field);
     if (pi >= 0) {
         if (h->flux_bits == 64)
-            k_d2h<double><<<gb, 256, 0, h->st>>>(L, (const double *)h->prim + pi * L.fs, L.fs, n, h->stage);
+            k_d2h<double><<<xg, 256, 0, h->st>>>(L, (const double *)h->prim + pi * L.fs, L.fs, n, h->stage);
         else
-            k_d2h<float><<<gb, 256, 0, h->st>>>(L, (const float *)h->prim + pi * L.fs, L.fs, n, h->stage);
+            k_d2h<float><<<xg, 256, 0, h->st>>>(L, (const float *)h->prim + pi * L.fs, L.fs, n, h->stage);
     } else if (field == EU3D_FIELD_C || field == EU3D_FIELD_MC || field == EU3D_FIELD_DI) {
         if (h->flux_bits == 64)
             k_derive<double><<<gb, 256, 0, h->st>>>(L, (const double *)h->prim, h->cs, field, h->stage, n);
         else
             k_derive<float><<<gb, 256, 0, h->st>>>(L, (const float *)h->prim, h->cs, field, h->stage, n);
     } else if (field == EU3D_FIELD_NCHEM) {
-        k_d2h<int><<<gb, 256, 0, h->st>>>(L, h->nchem, L.fs, 1, h->stage);
+        k_d2h<int><<<xg, 256, 0, h->st>>>(L, h->nchem, L.fs, 1, h->stage);
     } else {
         const double *src =
             field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
-        k_d2h<double><<<gb, 256, 0, h->st>>>(L, src, L.fs, n, h->stage);
+        k_d2h<double><<<xg, 256, 0, h->st>>>(L, src, L.fs, n, h->stage);
     }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(host, h->stage, bytes, cudaMemcpyDeviceToHost, h->st));
