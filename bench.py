@@ -206,24 +206,31 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-# algorithmic work per cell and launch of the kernels a roofline may be quoted for
-KERNEL_WORK = {
-    # flux + residual: 16 FP32 primitives in, 13 FP64 residuals out
-    "advection": ("hbm", 16 * 4 + 13 * 8),
-    # decode after the flux update: 13 FP64 state + RHS in, state + T, E + 16 FP32 primitives out
-    "cell_adv": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
-    # surrogate apply: state + T, E + 10 FP32 outputs in; 9 species + T, E + 16 primitives out
-    "sur_apply": ("hbm", 13 * 8 + 16 + 40 + 9 * 8 + 16 + 16 * 4),
-    # MLP 12 -> 3 x 128 -> 10 forward: 2 (16 128 + 2 128 128 + 128 16) FLOP
-    "sur_mlp": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
-    # the network and its apply in one kernel: the network's FLOPs
-    "sur_mlp_apply": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
-    "cell_imex": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
-    # stage 1: CS^n and RHS in, the stage state out (CS^n stays in place)
-    "cell_rk1": ("hbm", 13 * 8 * 3 + 2 * 8 * 2 + 16 * 4),
-    # stage 2: CS^n, the stage state and RHS in, CS out
-    "cell_rk2": ("hbm", 13 * 8 * 4 + 2 * 8 * 2 + 16 * 4),
-}
+def kernel_work(pb=4):
+    """Algorithmic work per cell and launch of the kernels a roofline may be
+    quoted for; pb = bytes of a primitive and of a residual value (4 with
+    the FP32 flux path, 8 with the FP64 one)."""
+    R = 13 * pb  # the flux residual of a cell
+    return {
+        # flux + residual: 16 primitives in, 13 residuals out
+        "advection": ("hbm", 16 * pb + R),
+        # decode after the flux update: 13 FP64 state + RHS in, state + T, E + 16 primitives out
+        "cell_adv": ("hbm", 13 * 8 * 2 + R + 2 * 8 * 2 + 16 * pb),
+        # surrogate apply: state + T, E + 10 FP32 outputs in; 9 species + T, E + 16 primitives out
+        "sur_apply": ("hbm", 13 * 8 + 16 + 40 + 9 * 8 + 16 + 16 * pb),
+        # MLP 12 -> 3 x 128 -> 10 forward: 2 (16 128 + 2 128 128 + 128 16) FLOP
+        "sur_mlp": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
+        # the network and its apply in one kernel: the network's FLOPs
+        "sur_mlp_apply": ("tensor", 2 * (16 * 128 + 2 * 128 * 128 + 128 * 16)),
+        "cell_imex": ("hbm", 13 * 8 * 2 + R + 2 * 8 * 2 + 16 * pb),
+        # stage 1: CS^n and RHS in, the stage state out (CS^n stays in place)
+        "cell_rk1": ("hbm", 13 * 8 * 2 + R + 2 * 8 * 2 + 16 * pb),
+        # stage 2: CS^n, the stage state and RHS in, CS out
+        "cell_rk2": ("hbm", 13 * 8 * 3 + R + 2 * 8 * 2 + 16 * pb),
+    }
+
+
+KERNEL_WORK = kernel_work(4)  # the default FP32 flux path
 
 
 def timed_steps(dev, step, K, W, torch, world, dist, clocks=False, local=0):
@@ -270,17 +277,18 @@ def profiled(dev, step, K):
     return prof
 
 
-def roofline(prof, cells, hbm, tflops, src):
+def roofline(prof, cells, hbm, tflops, src, pb=4):
     """Roofline of the kernel with the largest share of the step among those
-    with a stated algorithmic work."""
-    cand = [(k, v) for k, v in prof.items() if k in KERNEL_WORK]
+    with a stated algorithmic work (pb: bytes of a primitive / residual)."""
+    kw = kernel_work(pb)
+    cand = [(k, v) for k, v in prof.items() if k in kw]
     k, v = max(cand, key=lambda kv: kv[1][0])
     avg_ms = v[0] / v[1]
-    bound, work = KERNEL_WORK[k]
+    bound, work = kw[k]
     if bound == "hbm":
         ach = work * cells / (avg_ms * 1e-3) / 1e9
         return {"bound": "hbm", "kernel": k, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
+                "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL and pb == 4 else None,
                 "traffic_note": "ncu DRAM bytes of one launch on a 2.10 M-cell case, scaled by cells",
                 "per_cell": f"{work} B", "avg_ms": avg_ms, "peak_source": src,
                 "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; frac of {src} peak "
@@ -288,7 +296,7 @@ def roofline(prof, cells, hbm, tflops, src):
                            else "(MEASURED_PEAKS.json absent: the pool's earlier copy measurement, 6650 GB/s)")}
     ach = work * cells / (avg_ms * 1e-3) / 1e12
     return {"bound": "tensor", "kernel": k, "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops,
-            "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL else None,
+            "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL and pb == 4 else None,
             "per_cell": f"{work} FLOP", "avg_ms": avg_ms, "peak_source": src,
             "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; frac of {src} peak "
                     + ("(MEASURED_PEAKS.json bf16_tflops)" if src == "measured"
@@ -375,7 +383,7 @@ def run_ours(a, rank, world, local):
     prof = profs["surrogate"]
     prof_total = sum(v[0] for v in prof.values())
     launches = sum(v[1] for v in prof.values()) * a.steps // max(a.steps, 1)
-    rf = roofline(prof, cells, hbm, tfl, src)
+    rf = roofline(prof, cells, hbm, tfl, src, pb=4 if a.flux_bits == 32 else 8)
     ms = timing["surrogate"]
     value = cells * a.steps / (ms * 1e-3) / 1e6
     integ = {k: cells * a.steps / (timing[k] * 1e-3) / 1e6 for k in ("imex", "adaptive")}

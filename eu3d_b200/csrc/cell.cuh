@@ -527,7 +527,8 @@ __device__ __forceinline__ int nchem_bin(int n) { return 31 - __clz(max(n, 1)); 
 struct CellArgs {
     Layout L;
     unsigned quirks;
-    double *cs, *rhs, *T, *E, *cs0;
+    double *cs, *T, *E, *cs0;
+    const void *rhs;  // flux residual, in the primitives' precision (P)
     int *nchem;
     const double *scal;  // [0] = dt
     Status *st;
@@ -547,12 +548,19 @@ __device__ __forceinline__ bool solid_cell(const CellArgs &a, int i, int j)
     return x > a.wedge[0] && (y - a.wedge[1]) < (x - a.wedge[0]) * a.wedge[2];
 }
 
+// the flux residual of cell index i as FP64 (its storage has the primitives' precision)
+template <class P>
+__device__ __forceinline__ double rhs_at(const CellArgs &a, long long i)
+{
+    return (double)static_cast<const P *>(a.rhs)[i];
+}
+
 // Split adaptive step of one cell: the flux residual (CS += RHS, then a
 // decode; skipped with with_rhs = false when it was applied already), the
 // closed-reactor chemistry over dt at that state with the adaptive
 // integrator, applied as CS_s = rho (Y_s + dY_s) with negatives clipped, and
 // a decode (o).  Returns the substeps taken.
-template <bool SPEC>
+template <class P, bool SPEC>
 __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, double cs[NV], double T, double Eold,
                                                 bool with_rhs, Decoded &o, int &capped_any)
 {
@@ -562,7 +570,7 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
     int cp = 0;
     if (with_rhs) {
 #pragma unroll
-        for (int v = 0; v < NV; v++) cs[v] = cs[v] + a.rhs[v * fs + c];
+        for (int v = 0; v < NV; v++) cs[v] = cs[v] + rhs_at<P>(a, v * fs + c);
         decode(cs, T, Eold, qk, o, cp);
         capped_any |= cp;
     } else {
@@ -625,7 +633,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         // Flowfield::Update_IMEX, src/Flowfield.cpp:1219-1228
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            double r = a.rhs[v * fs + c];
+            double r = rhs_at<P>(a, v * fs + c);
             if (v < NS) {
                 r = r + CMS[v] * dt;
                 cs[v] = cs[v] + r / (1.0 - dt * MD[v]);
@@ -639,7 +647,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         // split step: the flux residual first (Update_after_Adv + decode),
         // then the chemistry of the closed reactor at that state over dt
         // (adaptive integrator, element-projected), then a decode
-        const int nsub = adapt_split_step<SPEC>(a, c, cs, T, Eold, !a.rhs_applied, o, capped_any);
+        const int nsub = adapt_split_step<P, SPEC>(a, c, cs, T, Eold, !a.rhs_applied, o, capped_any);
         warp_sum(&a.st->substeps, (unsigned long long)nsub);
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);
@@ -655,7 +663,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         constexpr double ws = MODE == M_RK_STAGE2 ? 0.5 : MODE == M_RK3_STAGE2 ? 0.25 : 2.0 / 3.0;
 #pragma unroll
         for (int v = 0; v < NV; v++) {
-            const double r = a.rhs[v * fs + c];
+            const double r = rhs_at<P>(a, v * fs + c);
             if (MODE == M_RK_STAGE1)
                 cs[v] = cs[v] + r;
             else
@@ -668,7 +676,7 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         const int nv = (qk & EU3D_Q_ADV_SPECIES_ONLY) ? NS : NV;
 #pragma unroll
         for (int v = 0; v < NV; v++)
-            if (v < nv) cs[v] = cs[v] + a.rhs[v * fs + c];
+            if (v < nv) cs[v] = cs[v] + rhs_at<P>(a, v * fs + c);
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;
         if (MODE == M_TRAP0 || MODE == M_NOCHEM) {

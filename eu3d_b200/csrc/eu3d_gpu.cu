@@ -64,7 +64,8 @@ struct eu3d_handle {
     Layout L{};
     int flux_bits = 64;
     unsigned quirks = 0;
-    double *cs = nullptr, *rhs = nullptr, *cs0 = nullptr, *T = nullptr, *E = nullptr;
+    double *cs = nullptr, *cs0 = nullptr, *T = nullptr, *E = nullptr;
+    void *rhs = nullptr;  // flux residual, NV fields in the primitives' precision
     void *prim = nullptr;
     int *nchem = nullptr;
     double *xn = nullptr, *yn = nullptr, *zn = nullptr;
@@ -373,19 +374,20 @@ void launch_adv_t(eu3d_handle *h)
         if (h->flux_stage == 2 && h->tq_ok) {
             dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
             dim3 bs(FT_X, FR_TY + 2);
-            k_flux_ring<DIFF><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, h->rhs,
+            k_flux_ring<DIFF><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs,
                                                                  sq, kz, h->status);
             return;
         }
         if (h->flux_stage) {
             dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
             dim3 bs(FT_X, FS_TY + 2);
-            k_flux_stage<DIFF><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal, h->rhs, sq,
+            k_flux_stage<DIFF><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs, sq,
                                                                    kz);
             return;
         }
     }
-    k_flux_tile<P, DIFF><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal, h->rhs, sq, kz);
+    k_flux_tile<P, DIFF><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal, (P *)h->rhs, sq,
+                                                kz);
 }
 
 template <class P>
@@ -770,7 +772,7 @@ int stage_op(eu3d_handle *h, const eu3d_step_desc *s, int stage)
     const int mode = s->timeadv == EU3D_ADV_SSPRK2 ? M_RK_STAGE2 : stage == 2 ? M_RK3_STAGE2 : M_RK3_STAGE3;
     if ((rc = cell_op(h, mode))) return rc;
     if (stage == rk_stages(s->timeadv))
-        CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * sizeof(double), h->st));
+        CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * prim_bytes(h), h->st));
     return EU3D_OK;
 }
 
@@ -966,7 +968,7 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
         return fail(EU3D_ERR_CUDA, "stream creation failed");
     }
     ALLOC(h->cs, NV * f8);
-    ALLOC(h->rhs, NV * f8);
+    ALLOC(h->rhs, (size_t)NV * L.fs * prim_bytes(h));
     ALLOC(h->T, f8);
     ALLOC(h->E, f8);
     ALLOC(h->prim, (size_t)NPRIM * L.fs * prim_bytes(h));
@@ -983,7 +985,7 @@ int eu3d_create(const eu3d_desc *d, eu3d_handle **out)
     ALLOC(h->status, sizeof(Status));
 #undef ALLOC
     cudaMemsetAsync(h->cs, 0, NV * f8, h->st);
-    cudaMemsetAsync(h->rhs, 0, NV * f8, h->st);
+    cudaMemsetAsync(h->rhs, 0, (size_t)NV * L.fs * prim_bytes(h), h->st);
     cudaMemsetAsync(h->T, 0, f8, h->st);
     cudaMemsetAsync(h->E, 0, f8, h->st);
     cudaMemsetAsync(h->prim, 0, (size_t)NPRIM * L.fs * prim_bytes(h), h->st);
@@ -1117,8 +1119,13 @@ int eu3d_upload_field(eu3d_handle *h, int field, const double *host)
             k_h2d<double><<<xg, 256, 0, h->st>>>(L, h->stage, n, (double *)h->prim + pi * L.fs, L.fs);
         else
             k_h2d<float><<<xg, 256, 0, h->st>>>(L, h->stage, n, (float *)h->prim + pi * L.fs, L.fs);
+    } else if (field == EU3D_FIELD_RHS) {
+        if (h->flux_bits == 64)
+            k_h2d<double><<<xg, 256, 0, h->st>>>(L, h->stage, n, (double *)h->rhs, L.fs);
+        else
+            k_h2d<float><<<xg, 256, 0, h->st>>>(L, h->stage, n, (float *)h->rhs, L.fs);
     } else {
-        double *dst = field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
+        double *dst = field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : h->cs;
         k_h2d<double><<<xg, 256, 0, h->st>>>(L, h->stage, n, dst, L.fs);
     }
     CK(cudaGetLastError());
@@ -1151,9 +1158,13 @@ int eu3d_download_field(eu3d_handle *h, int field, double *host)
             k_derive<float><<<gb, 256, 0, h->st>>>(L, (const float *)h->prim, h->cs, field, h->stage, n);
     } else if (field == EU3D_FIELD_NCHEM) {
         k_d2h<int><<<xg, 256, 0, h->st>>>(L, h->nchem, L.fs, 1, h->stage);
+    } else if (field == EU3D_FIELD_RHS) {
+        if (h->flux_bits == 64)
+            k_d2h<double><<<xg, 256, 0, h->st>>>(L, (const double *)h->rhs, L.fs, n, h->stage);
+        else
+            k_d2h<float><<<xg, 256, 0, h->st>>>(L, (const float *)h->rhs, L.fs, n, h->stage);
     } else {
-        const double *src =
-            field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : field == EU3D_FIELD_CS ? h->cs : h->rhs;
+        const double *src = field == EU3D_FIELD_T ? h->T : field == EU3D_FIELD_E ? h->E : h->cs;
         k_d2h<double><<<xg, 256, 0, h->st>>>(L, src, L.fs, n, h->stage);
     }
     CK(cudaGetLastError());

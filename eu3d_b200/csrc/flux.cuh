@@ -209,8 +209,8 @@ __device__ __forceinline__ void face_flux_src(const Src &src, bool zspec, float 
 // ax = -dt/dx, by = dt/dy, cz = dt/dz.  FP64 fluxes: FP64 in the
 // reference's order.  FP32 fluxes: the three differences and the sum in
 // FP32, each operation rounded explicitly so that every FP32 kernel forms
-// the same bits, converted once for the FP64 store -- its rounding (2^-24
-// of the residual) is below the error the FP32 fluxes carry already.
+// the same bits, stored in FP32 -- its rounding (2^-24 of the residual) is
+// below the error the FP32 fluxes carry already.
 __device__ __forceinline__ double residual(double ax, double by, double cz, double xr, double xl, double yt, double yb,
                                            double za, double zb)
 {
@@ -218,11 +218,11 @@ __device__ __forceinline__ double residual(double ax, double by, double cz, doub
     return (r - by * (yt - yb)) - cz * (za - zb);
 }
 
-__device__ __forceinline__ double residual(float ax, float by, float cz, float xr, float xl, float yt, float yb,
-                                           float za, float zb)
+__device__ __forceinline__ float residual(float ax, float by, float cz, float xr, float xl, float yt, float yb,
+                                          float za, float zb)
 {
     const float r = __fmaf_rn(-by, __fsub_rn(yt, yb), __fmul_rn(ax, __fsub_rn(xr, xl)));
-    return (double)__fmaf_rn(-cz, __fsub_rn(za, zb), r);
+    return __fmaf_rn(-cz, __fsub_rn(za, zb), r);
 }
 
 // Cells a-1 .. a+2 at element step st from qc (cell a-1 of field 0), fields
@@ -342,7 +342,7 @@ constexpr int flux_threads()
 template <class P, int DIFF>
 __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
     Layout L, const P *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
-    const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
+    const double *__restrict__ zn, const double *__restrict__ dtp, P *__restrict__ rhs, int species_quirk, int kz)
 {
     constexpr int TY = FluxTile<P>::TY;
     // two buffers: plane k+1 may fill one while slow threads still read plane k
@@ -414,7 +414,7 @@ struct FluxStage {
 template <int DIFF>
 __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
     Layout L, const float *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
-    const double *__restrict__ zn, const double *__restrict__ dtp, double *__restrict__ rhs, int species_quirk, int kz)
+    const double *__restrict__ zn, const double *__restrict__ dtp, float *__restrict__ rhs, int species_quirk, int kz)
 {
     constexpr int TY = FS_TY, HX = FS_HX, HY = FS_HY, PL = HX * HY;
     extern __shared__ __align__(16) unsigned char flux_smem[];
@@ -525,7 +525,7 @@ template <int DIFF>
 __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     const __grid_constant__ CUtensorMap tq, Layout L, const float *__restrict__ q, const double *__restrict__ xn,
     const double *__restrict__ yn, const double *__restrict__ zn, const double *__restrict__ dtp,
-    double *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat)
+    float *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat)
 {
     constexpr int TY = FR_TY, HX = FR_HX, PL = FR_PL;
     extern __shared__ unsigned char fr_raw[];
@@ -610,13 +610,13 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
             // The right x face comes from the next lane; lane 31's (face 32
             // of the row) is sent by lane 0 from the face warp's slot.
             const float cz = (float)(dt / (zn[k] - zn[k - 1]));
-            double *out = rhs + L.at(min(i, ilast), min(j, jlast), k);
+            float *out = rhs + L.at(min(i, ilast), min(j, jlast), k);
 #pragma unroll
             for (int v = 0; v < NV; v++) {
                 float send = fo[v];
                 if (tx == 0) send = fxe[ty][v];
                 const float fr = __shfl_sync(0xffffffffu, send, (tx + 1) & (FT_X - 1));
-                const double val = residual(ax, by, cz, fr, fo[v], fy[ty + 1][tx][v], fy[ty][tx][v], qa[v], qb[v]);
+                const float val = residual(ax, by, cz, fr, fo[v], fy[ty + 1][tx][v], fy[ty][tx][v], qa[v], qb[v]);
                 if (act) out[v * L.fs] = val;
                 qb[v] = qa[v];
             }
