@@ -304,10 +304,11 @@ def roofline(prof, cells, hbm, tflops, src, pb=4):
 
 
 # DRAM bytes per cell of a launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch on the 256 x 128 x 64 ODW, 2.10 M cells: the full 33.5 M-cell
-# case is too large to capture under the profiling rule), scaled to a launch
-# by cells; the flux kernel's traffic grows with cells (one pass, no re-reads)
-TRAFFIC_PER_CELL = {"advection": (192.838656e6 + 180.969216e6) / 2097152}
+# of one launch on the 256 x 128 x 64 ODW, 2.10 M cells, with the benchmark's 64
+# z planes per block: the full 33.5 M-cell case is too large to capture under
+# the profiling rule), scaled to a launch by cells; the flux kernel's traffic
+# grows with cells (one pass; the tile halos add 3 % of reads)
+TRAFFIC_PER_CELL = {"advection": (168.854016e6 + 81.255936e6) / 2097152}
 
 
 def developed_state(mech, ni, nj, nk, steps2d, seed):
