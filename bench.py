@@ -394,8 +394,7 @@ def run_ours(a, rank, world, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": W,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "bf16 (network) + f64 (state, decode, fallback integrator)", "data": "synthetic",
-        "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge, "
-                               f"1 % seeded inflow density perturbation)",
+        "config": {"workload": workload_name(ni, nj, nk),
                    "cells": cells, "cells_per_gpu": n_loc * nj * nk, "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback",
                    "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state",
                    "time": f"SSP-RK2, CFL {CFL}",
@@ -473,6 +472,11 @@ def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
                         "read, download CS,T"}
 
 
+def workload_name(ni, nj, nk):
+    return (f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge, "
+            f"1 % seeded inflow density perturbation)")
+
+
 def run_reference(a, rank, world):
     if rank != 0:
         return None
@@ -488,7 +492,10 @@ def run_reference(a, rank, world):
     return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"3D oblique detonation {ni}x{nj}x{nk} (ODW), bounded host samples"},
+            "config": {"workload": workload_name(ni, nj, nk), "cells": ni * nj * nk,
+                       "chemistry": "the reference's own FP64 IMEX (Euler::IMEX), no learned chemistry",
+                       "flux": "the reference's MUSCL_2/minmod + AUSM, FP64", "time": "TimeAdv::EE",
+                       "measured_on": "bounded host samples of the workload (cpu_baseline.sample), per cell-step"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
