@@ -64,7 +64,10 @@ typedef struct eu3d_handle eu3d_handle;
 typedef struct eu3d_surrogate eu3d_surrogate;
 
 /* Field identifiers for upload/download.  Shapes (reference layout):
-   3D fields NI*NJ*NK; EU3D_FIELD_YI/MC/DI NI*NJ*NK*NS; CS/RHS NI*NJ*NK*(NS+4). */
+   3D fields NI*NJ*NK; EU3D_FIELD_YI/MC/DI NI*NJ*NK*NS; CS/RHS NI*NJ*NK*(NS+4).
+   Host arrays are always double.  On the device the primitives (U V W P D H
+   Gamma Yi) and the flux residual RHS have the flux precision (flux_bits: FP32
+   or FP64); CS, T and E are FP64. */
 enum {
     EU3D_FIELD_U = 0, EU3D_FIELD_V, EU3D_FIELD_W, EU3D_FIELD_P, EU3D_FIELD_D, EU3D_FIELD_T,
     EU3D_FIELD_H, EU3D_FIELD_GAMMA, EU3D_FIELD_E,
