@@ -596,6 +596,15 @@ class DeviceSurrogate:
         _check(self.L.eu3d_sur_infer(self.s, x_ptr, n, out_ptr, stream or None))
 
 
+def tecplot_path(numprocs: int, react: str, num: int, rank: int) -> str:
+    """The reference's result-file name (Euler::Output, src/Euler.cpp:802-805):
+    output_<numprocs>/results/Series<react><num>_<rank>.dat on one rank,
+    output_<numprocs>/results<react><num>_<rank>.dat on several."""
+    if numprocs == 1:
+        return f"./output_{numprocs}/results/Series{react}{num}_{rank}.dat"
+    return f"./output_{numprocs}/results{react}{num}_{rank}.dat"
+
+
 def write_tecplot_host(path: str, grid, cols, lcol, wait_time: float = 0.0):
     """The Tecplot block file from host arrays: cols (13, n) T D P U V Ma Y1..Y7 and
     lcol (n,) counts, both in the file's cell order (k outer, i inner)."""

@@ -92,6 +92,12 @@ def test_host_writer_format(tmp_path):
     assert b["Z"] == ["%.6g" % g.znode[g.bc + k] for k in [0] * 6 + [1] * 6]
 
 
+def test_result_file_names():
+    # the published t = 0 files of the 8-rank RSBI run are output_8/resultsIMEX0_<rank>.dat
+    assert gpu.tecplot_path(8, "IMEX", 0, 5) == "./output_8/resultsIMEX0_5.dat"
+    assert gpu.tecplot_path(1, "Trapezoid", 12, 0) == "./output_1/results/SeriesTrapezoid12_0.dat"
+
+
 def test_host_writer_errors(tmp_path):
     _library_or_skip()
     g = small_grid(3, 2, 2)
