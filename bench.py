@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
+    ap.add_argument("--accuracy-full", action="store_true",
+                    help="also compare on the benchmark's full grid (about 2.5 more minutes)")
     ap.add_argument("--develop", type=int, default=1500, help="2D steps that develop the timed state")
     ap.add_argument("--model", default=os.path.join(ROOT, "eu3d_b200", "data", "sur_h2_ja919.npz"))
     return ap.parse_args()
@@ -425,6 +427,8 @@ def run_ours(a, rank, world, local):
         from eu3d_b200.validate import accuracy_2d, accuracy_3d
         out["accuracy"] = accuracy_2d(mech, model, a.accuracy_steps, cfl=CFL)
         out["accuracy_3d"] = accuracy_3d(mech, model, a.accuracy_steps, nk=16, cfl=CFL)
+        if a.accuracy_full:
+            out["accuracy_full_grid"] = accuracy_3d(mech, model, a.accuracy_steps, ni, nj, nk, cfl=CFL)
     if not a.no_e2e:
         reset()
         out["e2e"] = run_e2e(dev, stepper(dict(base, react=gpu.REACT_SURROGATE)), a.steps, cells, torch, world, dist)
