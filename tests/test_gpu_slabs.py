@@ -202,3 +202,28 @@ def test_dlb_odw_wedge_slabs_equal_single_domain(mech):
     _, plans = _dlb_run(full, pieces, spec, 2, wedge=True)
     _compare(full, pieces, names=("CS", "T", "P", "Yi", "Nchem"))
     assert any(plans), plans
+
+
+@pytest.mark.parametrize("flux_bits", [64, 32])
+def test_weno_rk3_slabs_equal_single_domain(mech, flux_bits):
+    """WENO + SSP-RK3 on three device slabs equal the single domain bit for bit."""
+    from _cases import fill_state
+    from pyoracle import Oracle
+    g = dyadic_grid(96, 20, 9)
+    o = Oracle(mech, g, gpu.QUIRKS_FIXED)
+    fill_state(o, 7, 1100.0, 2600.0)
+    full = gpu.DeviceFlowfield(mech, g, gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+    full.upload_state(o)
+    full.dt = 1e-8
+    pieces = _cut(full, mech, g, 3, "partition", flux_bits)
+    spec = StepSpec(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK3, diff=gpu.DIFF_WENO, bc_kind=gpu.BC_RSBI, cfl=0.5,
+                    final_time=1.0)
+    slabs = [DeviceSlab(d, r, 3) for r, (_, _, d) in enumerate(pieces)]
+    run = SlabRun(slabs, LoopbackTransport())
+    for _ in range(3):
+        full.step(**spec.kw())
+        run.step(spec)
+    full.synchronize()
+    for _, _, d in pieces:
+        d.synchronize()
+    _compare(full, pieces)

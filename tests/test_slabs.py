@@ -83,3 +83,16 @@ def test_two_gloo_ranks_equal_single_domain(mech, tmp_path, layout, timeadv):
             ref = full.view(f)[b:full.ni + b, b:full.nj + b, b:full.nk + b][i0:i0 + n]
             assert np.array_equal(d[f], ref), f
         assert float(d["time"]) == full.time and float(d["dt"]) == full.dt
+
+
+def test_loopback_slabs_weno_rk3_equal_single_domain(mech):
+    """The WENO reconstruction reads the same two cells on each side as
+    MUSCL_2, so the two-plane halo suffices: slabs equal the single domain."""
+    full = full_oracle(mech, (24, 6, 4))
+    pieces = cut(mech, full, 3, "partition")
+    slabs = [OracleSlab(o, r, 3, overlap=0) for r, (_, _, o) in enumerate(pieces)]
+    spec = StepSpec(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK3, diff=gpu.DIFF_WENO, bc_kind=gpu.BC_RSBI, cfl=0.5,
+                    final_time=1.0)
+    SlabRun(slabs, LoopbackTransport()).run(3, spec)
+    _full_run(full, spec, 3)
+    assert_slabs_equal_full(full, pieces)
