@@ -170,3 +170,25 @@ def test_entry_points_reject_bad_arguments():
     assert L.eu3d_dlb_select(None, 0, None, None, None) == -1
     assert L.eu3d_dlb_guest(None, 0, None, None, None) == -1
     assert b"null" in L.eu3d_last_error() or b"bad" in L.eu3d_last_error()
+
+
+@pytest.mark.parametrize("nranks,seed", [(2, 1), (3, 2), (4, 3), (5, 4), (5, 5)])
+def test_loopback_host_slabs_random_hot_spots(nranks, seed):
+    """Random hot rows on random ranks: every plan the planner makes moves
+    whole rows out and back without changing any cell's result."""
+    _library_or_skip()
+    rng = np.random.default_rng(seed)
+    data = []
+    for r in range(nranks):
+        vals = rng.uniform(0.0, 0.75, (10, 6))
+        hot = rng.random(10) < rng.uniform(0.0, 0.6)
+        vals[hot] = rng.uniform(0.8, 1.0, (int(hot.sum()), 6))
+        solid = rng.random((10, 6)) < 0.05
+        data.append((vals, solid))
+    slabs = [HostSlab(v, s, r, nranks) for r, (v, s) in enumerate(data)]
+    spec = StepSpec(react=gpu.REACT_TRAPEZOID, type_=1, dlb=True)
+    SlabRun(slabs, LoopbackTransport()).run(2, spec)
+    for got, want in zip([s.vals for s in slabs], _expected(data, 2)):
+        assert np.array_equal(got, want)
+    plan = slabs[0].last_plan
+    assert plan == oracle_plan(slabs[0].loads)
