@@ -279,30 +279,34 @@ def profiled(dev, step, K):
     return prof
 
 
-def roofline(prof, cells, hbm, tflops, src, pb=4):
-    """Roofline of the kernel with the largest share of the step among those
-    with a stated algorithmic work (pb: bytes of a primitive / residual)."""
+def roofline(prof, units, hbm, tflops, src, pb=4, kernel=None):
+    """Roofline of one kernel -- by default the one with the largest share of
+    the step among those with a stated algorithmic work (pb: bytes of a
+    primitive / residual).  units: kernel -> cells whose work a launch must do
+    (the fluid cells for the flux and cell kernels, which leave the wedge's
+    solid cells out; the listed cells for the network)."""
     kw = kernel_work(pb)
     cand = [(k, v) for k, v in prof.items() if k in kw]
-    k, v = max(cand, key=lambda kv: kv[1][0])
+    k, v = (kernel, prof[kernel]) if kernel else max(cand, key=lambda kv: kv[1][0])
     avg_ms = v[0] / v[1]
     bound, work = kw[k]
+    cells = units[k]
     if bound == "hbm":
         ach = work * cells / (avg_ms * 1e-3) / 1e9
         return {"bound": "hbm", "kernel": k, "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL and pb == 4 else None,
-                "traffic_note": "ncu DRAM bytes of one launch on a 2.10 M-cell case, scaled by cells",
-                "per_cell": f"{work} B", "avg_ms": avg_ms, "peak_source": src,
-                "note": f"achieved = {work} B/cell x {cells} cells / average launch of {k}; frac of {src} peak "
+                "traffic_note": TRAFFIC_NOTE.get(k),
+                "per_cell": f"{work} B", "cells": cells, "avg_ms": avg_ms, "peak_source": src,
+                "note": f"achieved = {work} B/cell x {cells} fluid cells / average launch of {k}; frac of {src} peak "
                         + ("(MEASURED_PEAKS.json hbm_gbs)" if src == "measured"
                            else "(MEASURED_PEAKS.json absent: the pool's earlier copy measurement, 6650 GB/s)")}
     ach = work * cells / (avg_ms * 1e-3) / 1e12
     return {"bound": "tensor", "kernel": k, "achieved": ach, "peak": tflops, "unit": "TFLOP/s", "frac": ach / tflops,
             "traffic": TRAFFIC_PER_CELL[k] * cells if k in TRAFFIC_PER_CELL and pb == 4 else None,
-            "per_cell": f"{work} FLOP", "avg_ms": avg_ms, "peak_source": src,
-            "note": f"achieved = {work} FLOP/cell x {cells} cells / average launch of {k}; frac of {src} peak "
-                    + ("(MEASURED_PEAKS.json bf16_tflops)" if src == "measured"
-                       else "(MEASURED_PEAKS.json absent: the pool's earlier cuBLAS measurement, 1590 TFLOP/s)")}
+            "per_cell": f"{work} FLOP", "cells": cells, "avg_ms": avg_ms, "peak_source": src,
+            "note": f"achieved = {work} FLOP/cell x {cells} network cells / average launch of {k}; frac of {src} "
+                    "peak " + ("(MEASURED_PEAKS.json bf16_tflops)" if src == "measured"
+                               else "(MEASURED_PEAKS.json absent: the pool's earlier cuBLAS measurement, 1590 TFLOP/s)")}
 
 
 # DRAM bytes per cell of a launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
@@ -311,6 +315,22 @@ def roofline(prof, cells, hbm, tflops, src, pb=4):
 # the profiling rule), scaled to a launch by cells; the flux kernel's traffic
 # grows with cells (one pass; the tile halos add 3 % of reads)
 TRAFFIC_PER_CELL = {"advection": (168.854016e6 + 81.255936e6) / 2097152}
+TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on a 2.10 M-cell case, per cell, times the fluid cells"}
+
+
+def fluid_cells(case, i0=0, n_loc=None):
+    """Interior cells of the case (or of the x slab i0 .. i0 + n_loc) outside its wedge."""
+    g = case.grid
+    x = g.xnode[g.bc:-g.bc][i0:i0 + (n_loc or g.ni)][:, None]
+    y = g.ynode[g.bc:-g.bc][None, :]
+    w = case.wedge
+    solid = (x > w[0]) & ((y - w[1]) < (x - w[0]) * w[2])
+    return int((~solid).sum()) * g.nk
+
+
+# kernels of the step that make up its chemistry (the rest: ghost fills, CFL,
+# flux sweeps and stage updates)
+CHEM_KERNELS = {"cell_imex", "cell_adapt", "sur_gate", "sur_mlp", "sur_apply", "sur_fallback", "sur_mlp_apply"}
 
 
 def developed_state(mech, ni, nj, nk, steps2d, seed):
@@ -352,7 +372,8 @@ def run_ours(a, rank, world, local):
     dev = gpu.DeviceFlowfield(mech, grid, quirks=gpu.QUIRKS_FIXED, flux_bits=a.flux_bits, device=local)
     setup_odw(dev, case)
     dev.set_elements(S.atoms_matrix(mech))
-    model.attach(dev, 4099)
+    model.attach(dev, 4099, gate=S.GATE)
+    fluid = fluid_cells(case, i0, n_loc) if world > 1 else fluid_cells(case)
 
     def reset():
         extrude_state(d2, dev, i0=i0)
@@ -384,20 +405,42 @@ def run_ours(a, rank, world, local):
         profs[name] = profiled(dev, step, a.steps)
     hbm, tfl, src = peaks()
     prof = profs["surrogate"]
-    prof_total = sum(v[0] for v in prof.values())
-    launches = sum(v[1] for v in prof.values()) * a.steps // max(a.steps, 1)
-    rf = roofline(prof, cells, hbm, tfl, src, pb=4 if a.flux_bits == 32 else 8)
+    st = statuses["surrogate"]
+    # cells one launch must process: the fluid cells of this rank; the network
+    # takes the cells the frozen-chemistry gate listed, per step
+    steps_run = a.steps + W
+    net_cells = (st["surrogate_cells"] + st["surrogate_fallback"] + st["surrogate_audited"]) // max(steps_run, 1)
+    units = {k: fluid for k in kernel_work(4)}
+    units["sur_mlp"] = units["sur_mlp_apply"] = net_cells
+    pb = 4 if a.flux_bits == 32 else 8
+    rf = roofline(prof, units, hbm, tfl, src, pb=pb)
+    rf_more = {k: {f: r[f] for f in ("achieved", "unit", "frac", "avg_ms", "cells", "per_cell")}
+               for k, r in ((k, roofline(prof, units, hbm, tfl, src, pb=pb, kernel=k))
+                            for k in ("advection", "cell_rk1", "cell_rk2", "sur_mlp", "sur_apply") if k in prof)}
     ms = timing["surrogate"]
     value = cells * a.steps / (ms * 1e-3) / 1e6
     integ = {k: cells * a.steps / (timing[k] * 1e-3) / 1e6 for k in ("imex", "adaptive")}
-    st = statuses["surrogate"]
-    tot = st["surrogate_cells"] + st["surrogate_fallback"]
+    tot = st["surrogate_cells"] + st["surrogate_fallback"] + st["surrogate_audited"] + st["surrogate_frozen"]
+    # per-step split from the per-kernel events: chemistry and the rest
+    split = {}
+    for f, pr in profs.items():
+        chem = sum(v[0] for k, v in pr.items() if k in CHEM_KERNELS) / a.steps
+        rest = sum(v[0] for k, v in pr.items() if k not in CHEM_KERNELS) / a.steps
+        split[f] = {"chemistry_ms": chem, "non_chemistry_ms": rest}
+    nc = split["imex"]["non_chemistry_ms"]
+    amdahl = (nc + split["imex"]["chemistry_ms"]) / nc
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": W,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "bf16 (network) + f64 (state, decode, fallback integrator)", "data": "synthetic",
         "config": {"workload": workload_name(ni, nj, nk),
-                   "cells": cells, "cells_per_gpu": n_loc * nj * nk, "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback",
+                   "cells": cells, "cells_per_gpu": n_loc * nj * nk,
+                   "fluid_cells_per_gpu": fluid,
+                   "cell_count_note": "value counts every interior cell of the grid, the wedge's solid ones "
+                                      "included; the kernels skip solid cells (and the flux kernel all-solid "
+                                      "tiles), so per fluid cell the rate is value x cells / fluid cells",
+                   "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback; frozen-chemistry "
+                                "gate: cells below 600 K with radicals <= 1e-6 skip the network",
                    "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state",
                    "time": f"SSP-RK2, CFL {CFL}",
                    "state": f"developed: 2D case advanced {a.develop} steps with the FP64 adaptive integrator, "
@@ -409,26 +452,37 @@ def run_ours(a, rank, world, local):
         "integrator": {"imex_value": integ["imex"], "adaptive_value": integ["adaptive"],
                        "ratio_vs_imex": value / integ["imex"], "ratio_vs_adaptive": value / integ["adaptive"],
                        "ms_per_step": {k: timing[k] / a.steps for k in timing},
+                       "split_ms_per_step": split,
+                       "amdahl_bound_vs_imex": amdahl,
+                       "amdahl_note": "the IMEX step over its non-chemistry part: the ratio a free chemistry would "
+                                      "reach against plain IMEX with the same flux, stage and boundary kernels",
                        "note": "same GPU, same state and step; imex = the reference's one-step FP64 IMEX, "
                                "adaptive = FP64 adaptive integrator (the surrogate's teacher and fallback)"},
-        "surrogate": {"fallback_frac": st["surrogate_fallback"] / max(tot, 1), "rejects": st["surrogate_rejects"],
+        "surrogate": {"fallback_frac": st["surrogate_fallback"] / max(tot, 1),
+                      "frozen_frac": st["surrogate_frozen"] / max(tot, 1), "rejects": st["surrogate_rejects"],
                       "audited": st["surrogate_audited"], "audit_max_dT_K": st["surrogate_audit_max_dT"],
+                      "frozen_audited": st["frozen_audited"], "frozen_audit_max_dT_K": st["frozen_audit_max_dT"],
                       "model": os.path.relpath(a.model, ROOT)},
         "gpu_launches": int(sum(v[1] for v in prof.values())),
         "kernels": {f: {k: {"ms_avg": v[0] / v[1], "share": v[0] / sum(x[0] for x in profs[f].values()),
                             "launches": v[1]} for k, v in sorted(profs[f].items(), key=lambda kv: -kv[1][0])}
                     for f in profs},
         "roofline": rf,
+        "roofline_other_kernels": rf_more,
         "status": {k: st[k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")},
     }
     if clocks:
         out["clocks"] = clocks
     if not a.no_accuracy and rank == 0:
+        # errors of the FP32-flux, surrogate and IMEX forms against the all-FP64 run
         from eu3d_b200.validate import accuracy_2d, accuracy_3d
         out["accuracy"] = accuracy_2d(mech, model, a.accuracy_steps, cfl=CFL)
         out["accuracy_3d"] = accuracy_3d(mech, model, a.accuracy_steps, nk=16, cfl=CFL)
         if a.accuracy_full:
             out["accuracy_full_grid"] = accuracy_3d(mech, model, a.accuracy_steps, ni, nj, nk, cfl=CFL)
+        else:
+            out["accuracy_full_grid"] = ("not run by default (about five minutes): python -m eu3d_b200.validate "
+                                         "--grid 512,256,256, or bench.py --accuracy-full")
     if not a.no_e2e:
         reset()
         out["e2e"] = run_e2e(dev, stepper(dict(base, react=gpu.REACT_SURROGATE)), a.steps, cells, torch, world, dist)
@@ -473,7 +527,8 @@ def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
     return {"value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
             "d2h_bytes_per_step": d2h // K, "ms": ms,
             "protocol": "upload CS,T,E (pinned) + decode, K eu3d_step calls (surrogate chemistry) each with a status "
-                        "read, download CS,T"}
+                        "read, download CS,T; the state stays on the device between steps (the drop-in's design), "
+                        "so the host copies are amortised over the K steps and the value depends on K"}
 
 
 def workload_name(ni, nj, nk):

@@ -377,10 +377,13 @@ struct AdaptCfg {
 };
 
 // One substep of chem_adaptive: cs, T advance by h, the time left trem
-// shrinks by h, the count k grows by one.
+// shrinks by h, the count k grows by one.  forced is set when the substep
+// cap made h longer than the controller's choice (h = dt / nmax at least,
+// the last allowed substep takes the time left).
 template <bool SPEC>
 __device__ __forceinline__ void adapt_substep(double cs[NV], double &T, double Eold, unsigned qk, double &trem, int &k,
-                                              double hmin, const AdaptCfg &cfg, Decoded &o, int &capped_any)
+                                              double hmin, const AdaptCfg &cfg, Decoded &o, int &capped_any,
+                                              int &forced)
 {
     double CMS[NS], MD[NS];
     imex_source<SPEC>(cs, T, qk, CMS, MD, false);
@@ -394,8 +397,10 @@ __device__ __forceinline__ void adapt_substep(double cs[NV], double &T, double E
         if (w > 0.0) h = fmin(h, cfg.rel * (cs[s] + 1e-9 * D) / w);
         if (MD[s] > 0.0) h = fmin(h, cfg.amp / MD[s]);
     }
+    const double hc = h;
     h = fmin(fmax(h, hmin), trem);
     if (k == cfg.nmax - 1) h = trem;
+    if (h > hc) forced = 1;
 #pragma unroll
     for (int s = 0; s < NS; s++) cs[s] = fmax(cs[s] + h * CMS[s] / (1.0 - h * MD[s]), 0.0);
     int cp = 0;
@@ -408,13 +413,13 @@ __device__ __forceinline__ void adapt_substep(double cs[NV], double &T, double E
 
 template <bool SPEC>
 __device__ __forceinline__ int chem_adaptive(double cs[NV], double &T, double Eold, unsigned qk, double dt,
-                                             const AdaptCfg &cfg, int &capped_any)
+                                             const AdaptCfg &cfg, int &capped_any, int &forced)
 {
     double trem = dt;
     int k = 0;
     const double hmin = dt / cfg.nmax;
     Decoded o;
-    while (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Eold, qk, trem, k, hmin, cfg, o, capped_any);
+    while (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Eold, qk, trem, k, hmin, cfg, o, capped_any, forced);
     return k;
 }
 
@@ -473,13 +478,13 @@ __device__ __forceinline__ void elem_project(const double Y[NS], double dY[NS], 
 template <bool SPEC>
 __device__ __forceinline__ int chem_increment(const double cs0[NV], double T0, double Eold, unsigned qk, double dt,
                                               const AdaptCfg &cfg, double proj_eps, double dY[NS], double &Tchem,
-                                              int &capped_any)
+                                              int &capped_any, int &forced)
 {
     double cs[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) cs[v] = cs0[v];
     double T = T0;
-    const int n = chem_adaptive<SPEC>(cs, T, Eold, qk, dt, cfg, capped_any);
+    const int n = chem_adaptive<SPEC>(cs, T, Eold, qk, dt, cfg, capped_any, forced);
     double D0 = 0.0, Dn = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
@@ -562,7 +567,7 @@ __device__ __forceinline__ double rhs_at(const CellArgs &a, long long i)
 // a decode (o).  Returns the substeps taken.
 template <class P, bool SPEC>
 __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, double cs[NV], double T, double Eold,
-                                                bool with_rhs, Decoded &o, int &capped_any)
+                                                bool with_rhs, Decoded &o, int &capped_any, int &forced)
 {
     const long long fs = a.L.fs;
     const unsigned qk = a.quirks;
@@ -589,7 +594,7 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
         o.D = D;
     }
     double dY[NS], Tc;
-    const int n = chem_increment<SPEC>(cs, o.T, o.E, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped_any);
+    const int n = chem_increment<SPEC>(cs, o.T, o.E, qk, dt, a.acfg, a.proj_eps, dY, Tc, capped_any, forced);
     const double D = o.D;
 #pragma unroll
     for (int s = 0; s < NS; s++) cs[s] = fmax(D * (o.Y[s] + dY[s]), 0.0);
@@ -647,8 +652,10 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
         // split step: the flux residual first (Update_after_Adv + decode),
         // then the chemistry of the closed reactor at that state over dt
         // (adaptive integrator, element-projected), then a decode
-        const int nsub = adapt_split_step<P, SPEC>(a, c, cs, T, Eold, !a.rhs_applied, o, capped_any);
+        int forced = 0;
+        const int nsub = adapt_split_step<P, SPEC>(a, c, cs, T, Eold, !a.rhs_applied, o, capped_any, forced);
         warp_sum(&a.st->substeps, (unsigned long long)nsub);
+        if (forced) atomicAdd(&a.st->substep_capped, 1);
     } else if (MODE == M_DECODE) {
         decode(cs, T, Eold, qk, o, capped);
         capped_any |= capped;

@@ -61,6 +61,10 @@ struct Status {
     unsigned long long audit_max_dT_bits;  // largest |T_surrogate - T_integrator| (double bits)
     unsigned long long sur_reject[4];      // rejections: envelope, network output, energy residual, decode
     unsigned long long wait_timeouts;      // kernels that gave up a bounded wait (shared-memory ring, TMA)
+    unsigned long long sur_frozen;         // cells the frozen-chemistry gate left out of the network
+    unsigned long long frozen_audit_cells; // of those, cells also run through the integrator
+    unsigned long long frozen_audit_max_dT_bits;  // largest |T_integrator - T| over them (double bits)
+    unsigned long long drain_timeouts;     // a bounded wait for copies in flight after a timeout ran out too
 };
 
 // Powers of T shared by every species' polynomial at one temperature.

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -89,6 +90,8 @@ struct eu3d_handle {
     int chem_queue = 1; // adaptive trapezoid on the persistent work queue (0: one thread per cell)
     int queue_blocks = 3;  // resident queue blocks per SM
     int sur_fused = 0;     // surrogate: network and apply in one kernel (1) or two kernels (0, faster)
+    unsigned wait_tries = 1u << 19;  // bound of the flux ring's copy waits (eu3d_set_wait_limit)
+    int adapt_queue = 0;   // FP64 adaptive chemistry on the persistent queue (1) or one thread per cell (0)
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
@@ -111,6 +114,10 @@ struct eu3d_handle {
     double *sur_audit = nullptr;
     long long sur_cap = 0;
     int sur_audit_stride = 0;
+    int *sur_active = nullptr;  // cells the frozen-chemistry gate passes to the network
+    double gate_T = 0.0, gate_y = 0.0;  // eu3d_set_surrogate_gate (gate_T = 0: off)
+    unsigned gate_mask = 0;
+    int gate_audit = 0;
     // result files (eu3d_write_tecplot): gathered columns on the device and in
     // pinned host memory, and the background writer
     double *tp_dev = nullptr, *tp_host = nullptr;
@@ -364,6 +371,7 @@ void launch_adv_t(eu3d_handle *h)
     const int sq = (h->quirks & EU3D_Q_SPECIES_FACES) ? 1 : 0;
     const Layout &L = h->L;
     const int kz = h->flux_kz;
+    const FluxSolid wedge{h->wedge[0], h->wedge[1], h->wedge[2], h->wedge_on};
     constexpr int TY = FluxTile<P>::TY;
     dim3 g((L.ni + FT_X - 1) / FT_X, (L.nj + TY - 1) / TY, (L.nk + kz - 1) / kz);
     dim3 b(FT_X, TY + 2);
@@ -375,19 +383,19 @@ void launch_adv_t(eu3d_handle *h)
             dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
             dim3 bs(FT_X, FR_TY + 2);
             k_flux_ring<DIFF><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs,
-                                                                 sq, kz, h->status);
+                                                                 sq, kz, h->status, wedge, h->wait_tries);
             return;
         }
         if (h->flux_stage) {
             dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FS_TY - 1) / FS_TY, (L.nk + kz - 1) / kz);
             dim3 bs(FT_X, FS_TY + 2);
             k_flux_stage<DIFF><<<gs, bs, FluxStage::SMEM, h->st>>>(L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs, sq,
-                                                                   kz);
+                                                                   kz, wedge);
             return;
         }
     }
     k_flux_tile<P, DIFF><<<g, b, smem, h->st>>>(L, (const P *)h->prim, h->xn, h->yn, h->zn, h->scal, (P *)h->rhs, sq,
-                                                kz);
+                                                kz, wedge);
 }
 
 template <class P>
@@ -722,7 +730,7 @@ void free_handle(eu3d_handle *h)
                     h->nchem,   h->xn,     h->yn,     h->zn,      h->scal,      h->partial,
                     h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
                     h->sur_audit, h->qlist,   h->qbins,  h->wedge_band, h->dlb_rowload, h->g_cs,
-                    h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim};
+                    h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim, h->sur_active};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->writer.joinable()) h->writer.join();
@@ -776,6 +784,66 @@ int stage_op(eu3d_handle *h, const eu3d_step_desc *s, int stage)
     return EU3D_OK;
 }
 
+// Cell list and queue buffers shared by the surrogate's fallback and the
+// queued adaptive chemistry (allocated outside any stream capture).
+int ensure_cell_list(eu3d_handle *h)
+{
+    const long long n = h->L.interior_cells();
+    if (h->L.fs > (long long)SUR_CELL_MASK) return fail(EU3D_ERR_ARG, "grid too large for the cell list");
+    if (h->sur_cap < n) {
+        CK(cudaStreamSynchronize(h->st));
+        void *ptrs[] = {h->sur_out, h->sur_list, h->sur_audit, h->sur_active};
+        for (void *q : ptrs)
+            if (q) cudaFree(q);
+        h->sur_out = nullptr;
+        h->sur_list = nullptr;
+        h->sur_audit = nullptr;
+        h->sur_active = nullptr;
+        h->sur_cap = 0;
+        CK(cudaMalloc(&h->sur_out, (size_t)n * SUR_NOUT * sizeof(float)));
+        CK(cudaMalloc(&h->sur_list, (size_t)n * sizeof(int)));
+        CK(cudaMalloc(&h->sur_audit, (size_t)n * sizeof(double)));
+        CK(cudaMalloc(&h->sur_active, (size_t)n * sizeof(int)));
+        h->sur_cap = n;
+    }
+    if (!h->sur_count) CK(cudaMalloc(&h->sur_count, 4 * sizeof(int)));
+    return EU3D_OK;
+}
+
+// FP64 adaptive chemistry on the persistent queue (tuning adapt_queue): every
+// fluid cell is listed and the surrogate's fallback workers integrate them,
+// one cell per lane with refill, so a warp never waits for the slowest cell
+// of a fixed batch.  Same split step and arithmetic as k_cell<M_ADAPT>.
+template <class P, bool SPEC>
+void adapt_queue_t(eu3d_handle *h, bool decoded)
+{
+    const Layout &L = h->L;
+    P *q = (P *)h->prim;
+    cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
+    if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
+    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, L.interior_cells()};
+    {
+        ProfScope ps(h, "adapt_list");
+        k_list_fluid<<<cell_grid(L, 256), 256, 0, h->st>>>(cell_args(h), qu);
+    }
+    ProfScope ps(h, "adapt_queue");
+    k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+}
+
+int adapt_queue_op(eu3d_handle *h, bool decoded)
+{
+    if (!h->sur_count) return fail(EU3D_ERR_STATE, "adaptive queue buffers missing");
+    if (h->flux_bits == 64) {
+        if (h->spec) adapt_queue_t<double, true>(h, decoded);
+        else adapt_queue_t<double, false>(h, decoded);
+    } else {
+        if (h->spec) adapt_queue_t<float, true>(h, decoded);
+        else adapt_queue_t<float, false>(h, decoded);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
 int react_op(eu3d_handle *h, const eu3d_step_desc *s)
 {
     switch (s->react) {
@@ -787,6 +855,7 @@ int react_op(eu3d_handle *h, const eu3d_step_desc *s)
     // after SSP-RK the state is decoded and RHS holds zeros already
     case EU3D_REACT_SURROGATE: return sur_chem_op(h, is_rk(s->timeadv));
     case EU3D_REACT_ADAPTIVE: {
+        if (h->adapt_queue) return adapt_queue_op(h, is_rk(s->timeadv));
         h->rhs_applied = is_rk(s->timeadv);
         const int rc = cell_op(h, M_ADAPT);
         h->rhs_applied = false;
@@ -834,7 +903,9 @@ static __device__ __align__(256) double g_cfl_scratch[NOALLOC_CFL_MAX_BLOCKS];
 // Device address of g_cfl_scratch per device.  In host code the symbol
 // g_cfl_scratch names a host-side stand-in, not device memory, so kernels are
 // given this address, obtained once per device with that device current.
-double *g_cfl_scratch_dev[NOALLOC_MAX_DEVICES] = {};
+// Atomic: host threads making their first call on one device at the same time
+// may both look it up (the same value); neither reads a torn pointer.
+std::atomic<double *> g_cfl_scratch_dev[NOALLOC_MAX_DEVICES] = {};
 
 struct CflFields {
     const double *D, *U, *V, *W, *P, *G;
@@ -1508,6 +1579,8 @@ int ensure_guest(eu3d_handle *h, long long cells)
 {
     if (cells <= h->g_cap) return EU3D_OK;
     const long long cap = std::max<long long>(cells, 2 * h->g_cap);
+    // earlier guest work queued on the handle's stream may still read the old store
+    CK(cudaStreamSynchronize(h->st));
     void *old[] = {h->g_cs, h->g_T, h->g_E, h->g_nchem, h->g_list, h->g_prim};
     for (void *p : old)
         if (p) cudaFree(p);
@@ -1767,12 +1840,13 @@ int eu3d_cfl_noalloc(const double *D, const double *U, const double *V, const do
     int dev = 0;
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(EU3D_ERR_ARG, "device ordinal beyond 63");
-    if (!g_cfl_scratch_dev[dev]) {
+    double *scratch = g_cfl_scratch_dev[dev].load(std::memory_order_acquire);
+    if (!scratch) {
         void *p = nullptr;
         CK(cudaGetSymbolAddress(&p, g_cfl_scratch));
-        g_cfl_scratch_dev[dev] = (double *)p;
+        scratch = (double *)p;
+        g_cfl_scratch_dev[dev].store(scratch, std::memory_order_release);
     }
-    double *scratch = g_cfl_scratch_dev[dev];
     CflFields f{D, U, V, W, Pp, Gamma, ni, nj, nk, bc, pitch, plane};
     cudaStream_t st = (cudaStream_t)stream;
     k_cfl_fields_partial<<<nblocks, 256, 0, st>>>(f, dx, dy, dz, use_z, scratch);
@@ -1829,7 +1903,7 @@ int eu3d_react_adaptive(eu3d_handle *h)
 {
     if (!h) return fail(EU3D_ERR_ARG, "null handle");
     if (!h->elements) return fail(EU3D_ERR_STATE, "element composition not set (eu3d_set_elements)");
-    return cell_op(h, M_ADAPT);
+    return h->adapt_queue ? adapt_queue_op(h, false) : cell_op(h, M_ADAPT);
 }
 
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
@@ -1844,6 +1918,21 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
     h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
     h->sur_fused = t->sur_fused ? 1 : 0;
+    h->adapt_queue = t->adapt_queue ? 1 : 0;
+    if (h->adapt_queue) {
+        int rc = ensure_cell_list(h);
+        if (rc) return rc;
+    }
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    return EU3D_OK;
+}
+
+int eu3d_set_wait_limit(eu3d_handle *h, long long tries)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (tries < 0 || tries > (1LL << 24)) return fail(EU3D_ERR_ARG, "wait limit must be in [0, 2^24]");
+    h->wait_tries = (unsigned)tries;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;
@@ -1857,6 +1946,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
     t->queue_blocks = h->queue_blocks;
     t->flux_stage = h->flux_stage;
     t->sur_fused = h->sur_fused;
+    t->adapt_queue = h->adapt_queue;
     return EU3D_OK;
 }
 
@@ -1865,7 +1955,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
     CK(cudaSetDevice(h->dev));
-    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage, h->sur_fused};
+    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage, h->sur_fused, h->adapt_queue};
     // the trials advance the state: keep a copy and put it back after each
     const size_t fs = (size_t)h->L.fs;
     const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
@@ -1890,15 +1980,18 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     copy(true);
     std::vector<eu3d_tuning> cands;
     const bool q = s->react == EU3D_REACT_TRAPEZOID && s->type == 1;
+    const bool aq = s->react == EU3D_REACT_ADAPTIVE;
     for (int fst : {0, 1, 2})
-        for (int kz : {4, 8, 16, 32})
+        for (int kz : {4, 8, 16, 32, 64})
             for (int cq : {0, 1})
-                for (int qb : {2, 3, 4}) {
-                    if (h->flux_bits == 64 && fst != start.flux_stage) continue;
-                    if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
-                    if (q && cq == 0 && qb != start.queue_blocks) continue;
-                    cands.push_back({kz, cq, qb, fst, start.sur_fused});
-                }
+                for (int qb : {2, 3, 4})
+                    for (int ad : {0, 1}) {
+                        if (h->flux_bits == 64 && fst != start.flux_stage) continue;
+                        if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
+                        if (q && cq == 0 && qb != start.queue_blocks) continue;
+                        if (!aq && ad != start.adapt_queue) continue;
+                        cands.push_back({kz, cq, qb, fst, start.sur_fused, ad});
+                    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1967,6 +2060,11 @@ int eu3d_get_status(eu3d_handle *h, eu3d_status *o)
     o->surrogate_audit_max_dT = mx;
     for (int r = 0; r < 4; r++) o->surrogate_rejects[r] = (long long)s.sur_reject[r];
     o->wait_timeouts = (long long)s.wait_timeouts;
+    o->surrogate_frozen = (long long)s.sur_frozen;
+    o->frozen_audited = (long long)s.frozen_audit_cells;
+    memcpy(&mx, &s.frozen_audit_max_dT_bits, sizeof(double));
+    o->frozen_audit_max_dT = mx;
+    o->drain_timeouts = (long long)s.drain_timeouts;
     o->dt = sc[0];
     o->time = sc[1];
     return EU3D_OK;

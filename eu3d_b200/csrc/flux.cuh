@@ -312,6 +312,18 @@ __device__ __forceinline__ void face_flux_up(const P *__restrict__ qc, int fs, i
     }
 }
 
+// Wedge immersed boundary as the flux kernels see it: a tile none of whose
+// cells is fluid forms no residual (nothing reads the residual of a solid
+// cell: the stage updates, the chemistry and the surrogate skip them).
+struct FluxSolid {
+    double x0, y0, tn;
+    int on;
+    __device__ __forceinline__ bool solid(double x, double y) const
+    {
+        return on && x > x0 && (y - y0) < (x - x0) * tn;
+    }
+};
+
 constexpr int FT_X = 32;
 // tile height: 8 rows for FP32 primitives, 4 for FP64; face fluxes live in
 // dynamic shared memory (two buffers of x and y faces)
@@ -342,7 +354,8 @@ constexpr int flux_threads()
 template <class P, int DIFF>
 __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
     Layout L, const P *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
-    const double *__restrict__ zn, const double *__restrict__ dtp, P *__restrict__ rhs, int species_quirk, int kz)
+    const double *__restrict__ zn, const double *__restrict__ dtp, P *__restrict__ rhs, int species_quirk, int kz,
+    FluxSolid wedge)
 {
     constexpr int TY = FluxTile<P>::TY;
     // two buffers: plane k+1 may fill one while slow threads still read plane k
@@ -357,6 +370,7 @@ __global__ void __launch_bounds__(flux_threads<P>(), 2) k_flux_tile(
     const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
     const bool cellw = ty < TY;  // warps that own cells (the other two only add faces)
     const bool act = cellw && i <= ilast && j <= jlast;
+    if (!__syncthreads_or(act && !wedge.solid(xn[i], yn[j]))) return;  // an all-solid tile
     const int fs = (int)L.fs, sy = L.px, sz = L.px * L.NJ;
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
@@ -414,7 +428,8 @@ struct FluxStage {
 template <int DIFF>
 __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
     Layout L, const float *__restrict__ q, const double *__restrict__ xn, const double *__restrict__ yn,
-    const double *__restrict__ zn, const double *__restrict__ dtp, float *__restrict__ rhs, int species_quirk, int kz)
+    const double *__restrict__ zn, const double *__restrict__ dtp, float *__restrict__ rhs, int species_quirk, int kz,
+    FluxSolid wedge)
 {
     constexpr int TY = FS_TY, HX = FS_HX, HY = FS_HY, PL = HX * HY;
     extern __shared__ __align__(16) unsigned char flux_smem[];
@@ -430,6 +445,7 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
     const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
     const bool cellw = ty < TY;
     const bool act = cellw && i <= ilast && j <= jlast;
+    if (!__syncthreads_or(act && !wedge.solid(xn[i], yn[j]))) return;  // an all-solid tile
     const int fs = (int)L.fs, sz = L.px * L.NJ;
     const double dt = *dtp;
     const bool zs_cell = species_quirk && i >= L.ni;
@@ -525,7 +541,8 @@ template <int DIFF>
 __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     const __grid_constant__ CUtensorMap tq, Layout L, const float *__restrict__ q, const double *__restrict__ xn,
     const double *__restrict__ yn, const double *__restrict__ zn, const double *__restrict__ dtp,
-    float *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat)
+    float *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat, FluxSolid wedge,
+    unsigned wait_tries)
 {
     constexpr int TY = FR_TY, HX = FR_HX, PL = FR_PL;
     extern __shared__ unsigned char fr_raw[];
@@ -543,6 +560,8 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     const int ilast = L.ni + L.bc - 1, jlast = L.nj + L.bc - 1;
     const bool cellw = ty < TY;
     const bool act = cellw && i <= ilast && j <= jlast;
+    // an all-solid tile leaves before its barriers and copies exist
+    if (!__syncthreads_or(act && !wedge.solid(xn[i], yn[j]))) return;
     const int fs = (int)L.fs, sz = L.px * L.NJ;
     // plane kb + p into buffer p % 3; the block loads planes kb .. kb + np
     // (the last one only feeds the top z face).  x = i0 - 2 = 32 blockIdx.x
@@ -575,8 +594,8 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     int p = 0;
     for (; p < np; p++) {
         const int b0 = p % FR_NBUF, b1 = (p + 1) % FR_NBUF;
-        if (p == 0) ok = tc::mbar_wait(mb_s + 8u * b0, 0) && ok;
-        ok = tc::mbar_wait(mb_s + 8u * b1, ((p + 1) / FR_NBUF) & 1) && ok;
+        if (p == 0) ok = tc::mbar_wait(mb_s + 8u * b0, 0, wait_tries) && ok;
+        ok = tc::mbar_wait(mb_s + 8u * b1, ((p + 1) / FR_NBUF) & 1, wait_tries) && ok;
         const float *S0 = ring + b0 * FluxRing::PLANE, *S1 = ring + b1 * FluxRing::PLANE;
         const int k = kb + p;
         // y face g = ty of column i, between b = j0+g-1 and b+1 (staged rows
@@ -628,10 +647,16 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         }
     }
     if (p < np) {
-        // a wait ran out: count it, let the copies in flight land, stop
+        // a wait ran out: count it, let the copies in flight land (with the
+        // full bound, whatever wait_tries was), stop.  If even that wait runs
+        // out, copies may still be writing this block's shared memory when it
+        // exits: drain_timeouts marks the device state as untrusted.
         if (tid == 0) {
             atomicAdd(&stat->wait_timeouts, 1ull);
-            for (int pl = p; pl < issued; pl++) tc::mbar_wait(mb_s + 8u * (pl % FR_NBUF), (pl / FR_NBUF) & 1);
+            bool drained = true;
+            for (int pl = p; pl < issued; pl++)
+                drained = tc::mbar_wait(mb_s + 8u * (pl % FR_NBUF), (pl / FR_NBUF) & 1) && drained;
+            if (!drained) atomicAdd(&stat->drain_timeouts, 1ull);
         }
         __syncthreads();
     }

@@ -218,6 +218,8 @@ int sur_set_attrs()
                             SURK_SMEM));
     CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcFieldApply<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             SURK_SMEM));
+    CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcList<float>>, cudaFuncAttributeMaxDynamicSharedMemorySize, SURK_SMEM));
+    CK(cudaFuncSetAttribute(k_sur_mlp<SurSrcList<double>>, cudaFuncAttributeMaxDynamicSharedMemorySize, SURK_SMEM));
     done = true;
     return EU3D_OK;
 }
@@ -230,7 +232,8 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     const Layout &L = h->L;
     const long long n = L.interior_cells();
     P *q = (P *)h->prim;
-    cudaMemsetAsync(h->sur_count, 0, 2 * sizeof(int), h->st);
+    // [0] fallback list length, [1] its work cursor, [2] active list length
+    cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
     // split step: the flux update and its decode first (Update_after_Adv),
     // unless the time scheme left the state decoded with the update in
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
@@ -238,7 +241,30 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     SurApplyArgs a{cell_args(h), s->norm_d, h->sur_out, n, qu, h->sur_audit_stride};
     const SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
     const long long ntiles = src.ntiles();
-    if (h->sur_fused) {
+    if (h->gate_T > 0.0) {
+        // frozen-chemistry gate: the network and its apply take the listed
+        // (active) cells only
+        int *acount = h->sur_count + 2;
+        {
+            ProfScope ps(h, "sur_gate");
+            const SurGate g{h->gate_T, h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, acount};
+            k_sur_gate<P><<<cell_grid(L, 256), 256, 0, h->st>>>(cell_args(h), q, g, qu);
+        }
+        const SurSrcList<P> lsrc{L, h->T, q, h->scal, h->sur_out, h->sur_active, acount, n};
+        {
+            ProfScope ps(h, "sur_mlp");
+            k_sur_mlp<SurSrcList<P>><<<sur_grid(lsrc.ntiles()), 128 * SUR_NG, SURK_SMEM, h->st>>>(
+                sur_weights(s), s->norm_d, lsrc, lsrc.ntiles(), s->err);
+        }
+        {
+            ProfScope ps(h, "sur_apply");
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
+            const long long need = (n + 127) / 128;
+            k_sur_apply_list<P><<<(unsigned)std::max<long long>(1, std::min<long long>(need, 7LL * sms)), 128, 0,
+                                  h->st>>>(a, q, h->sur_active, acount);
+        }
+    } else if (h->sur_fused) {
         // network and apply in one kernel (outputs stay on chip)
         ProfScope ps(h, "sur_mlp_apply");
         SurSrcFieldApply<P> fsrc;
@@ -598,27 +624,30 @@ int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride)
     if (s) {
         if (s->dev != h->dev) return fail(EU3D_ERR_ARG, "surrogate on another device");
         if (s->quirks != h->quirks) return fail(EU3D_ERR_ARG, "surrogate trained under another quirk policy");
-        const long long n = h->L.interior_cells();
-        if (n >= (1LL << 31)) return fail(EU3D_ERR_ARG, "grid too large for the fallback list");
-        if (h->sur_cap < n) {
-            void *ptrs[] = {h->sur_out, h->sur_list, h->sur_audit};
-            for (void *q : ptrs)
-                if (q) cudaFree(q);
-            h->sur_out = nullptr;
-            h->sur_list = nullptr;
-            h->sur_audit = nullptr;
-            h->sur_cap = 0;
-            CK(cudaMalloc(&h->sur_out, (size_t)n * SUR_NOUT * sizeof(float)));
-            CK(cudaMalloc(&h->sur_list, (size_t)n * sizeof(int)));
-            CK(cudaMalloc(&h->sur_audit, (size_t)n * sizeof(double)));
-            h->sur_cap = n;
-        }
-        if (!h->sur_count) CK(cudaMalloc(&h->sur_count, 2 * sizeof(int)));
+        // network outputs, active and fallback lists (list entries carry the
+        // ghosted cell index in 30 bits)
+        int rc = ensure_cell_list(h);
+        if (rc) return rc;
     }
     h->sur = s;
     h->sur_audit_stride = audit_stride;
     if (s) h->elements = true;  // eu3d_sur_create loaded the element matrix on this device
     // recorded step graphs hold the previous surrogate's buffers and settings
+    for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
+    h->graphs.clear();
+    return EU3D_OK;
+}
+
+int eu3d_set_surrogate_gate(eu3d_handle *h, double t_frozen, double y_max, unsigned species_mask, int audit_stride)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    if (!(t_frozen >= 0.0) || !(y_max >= 0.0)) return fail(EU3D_ERR_ARG, "gate temperature and fraction must be >= 0");
+    if (species_mask >> NS) return fail(EU3D_ERR_ARG, "species mask names a species past NS");
+    if (audit_stride < 0) return fail(EU3D_ERR_ARG, "audit stride must be >= 0");
+    h->gate_T = t_frozen;
+    h->gate_y = y_max;
+    h->gate_mask = species_mask;
+    h->gate_audit = audit_stride;
     for (auto &g : h->graphs) cudaGraphExecDestroy(g.second);
     h->graphs.clear();
     return EU3D_OK;

@@ -215,7 +215,8 @@ __global__ void __launch_bounds__(128, 3)
     if (kind == SUR_LABEL_ADAPTIVE) {
         int cp = 0;
         acfg.nmax = cap;
-        nsub = chem_increment<SPEC>(cs, T0, E0, q, dt, acfg, proj_eps, dY, Tg, cp);
+        int forced = 0;
+        nsub = chem_increment<SPEC>(cs, T0, E0, q, dt, acfg, proj_eps, dY, Tg, cp, forced);
         bad |= cp;
         projected = true;
     } else if (kind == SUR_LABEL_IMEX) {
@@ -381,6 +382,7 @@ struct SurSrcArray {  // normalised features, n x 16 FP32; outputs n x 16
     float *out;
     long long n;
     long long ntiles() const { return (n + 127) / 128; }
+    __device__ __forceinline__ long long tiles(long long host_tiles) const { return host_tiles; }
     __device__ __forceinline__ bool load(long long tile, int lane, const SurNorm &, float f[SUR_IN], long long &idx) const
     {
         idx = tile * 128 + lane;
@@ -406,6 +408,21 @@ struct SurSrcArray {  // normalised features, n x 16 FP32; outputs n x 16
 
 // Tiles follow x rows (tpr tiles of 128 cells per row) so that a tile's
 // cells are contiguous in memory and no 64-bit division is needed.
+// normalised network inputs of flowfield cell c: T, ln(p / 1 atm), ln(Y_k + floor), ln dt
+template <class P>
+__device__ __forceinline__ void sur_cell_features(const SurNorm &nrm, const double *__restrict__ T,
+                                                  const P *__restrict__ prim, long long fs, const double *scal,
+                                                  long long c, float f[SUR_IN])
+{
+    float raw[SUR_NIN];
+    raw[0] = (float)T[c];
+    raw[1] = __logf((float)prim[PP * fs + c] * (float)(1.0 / ATM_PA));
+#pragma unroll
+    for (int s = 0; s < NS; s++) raw[2 + s] = __logf(fmaxf((float)prim[(PY + s) * fs + c], 0.f) + SUR_YFLOOR);
+    raw[11] = __logf((float)scal[0]);
+    sur_features(nrm, raw, f);
+}
+
 template <class P>
 struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
     Layout L;
@@ -416,6 +433,7 @@ struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
     long long n;
     int tpr;  // tiles per x row
     long long ntiles() const { return (long long)tpr * L.nj * L.nk; }
+    __device__ __forceinline__ long long tiles(long long host_tiles) const { return host_tiles; }
     __device__ __forceinline__ bool load(long long tile, int lane, const SurNorm &nrm, float f[SUR_IN],
                                          long long &idx) const
     {
@@ -425,20 +443,45 @@ struct SurSrcField {  // interior cells of a flowfield; outputs SoA (10 x n)
         if (i >= L.ni) return false;
         const int j = r % L.nj, k = r / L.nj;
         idx = (long long)r * L.ni + i;
-        const long long c = L.at(i + L.bc, j + L.bc, k + L.bc);
-        float raw[SUR_NIN];
-        raw[0] = (float)T[c];
-        raw[1] = __logf((float)prim[PP * L.fs + c] * (float)(1.0 / ATM_PA));
-#pragma unroll
-        for (int s = 0; s < NS; s++) raw[2 + s] = __logf(fmaxf((float)prim[(PY + s) * L.fs + c], 0.f) + SUR_YFLOOR);
-        raw[11] = __logf((float)scal[0]);
-        sur_features(nrm, raw, f);
+        sur_cell_features<P>(nrm, T, prim, L.fs, scal, L.at(i + L.bc, j + L.bc, k + L.bc), f);
         return true;
     }
     __device__ __forceinline__ void store(long long, int, long long idx, const float o[SUR_OUT]) const
     {
 #pragma unroll
         for (int k = 0; k < SUR_NOUT; k++) out[k * n + idx] = o[k];
+    }
+};
+
+// The cells of a list (the active cells the frozen-chemistry gate kept):
+// tile t takes list positions 128 t .. 128 t + 127; the list's length is on
+// the device, so the kernel reads its tile count there.  Outputs SoA
+// (10 x cap) by list position.
+template <class P>
+struct SurSrcList {
+    Layout L;
+    const double *T;
+    const P *prim;
+    const double *scal;
+    float *out;
+    const int *list;
+    const int *count;
+    long long cap;
+    long long ntiles() const { return (cap + 127) / 128; }  // a bound for the grid size
+    __device__ __forceinline__ long long total() const { return min((long long)*count, cap); }
+    __device__ __forceinline__ long long tiles(long long) const { return (total() + 127) / 128; }
+    __device__ __forceinline__ bool load(long long tile, int lane, const SurNorm &nrm, float f[SUR_IN],
+                                         long long &idx) const
+    {
+        idx = tile * 128 + lane;
+        if (idx >= total()) return false;
+        sur_cell_features<P>(nrm, T, prim, L.fs, scal, (long long)list[idx], f);
+        return true;
+    }
+    __device__ __forceinline__ void store(long long, int, long long idx, const float o[SUR_OUT]) const
+    {
+#pragma unroll
+        for (int k = 0; k < SUR_NOUT; k++) out[k * cap + idx] = o[k];
     }
 };
 
@@ -551,6 +594,7 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
                    bb3 = tc::smem_u32(sm + SURK_BB3), bb4 = tc::smem_u32(sm + SURK_BB4);
     uint32_t phase = 0;
     bool ok = true;
+    ntiles = src.tiles(ntiles);  // the list form reads its length on the device
 
     for (long long tile = (long long)blockIdx.x * SUR_NG + g; tile < ntiles; tile += (long long)gridDim.x * SUR_NG) {
         long long idx = 0;
@@ -612,10 +656,15 @@ __global__ void __launch_bounds__(128 * SUR_NG, 1) k_sur_mlp(SurWeights W, const
 }
 
 // ------------------------------------------------------ coupled-step apply
+// Fallback list entries: the cell index (below 2^30) with two flags.
+constexpr unsigned SUR_AUDIT = 0x80000000u;         // an accepted cell re-run to judge the network
+constexpr unsigned SUR_FROZEN_AUDIT = 0x40000000u;  // a frozen cell re-run to judge the gate
+constexpr int SUR_CELL_MASK = 0x3fffffff;
+
 struct SurQueue {
-    int *list;      // cell indices; bit 31 marks an audited cell
+    int *list;      // cell indices with the flags above
     int *count;     // [0] list length, [1] work cursor
-    double *audit;  // per list slot: the surrogate's T for audited cells
+    double *audit;  // per list slot: the temperature to judge for audited cells
     long long cap;
 };
 
@@ -749,7 +798,7 @@ __device__ __forceinline__ void sur_apply_cell(const SurApplyArgs &s, P *__restr
             store_prims<P>(o, q, fs, c);
         }
     }
-    sur_push(s.qu, !ok || audit, (int)c | (audit ? (int)0x80000000u : 0), audit ? o.T : 0.0);
+    sur_push(s.qu, !ok || audit, (int)((unsigned)c | (audit ? SUR_AUDIT : 0u)), audit ? o.T : 0.0);
     warp_count(&a.st->sur_cells, ok && !audit);
     warp_count(&a.st->sur_fallback, !ok);
     warp_count(&a.st->sur_reject[0], !ok_env);
@@ -773,6 +822,94 @@ __global__ void __launch_bounds__(128, 7) k_sur_apply(SurApplyArgs s, P *__restr
 #pragma unroll
     for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + idx];
     sur_apply_cell<P>(s, q, i, j, k, o);
+}
+
+// Frozen-chemistry gate.  A fluid cell colder than T_frozen whose summed
+// mass fraction over the species of `mask` (the radicals) is at most y_max
+// keeps the state its flux update and decode left: over one flow time step
+// its chemistry changes nothing the FP64 integrator would resolve (cold
+// H2-air ahead of the shock has ignition delays of seconds against steps of
+// tens of nanoseconds).  The other fluid cells are listed for the network.
+// Every audit_stride-th frozen cell (by interior index) is also sent to the
+// fallback queue, whose FP64 integrator records the largest temperature
+// change the gate ignored.
+struct SurGate {
+    double T_frozen;
+    double y_max;
+    unsigned mask;
+    int audit_stride;  // 0: no audit
+    int *active;       // listed cells (ghosted indices)
+    int *acount;       // list length
+};
+
+template <class P>
+__global__ void __launch_bounds__(256) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g, SurQueue qu)
+{
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    if (solid_cell(a, i, j)) return;
+    const long long c = L.at(i, j, k);
+    const double T = a.T[c];
+    bool frozen = T < g.T_frozen;
+    if (frozen && g.mask) {
+        double y = 0.0;
+#pragma unroll
+        for (int s = 0; s < NS; s++)
+            if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c], 0.0);
+        frozen = y <= g.y_max;
+    }
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    const bool audit = frozen && g.audit_stride > 0 && ((unsigned)idx % (unsigned)g.audit_stride) == 0;
+    {
+        // warp-aggregated append of the active cells, in lane order
+        const unsigned act = __activemask();
+        const unsigned m = __ballot_sync(act, !frozen);
+        if (m) {
+            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(g.acount, __popc(m));
+            base = __shfl_sync(act, base, leader);
+            if (!frozen) g.active[base + __popc(m & ((1u << lane) - 1u))] = (int)c;
+        }
+    }
+    sur_push(qu, audit, (int)((unsigned)c | SUR_FROZEN_AUDIT), T);
+    warp_count(&a.st->sur_frozen, frozen);
+}
+
+// Lists every fluid interior cell (the queued adaptive chemistry's work).
+__global__ void __launch_bounds__(256) k_list_fluid(CellArgs a, SurQueue qu)
+{
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y;
+    const int k = L.bc + blockIdx.z;
+    if (i >= L.ni + L.bc) return;
+    if (solid_cell(a, i, j)) return;
+    sur_push(qu, true, (int)L.at(i, j, k), 0.0);
+}
+
+// The apply of the listed cells (grid-stride over the list, whose length is
+// on the device); network outputs by list position.
+template <class P>
+__global__ void __launch_bounds__(128, 7) k_sur_apply_list(SurApplyArgs s, P *__restrict__ q,
+                                                           const int *__restrict__ list, const int *__restrict__ count)
+{
+    const Layout &L = s.a.L;
+    const long long total = min((long long)*count, s.n);
+    const int plane = L.NJ * L.px;
+    for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
+         pos += (long long)gridDim.x * blockDim.x) {
+        const int c = list[pos];
+        const int k = c / plane, r = c - k * plane;
+        const int j = r / L.px, i = r - j * L.px;
+        float o[SUR_NOUT];
+#pragma unroll
+        for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
+        sur_apply_cell<P>(s, q, i, j, k, o);
+    }
 }
 
 // The MLP kernel's source for the fused form: features from the flowfield
@@ -817,11 +954,11 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
     const AdaptCfg cfg = a.acfg;
     const double hmin = dt / cfg.nmax;
     int slot = -1;  // list slot of the lane's cell; -1: needs one; >= total: none left
-    bool audit = false;
+    bool audit = false, faudit = false;
     long long c = 0;
     double cs0[NV], cs[NV];  // the cell's state before the chemistry; the integrator's copy
     double T = 0.0, Esub = 0.0, trem = 0.0;
-    int k = 0, capped = 0;
+    int k = 0, capped = 0, forced = 0;
     Decoded o;
     for (;;) {
         const bool need = slot < 0;
@@ -834,9 +971,10 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
             if (need) {
                 slot = base + __popc(m & ((1u << lane) - 1u));
                 if (slot < total) {
-                    const int ent = qu.list[slot];
-                    audit = ent < 0;
-                    c = (long long)(ent & 0x7fffffff);
+                    const unsigned ent = (unsigned)qu.list[slot];
+                    audit = (ent & SUR_AUDIT) != 0;
+                    faudit = (ent & SUR_FROZEN_AUDIT) != 0;
+                    c = (long long)(ent & (unsigned)SUR_CELL_MASK);
                     load_cs(a.cs, fs, c, cs0);
                     // the decoded state (adapt_split_step without the flux
                     // update): the integrator runs at its energy from its T
@@ -852,12 +990,13 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
                     trem = dt;
                     k = 0;
                     capped = 0;
+                    forced = 0;
                 }
             }
         }
         if (__all_sync(0xffffffffu, slot >= total)) break;
         if (slot < total) {
-            if (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Esub, qk, trem, k, hmin, cfg, o, capped);
+            if (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Esub, qk, trem, k, hmin, cfg, o, capped, forced);
             if (!(trem > 0.0 && k < cfg.nmax)) {
                 // chem_increment's projection, then adapt_split_step's update and decode
                 double D0 = 0.0, Dn = 0.0;
@@ -886,12 +1025,14 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
                 a.E[c] = o.E;
                 store_prims<P>(o, q, fs, c);
                 if (capped) atomicAdd(&a.st->newton_capped, 1ull);
+                if (forced) atomicAdd(&a.st->substep_capped, 1);
                 if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
-                if (audit) {
+                if (audit || faudit) {
                     const double d = fabs(qu.audit[slot] - o.T);
-                    atomicAdd(&a.st->audit_cells, 1ull);
-                    if (isfinite(d)) atomicMax(&a.st->audit_max_dT_bits, (unsigned long long)__double_as_longlong(d));
-                    else atomicMax(&a.st->audit_max_dT_bits, 0x7ff0000000000000ull);
+                    unsigned long long *mx = audit ? &a.st->audit_max_dT_bits : &a.st->frozen_audit_max_dT_bits;
+                    atomicAdd(audit ? &a.st->audit_cells : &a.st->frozen_audit_cells, 1ull);
+                    if (isfinite(d)) atomicMax(mx, (unsigned long long)__double_as_longlong(d));
+                    else atomicMax(mx, 0x7ff0000000000000ull);
                 }
                 slot = -1;
             }

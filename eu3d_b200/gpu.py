@@ -39,7 +39,8 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_sur_dataset_size", "eu3d_sur_add_random", "eu3d_sur_add_snapshot", "eu3d_sur_label",
            "eu3d_sur_get_dataset", "eu3d_sur_set_norm", "eu3d_sur_get_norm", "eu3d_sur_set_params",
            "eu3d_sur_get_params", "eu3d_sur_train", "eu3d_sur_loss_grad", "eu3d_sur_predict", "eu3d_sur_infer",
-           "eu3d_set_surrogate", "eu3d_react_surrogate", "eu3d_set_tuning", "eu3d_get_tuning", "eu3d_autotune",
+           "eu3d_set_surrogate", "eu3d_set_surrogate_gate", "eu3d_react_surrogate", "eu3d_set_tuning",
+           "eu3d_set_wait_limit", "eu3d_get_tuning", "eu3d_autotune",
            "eu3d_set_elements", "eu3d_set_adaptive", "eu3d_react_adaptive", "eu3d_halo_bytes", "eu3d_halo_pack",
            "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
            "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host", "eu3d_dlb_plan",
@@ -75,7 +76,9 @@ class Status(C.Structure):
                 ("nchem_max", C.c_int), ("substep_capped", C.c_int), ("surrogate_cells", C.c_longlong),
                 ("surrogate_fallback", C.c_longlong), ("dt", C.c_double), ("time", C.c_double),
                 ("surrogate_audited", C.c_longlong), ("surrogate_audit_max_dT", C.c_double),
-                ("surrogate_rejects", C.c_longlong * 4), ("wait_timeouts", C.c_longlong)]
+                ("surrogate_rejects", C.c_longlong * 4), ("wait_timeouts", C.c_longlong),
+                ("surrogate_frozen", C.c_longlong), ("frozen_audited", C.c_longlong),
+                ("frozen_audit_max_dT", C.c_double), ("drain_timeouts", C.c_longlong)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
@@ -85,7 +88,7 @@ class Status(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int), ("flux_stage", C.c_int),
-                ("sur_fused", C.c_int)]
+                ("sur_fused", C.c_int), ("adapt_queue", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -150,11 +153,13 @@ def load_library(path: Optional[str] = None):
     L.eu3d_sur_predict.argtypes = h + [_fp, C.c_longlong, _fp]
     L.eu3d_sur_infer.argtypes = h + [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
     L.eu3d_set_surrogate.argtypes = h + [C.c_void_p, C.c_int]
+    L.eu3d_set_surrogate_gate.argtypes = h + [C.c_double, C.c_double, C.c_uint, C.c_int]
     L.eu3d_react_surrogate.argtypes = h
     L.eu3d_set_elements.argtypes = h + [_dp]
     L.eu3d_set_adaptive.argtypes = h + [C.c_double, C.c_double, C.c_int]
     L.eu3d_react_adaptive.argtypes = h
     L.eu3d_set_tuning.argtypes = h + [C.POINTER(Tuning)]
+    L.eu3d_set_wait_limit.argtypes = h + [C.c_longlong]
     L.eu3d_get_tuning.argtypes = h + [C.POINTER(Tuning)]
     L.eu3d_autotune.argtypes = h + [C.POINTER(StepDesc), C.c_int, C.POINTER(Tuning), _dp]
     L.eu3d_halo_bytes.argtypes = h + [C.POINTER(C.c_longlong)]
@@ -335,6 +340,15 @@ class DeviceFlowfield:
         _check(self.L.eu3d_set_surrogate(self.h, sur.s if sur is not None else None, audit_stride))
         self._sur = sur  # keeps the surrogate alive while attached
 
+    def set_surrogate_gate(self, t_frozen: float, y_max: float = 0.0, species=(), audit_stride: int = 0):
+        """Frozen-chemistry gate of REACT_SURROGATE steps: fluid cells below
+        t_frozen [K] whose mass fractions summed over `species` (names) are at
+        most y_max skip the network.  t_frozen = 0 turns it off."""
+        mask = 0
+        for n in species:
+            mask |= 1 << self.mech.species.index(n)
+        _check(self.L.eu3d_set_surrogate_gate(self.h, float(t_frozen), float(y_max), mask, int(audit_stride)))
+
     def react_surrogate(self):
         _check(self.L.eu3d_react_surrogate(self.h))
 
@@ -427,8 +441,11 @@ class DeviceFlowfield:
         _check(self.L.eu3d_get_tuning(self.h, C.byref(t)))
         return t.as_dict()
 
-    def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None, sur_fused=None):
+    def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None, sur_fused=None,
+                   adapt_queue=None):
         t = Tuning(**self.tuning())
+        if adapt_queue is not None:
+            t.adapt_queue = 1 if adapt_queue else 0
         if flux_kz is not None:
             t.flux_kz = flux_kz
         if chem_queue is not None:
@@ -450,6 +467,10 @@ class DeviceFlowfield:
         ms = C.c_double()
         _check(self.L.eu3d_autotune(self.h, C.byref(s), steps, C.byref(t), C.byref(ms)))
         return t.as_dict(), ms.value
+
+    def set_wait_limit(self, tries: int = 1 << 19):
+        """Bound of the TMA-fed flux kernel's copy waits (0: give up at once)."""
+        _check(self.L.eu3d_set_wait_limit(self.h, int(tries)))
 
     def status(self) -> dict:
         s = Status()

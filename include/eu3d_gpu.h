@@ -92,7 +92,10 @@ typedef struct {
     long long newton_capped;     /* decodes that used all 10 Newton iterations */
     long long substeps;          /* adaptive-trapezoid substeps taken */
     int nchem_max;               /* largest per-cell substep count since the last reset */
-    int substep_capped;          /* cells whose substep count hit the cap */
+    int substep_capped;          /* cells whose substep count hit the cap: the adaptive trapezoid's
+                                    TrapezoidPrediction count above its cap, or an adaptive-chemistry
+                                    substep lengthened by nmax (dt / nmax at least, the last allowed
+                                    substep takes the time left) */
     long long surrogate_cells;   /* cells advanced by the learned surrogate */
     long long surrogate_fallback;/* cells sent back to the integrator */
     double dt, time;             /* device copies of Flowfield::dt / ::time */
@@ -103,6 +106,11 @@ typedef struct {
                                        residual, failed decode */
     long long wait_timeouts;     /* kernels that gave up a bounded wait on an asynchronous copy
                                     (their results for that launch are incomplete) */
+    long long surrogate_frozen;  /* cells the frozen-chemistry gate kept out of the network */
+    long long frozen_audited;    /* of those, cells also run through the FP64 integrator */
+    double frozen_audit_max_dT;  /* largest |T_integrator - T| over them [K] */
+    long long drain_timeouts;    /* after a timed-out wait, the bounded wait for the copies still in
+                                    flight ran out as well: treat the device state as untrusted */
 } eu3d_status;
 
 const char *eu3d_last_error(void);
@@ -267,19 +275,34 @@ int eu3d_dlb_unpack(eu3d_handle *h, const double *dev_back);
    TMA, 1 staged into shared memory by loads, 0 read through L1.  flux_stage
    2 needs the driver's tensor-map encoder and falls back to 1 without it.
    sur_fused 1: the surrogate's network and its apply in one kernel; 0
-   (default, faster on B200): two kernels; the same decisions either way.  Changing them drops the recorded step graphs. */
+   (default, faster on B200): two kernels; the same decisions either way.
+   adapt_queue 1: the FP64 adaptive chemistry (EU3D_REACT_ADAPTIVE) lists the
+   fluid cells and integrates them on the persistent queue, one cell per lane
+   with refill; 0 (default): one thread per cell.  Changing them drops the
+   recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
     int queue_blocks;
     int flux_stage;
     int sur_fused;
+    int adapt_queue;
 } eu3d_tuning;
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t);
+/* Bound of the waits of the TMA-fed flux kernel for its plane copies (new), in
+   sleep-waits of about a microsecond each (default 524288, about half a
+   second; at most 2^24).  A wait that runs out makes the kernel count
+   eu3d_status.wait_timeouts, wait with the default bound for the copies it
+   has in flight and return without storing the rest of its residuals; 0
+   gives up at the first wait, which tests that path without a fault or a
+   hang.  The residuals of such a launch are incomplete.  Drops the recorded
+   step graphs. */
+int eu3d_set_wait_limit(eu3d_handle *h, long long tries);
 int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t);
 /* Autotuner: times `steps` steps of s for each candidate setting (flux_kz in
-   {4, 8, 16, 32}, FP32 flux staged or not; for the adaptive trapezoid also
-   the queue on/off and 2..4 blocks per SM) on the handle's current state,
+   {4, 8, 16, 32, 64}, the three FP32 flux kernels; for the adaptive
+   trapezoid also the queue on/off and 2..4 blocks per SM; for the FP64
+   adaptive chemistry adapt_queue on/off) on the handle's current state,
    restoring the state after
    each trial, and keeps the fastest.  best / best_ms may be NULL.  Needs
    temporary device memory for one copy of the state. */
@@ -321,10 +344,12 @@ int eu3d_reset_status(eu3d_handle *h);
    that must not call cudaMalloc/cudaFree because they synchronise the device.
    The caller passes FP64 device fields D, U, V, W, P, Gamma on the ghosted
    grid (index k*plane + j*pitch + i, x fastest) and caller-owned device
-   doubles time_inout and dt_out; the result follows CFLcondition
-   (src/Flowfield.cpp:242-272): dt = cfl * min over interior cells of
-   min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C) if use_z]), C = sqrt(Gamma P / D),
-   clipped so that time does not pass final_time, then time += dt.
+   doubles time_inout and dt_out.  The result: dt = cfl * the minimum over
+   every interior cell of min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C) if use_z]),
+   C = sqrt(Gamma P / D), shortened so that time + dt does not pass
+   final_time; then time += dt.  Every interior cell counts: the caller's
+   fields carry no wedge, so unlike eu3d_cfl on a handle with eu3d_set_wedge,
+   solid cells are not left out.
    Scratch: a fixed 1024-double device array inside the library (kept by every
    GPU that loads it until exit); nblocks (reduction blocks, 0 = 592) above
    1024 is rejected with EU3D_ERR_ARG.  The first call on a device looks up
@@ -426,6 +451,18 @@ int eu3d_sur_infer(eu3d_surrogate *s, const float *X_dev, long long n, float *ou
    audit_stride-th accepted cell (0: none) also runs the FP64 integrator,
    which keeps its result and records the surrogate's temperature error. */
 int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride);
+/* Frozen-chemistry gate for EU3D_REACT_SURROGATE steps (new): a fluid cell
+   colder than t_frozen [K] whose mass fractions summed over the species in
+   species_mask (bit s = species s; 0: no composition test) are at most y_max
+   keeps the state of its flux update and decode -- over one flow step its
+   chemistry is below what the FP64 integrator resolves -- and only the other
+   cells go through the network and its apply.  Every audit_stride-th gated
+   cell (0: none) is integrated by the FP64 fallback as well, which keeps its
+   result and records the largest temperature change the gate ignored
+   (eu3d_status.frozen_audit_max_dT).  t_frozen = 0 (the default) turns the
+   gate off: every fluid cell takes the network.  With the gate on, sur_fused
+   is ignored. */
+int eu3d_set_surrogate_gate(eu3d_handle *h, double t_frozen, double y_max, unsigned species_mask, int audit_stride);
 /* Learned chemistry step of h after the flux residual is in RHS: network
    increment for the previous decode's state, element projection, envelope /
    negativity / energy-residual checks, EE update + FP64 decode; rejected

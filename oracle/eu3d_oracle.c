@@ -825,8 +825,9 @@ void orc_boundary(orc_field *f, const orc_mech *m, int kind, const double *wedge
     if (wedge) wedge_fill(f, m, wedge);
 }
 
-/* Flowfield::CFLcondition, src/Flowfield.cpp:242-272 (single rank) */
-void orc_cfl(orc_field *f, double cfl, double final_time)
+/* Flowfield::CFLcondition, src/Flowfield.cpp:242-272 (single rank); with a
+   wedge (new) its solid cells are left out, as the device reduction does. */
+static void cfl_scan(orc_field *f, double cfl, double final_time, const double *wedge)
 {
     const int bc = f->bc;
     double dx = f->xnode[1] - f->xnode[0];
@@ -837,6 +838,7 @@ void orc_cfl(orc_field *f, double cfl, double final_time)
         for (int j = bc; j < f->nj + bc; j++)
             for (int k = bc; k < f->nk + bc; k++) {
                 size_t c = ID3(f, i, j, k);
+                if (wedge && orc_wedge_solid(wedge, f->xnode[i], f->ynode[j])) continue;
                 double a = dx / (fabs(f->U[c]) + f->C[c]), b = dy / (fabs(f->V[c]) + f->C[c]);
                 temp = (b < a) ? b : a;
                 if (!(f->quirks & EU3D_Q_CFL_NO_Z)) {
@@ -850,11 +852,13 @@ void orc_cfl(orc_field *f, double cfl, double final_time)
     f->time += f->dt;
 }
 
+void orc_cfl(orc_field *f, double cfl, double final_time) { cfl_scan(f, cfl, final_time, NULL); }
+
 void orc_step(orc_field *f, const orc_mech *m, int react, int type, int timeadv, int diff, double cfl,
               double final_time, int bc_kind, const double *wedge)
 {
     const int NS = f->NS, bc = f->bc;
-    if (cfl != 0) orc_cfl(f, cfl, final_time);
+    if (cfl != 0) cfl_scan(f, cfl, final_time, wedge);
     orc_boundary(f, m, bc_kind, wedge);
     if (timeadv == EU3D_ADV_SSPRK2 || timeadv == EU3D_ADV_SSPRK3) {
         /* SSP Runge-Kutta for the advection (new), followed by the chemistry

@@ -71,11 +71,31 @@ def interior(a, bc=2):
     return a[bc:-bc, bc:-bc, bc:-bc]
 
 
-def rel_err(a, b):
-    """max |a - b| / max |b| over one field (the field-normalised error)."""
+def field_err(a, b):
+    """max |a - b| / max |b| over a whole array (the field-normalised error)."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     scale = np.max(np.abs(b))
     if scale == 0:
         return float(np.max(np.abs(a)))
     return float(np.max(np.abs(a - b)) / scale)
+
+
+def rel_err(a, b, mask=None):
+    """Per-variable relative error: each variable is normalised by its own
+    largest magnitude, and the worst variable is returned.  A 3D field
+    (ni, nj, nk) is one variable; the last axis of a per-cell vector field
+    (species mass fractions, the 13 conserved variables) indexes its
+    variables, so a radical at Y ~ 1e-6 is held to the same relative bar as
+    N2.  mask (ni, nj, nk), optional: only these cells count (the fluid cells
+    of an immersed wedge)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+        vec = a.ndim == 2
+    else:
+        vec = a.ndim == 4
+    if not vec:
+        return field_err(a, b)
+    return max(field_err(a[..., v], b[..., v]) for v in range(a.shape[-1]))

@@ -1,17 +1,22 @@
 """GPU path (libeu3d_gpu.so through the C ABI) against the oracle.
 
-Tolerance: the FP64 path must agree with the oracle to a field-normalised
-error (max |gpu - oracle| / max |oracle| per field) of 1e-10 on every state
-field after N steps -- the bar the reference comparison sets for the
+Tolerance: the FP64 path must agree with the oracle to a per-variable
+relative error (max |gpu - oracle| / max |oracle| of each variable: each
+species, each conserved variable, each primitive field) of 1e-10 on every
+state field after N steps -- the bar the reference comparison sets for the
 all-FP64 path.  Single-function checks use 1e-12.  The FP32-flux path is held
-to the stated mixed-precision bound (5e-5 after 3 steps).
+to the stated mixed-precision bound (5e-5 after 3 steps, field-normalised).
+Beside the small grids with odd extents, two workloads run as the benchmark
+configurations define them: the oblique detonation (ODM inflow, 25 degree
+wedge, SSP-RK2, IMEX, CFL 0.5) at the benchmark's cell size for 50 steps, and
+the 1D ZND detonation at its full 4000 x 2 x 2 cells for 200 steps.
 """
 import os
 
 import numpy as np
 import pytest
 
-from _cases import QUIRKS_FIXED, QUIRKS_REF, interior, make_oracle, rel_err, small_grid
+from _cases import QUIRKS_FIXED, QUIRKS_REF, field_err, interior, make_oracle, rel_err, small_grid
 from eu3d_b200 import gpu
 from eu3d_b200.readers import make_grid
 
@@ -154,7 +159,10 @@ GRIDS = {
 # per scheme and policy: (state window, cfl, dt, steps).  The trapezoid
 # schemes lose finiteness within a few steps on hot non-equilibrium states
 # (the shipped field form and the "DNN" path also corrupt momentum/energy),
-# so their runs are short or mild; IMEX runs four CFL-limited steps.
+# so their runs are short or mild; IMEX runs four CFL-limited steps.  The
+# fixed-policy adaptive trapezoid runs at dt = 5e-9 s: at 1e-8 s its oracle
+# run on the 10 x 6 x 4 grid goes non-finite in the second step (substep
+# counts up to 148), at 5e-9 s every grid stays finite with counts up to 49.
 MILD = dict(tlo=800.0, thi=1200.0, radicals=1e-6)
 SUBSTEP = dict(tlo=1500.0, thi=2200.0, radicals=1e-5)
 STEP_CASES = {
@@ -166,7 +174,7 @@ STEP_CASES = {
     ("imex_rk3", QUIRKS_REF): (COOL, 0.3, 0.0, 4),
     ("trap0", QUIRKS_FIXED): (MILD, 0.0, 1e-8, 4),
     ("trap0", QUIRKS_REF): (COOL, 0.0, 1e-8, 1),
-    ("trap1", QUIRKS_FIXED): (SUBSTEP, 0.0, 1e-8, 2),
+    ("trap1", QUIRKS_FIXED): (SUBSTEP, 0.0, 5e-9, 2),
     ("trap1", QUIRKS_REF): (COOL, 0.0, 1e-8, 4),
     ("nochem", QUIRKS_FIXED): (HOT, 0.3, 0.0, 4),
     ("nochem", QUIRKS_REF): (COOL, 0.3, 0.0, 1),
@@ -191,8 +199,7 @@ def test_steps_parity(mech, quirks, scheme, gname):
         o.step(react, typ, timeadv, 1, cfl, 1.0, gpu.BC_RSBI)
         d.step(react=react, type_=typ, timeadv=timeadv, diff=1, bc_kind=gpu.BC_RSBI, cfl=cfl, final_time=1.0)
     d.synchronize()
-    if not np.isfinite(interior(o.view("T"))).all():
-        pytest.skip("oracle run is non-finite for this policy/case")
+    assert np.isfinite(interior(o.view("T"))).all(), "the oracle run left the finite range"
     e, errs = worst(d, o)
     assert e < TOL_STEP, errs
     s = d.status()
@@ -200,6 +207,93 @@ def test_steps_parity(mech, quirks, scheme, gname):
     assert abs(s["time"] - o.time) <= 1e-12 * max(o.time, 1e-300)
     if scheme == "trap1":
         assert np.array_equal(interior(d.download("Nchem")), interior(o.view("Nchem")).astype(np.float64))
+
+
+def _odw_pair(mech, ni, nj, nk):
+    """The benchmark's oblique detonation at its cell size (dx = 0.2 m / 511)
+    on an ni x nj x nk grid: uniform Mach 7 free stream, seeded ODM inflow
+    planes, 25 degree wedge from x = 0.1 L.  The state is completed on the
+    oracle and uploaded, so both sides start from the same bits."""
+    from eu3d_b200.cases import odw_case
+    from pyoracle import Oracle
+    case = odw_case(mech, ni, nj, nk, L=0.2 * (ni - 1) / 511.0)
+    o = Oracle(mech, case.grid, QUIRKS_FIXED)
+    for n, v in (("P", case.P), ("T", case.T), ("U", case.U), ("V", 0.0), ("W", 0.0)):
+        o.view(n)[...] = v
+    o.view("Yi")[...] = case.Y
+    o.prims_from_state()
+    f = case.inflow
+    for n, k in (("Uint", "U"), ("Vint", "V"), ("Wint", "W"), ("Pint", "P"), ("Dint", "D"), ("Tint", "T"),
+                 ("Hint", "H"), ("Eint", "E"), ("Gint", "G"), ("Yint", "Y")):
+        o.view(n)[...] = f[k]
+    d = to_gpu(o, case.grid, QUIRKS_FIXED)
+    d.set_inflow(*[o.view(n) for n in ("Uint", "Vint", "Wint", "Pint", "Dint", "Tint", "Hint", "Eint", "Gint",
+                                       "Yint")])
+    d.set_wedge(*case.wedge)
+    g = case.grid
+    x = g.xnode[2:-2][:, None, None]
+    y = g.ynode[2:-2][None, :, None]
+    w = case.wedge
+    fluid = np.broadcast_to(~((x > w[0]) & ((y - w[1]) < (x - w[0]) * w[2])), (g.ni, g.nj, g.nk))
+    return o, d, case, fluid
+
+
+def test_odw_benchmark_setup_steps_parity(mech):
+    """The benchmark's step (ODM ghost fill, wedge band, MUSCL_2/AUSM, SSP-RK2,
+    IMEX, CFL 0.5, all FP64) on a 96 x 48 x 8 grid at the benchmark's cell
+    size, 50 steps through eu3d_step against the oracle: every state field
+    within 1e-10 per variable on the fluid cells (the wedge's solid cells are
+    not part of the flow; the device leaves them out of the CFL scan and the
+    updates), dt and time alike."""
+    o, d, case, fluid = _odw_pair(mech, 96, 48, 8)
+    for _ in range(50):
+        o.step(gpu.REACT_IMEX, 0, gpu.ADV_SSPRK2, gpu.DIFF_MUSCL2, 0.5, 1.0, gpu.BC_ODM, case.wedge)
+        d.step(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_ODM, cfl=0.5,
+               final_time=1.0)
+    d.synchronize()
+    To = interior(o.view("T"))
+    assert np.isfinite(To[fluid]).all()
+    assert To[fluid].max() > 1000.0  # the wedge shock has formed
+    errs = {n: rel_err(interior(d.download(n)), interior(o.view(n)), mask=fluid) for n in STATE}
+    assert max(errs.values()) < TOL_STEP, errs
+    s = d.status()
+    assert s["nonfinite_cells"] == 0
+    assert abs(s["time"] - o.time) <= 1e-12 * o.time
+    assert abs(s["dt"] - o.dt) <= 1e-12 * o.dt
+    d.close()
+
+
+@pytest.mark.parametrize("react,typ,steps", [(gpu.REACT_IMEX, 0, 200), (gpu.REACT_TRAPEZOID, 1, 10)],
+                         ids=["imex", "trap1"])
+def test_znd_full_grid_steps_parity(mech, react, typ, steps):
+    """The 1D ZND detonation at its full size (4000 x 2 x 2 cells on 0.1 m,
+    3000 K / 30 atm driver, transmissive ends), SSP-RK2, CFL 0.3, all FP64,
+    against the oracle: IMEX for 200 steps and the adaptive trapezoid for 10
+    (in the fixed policy its oracle run goes non-finite at the 12th step
+    through the ignition behind the driver's shock, so the comparison stops
+    before that).  Per-variable 1e-10 on every state field."""
+    from eu3d_b200.cases import znd_case
+    from pyoracle import Oracle
+    g, st = znd_case(mech)
+    o = Oracle(mech, g, QUIRKS_FIXED)
+    for n in ("U", "V", "W", "P", "T", "Yi"):
+        o.view(n)[...] = st[n]
+    o.prims_from_state()
+    d = to_gpu(o, g, QUIRKS_FIXED)
+    for _ in range(steps):
+        o.step(react, typ, gpu.ADV_SSPRK2, gpu.DIFF_MUSCL2, 0.3, 1.0, gpu.BC_TRANSMISSIVE)
+        d.step(react=react, type_=typ, timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_TRANSMISSIVE,
+               cfl=0.3, final_time=1.0)
+    d.synchronize()
+    assert np.isfinite(interior(o.view("T"))).all()
+    e, errs = worst(d, o)
+    assert e < TOL_STEP, errs
+    s = d.status()
+    assert s["nonfinite_cells"] == 0
+    assert abs(s["time"] - o.time) <= 1e-12 * o.time
+    if typ == 1:
+        assert np.array_equal(interior(d.download("Nchem")), interior(o.view("Nchem")).astype(np.float64))
+    d.close()
 
 
 @pytest.mark.parametrize("case_idx", range(8))
@@ -234,8 +328,8 @@ def test_fp32_flux_error_bound(mech, diff):
     for _ in range(3):
         o.step(1, 0, 0, diff, 0.3, 1.0, gpu.BC_RSBI)
         d.step(react=1, diff=diff, bc_kind=gpu.BC_RSBI, cfl=0.3)
-    e, errs = worst(d, o, names=["CS", "T", "P", "D"])
-    assert e < 5e-5, errs
+    errs = {n: field_err(interior(d.download(n)), interior(o.view(n))) for n in ("CS", "T", "P", "D")}
+    assert max(errs.values()) < 5e-5, errs
 
 
 @pytest.mark.parametrize("gname", list(GRIDS))

@@ -30,7 +30,10 @@ def _device_fields(d, torch):
     return out
 
 
-def test_noalloc_cfl_matches_handle_cfl_twice(mech):
+@pytest.mark.parametrize("nblocks", [0, 1, 1024], ids=["default", "one-block", "full-scratch"])
+def test_noalloc_cfl_matches_handle_cfl_twice(mech, nblocks):
+    """nblocks 0 (592 blocks), 1 (one block walks the whole grid) and 1024
+    (every entry of the scratch array filled)."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -54,7 +57,7 @@ def test_noalloc_cfl_matches_handle_cfl_twice(mech):
         t_ref = d.status()["time"]
         rc = L.eu3d_cfl_noalloc(*[f[n].data_ptr() for n in ("D", "U", "V", "W", "P", "Gamma")],
                                 g.ni, g.nj, g.nk, g.bc, NI, NI * NJ, dx, dy, dz, 1, cfl, final,
-                                t_dev.data_ptr(), dt_dev.data_ptr(), 0, stream)
+                                t_dev.data_ptr(), dt_dev.data_ptr(), nblocks, stream)
         assert rc == 0, L.eu3d_last_error()
         torch.cuda.synchronize()
         dt_new, t_new = float(dt_dev.item()), float(t_dev.item())
