@@ -67,7 +67,19 @@ def parse():
                     help="also compare on the benchmark's full grid (about 2.5 more minutes)")
     ap.add_argument("--develop", type=int, default=1500, help="2D steps that develop the timed state")
     ap.add_argument("--model", default=os.path.join(ROOT, "eu3d_b200", "data", "sur_h2_ja919.npz"))
+    ap.add_argument("--config", choices=list(CONFIGS), default="odw3d",
+                    help="odw3d: the headline (3D ODW 512x256x256); znd, odw2d, rsbi, surrogate: the other "
+                         "benchmark configurations, one GPU")
     return ap.parse_args()
+
+
+CONFIGS = {
+    "odw3d": "3D oblique detonation 512x256x256, surrogate chemistry vs the FP64 integrators",
+    "znd": "1D ZND detonation 4000x2x2, FP64",
+    "odw2d": "2D oblique detonation 1024x512, FP64 vs FP32 flux; adaptive chemistry queue vs one thread per cell",
+    "rsbi": "3D reactive shock-bubble interaction 256^3, FP32 flux vs FP64",
+    "surrogate": "chemistry surrogate: FP64 labels, training and inference on 2^22 states",
+}
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -328,6 +340,48 @@ def fluid_cells(case, i0=0, n_loc=None):
     return int((~solid).sum()) * g.nk
 
 
+# FP64 operations of the reference's per-cell chemistry, counted by running
+# its arithmetic on an operation-counting type (oracle/opcount.py,
+# reference_counts: 64 states of the surrogate's standalone set, the decode
+# at 3 Newton iterations): add, sub, mul, div 1 FLOP each; exp and log 20,
+# a non-integer pow 40, sqrt 1 FLOP-equivalents in the "equiv" figures.
+# tests/test_opcount.py recomputes them.
+CHEM_FLOP = {"imex_cell": 8277.0, "imex_cell_equiv": 10159.0,
+             "adaptive_substep": 7923.2, "adaptive_substep_equiv": 9625.2}
+# nominal FP64 peak of one B200 (no measured FP64 figure exists on this pool)
+FP64_PEAK_TFLOPS = 37.0
+
+
+def chem_roofline(profs, stats, fluid, steps_run, K):
+    """FP64 rooflines of the chemistry kernels: IMEX (CHEM_FLOP per fluid cell
+    a launch) and the adaptive integrator (CHEM_FLOP per substep taken)."""
+    out = {}
+    if "cell_imex" in profs.get("imex", {}):
+        ms, n = profs["imex"]["cell_imex"]
+        for key in ("imex_cell", "imex_cell_equiv"):
+            ach = CHEM_FLOP[key] * fluid / (ms / n * 1e-3) / 1e12
+            out.setdefault("cell_imex", {})[key.replace("imex_cell", "flop")] = {
+                "achieved": ach, "unit": "TFLOP/s", "peak": FP64_PEAK_TFLOPS, "frac": ach / FP64_PEAK_TFLOPS}
+        out["cell_imex"]["flop_per_cell"] = CHEM_FLOP["imex_cell"]
+        out["cell_imex"]["avg_ms"] = ms / n
+    ad = profs.get("adaptive", {})
+    key_k = "cell_adapt" if "cell_adapt" in ad else ("adapt_queue" if "adapt_queue" in ad else None)
+    if key_k and stats.get("adaptive"):
+        ms, n = ad[key_k]
+        sub = stats["adaptive"]["substeps"] / max(steps_run, 1)  # per launch
+        for key in ("adaptive_substep", "adaptive_substep_equiv"):
+            ach = CHEM_FLOP[key] * sub / (ms / n * 1e-3) / 1e12
+            out.setdefault(key_k, {})[key.replace("adaptive_substep", "flop")] = {
+                "achieved": ach, "unit": "TFLOP/s", "peak": FP64_PEAK_TFLOPS, "frac": ach / FP64_PEAK_TFLOPS}
+        out[key_k]["substeps_per_launch"] = sub
+        out[key_k]["avg_ms"] = ms / n
+    out["note"] = ("algorithmic FP64 work of the reference's arithmetic (oracle/opcount.py) / CUDA-event launch time, "
+                   "against a nominal 37 TFLOP/s FP64 peak; the device code evaluates the same chemistry with fewer "
+                   "operations (powers by multiplication, mixture polynomials summed once, zero stoichiometric "
+                   "factors dropped), so this is work done per second, not pipe occupancy")
+    return out
+
+
 # kernels of the step that make up its chemistry (the rest: ghost fills, CFL,
 # flux sweeps and stage updates)
 CHEM_KERNELS = {"cell_imex", "cell_adapt", "sur_gate", "sur_mlp", "sur_apply", "sur_fallback", "sur_mlp_apply"}
@@ -393,6 +447,13 @@ def run_ours(a, rank, world, local):
         return lambda: run.step(spec)
 
     W = max(a.warmup, 3)
+    tuned = None
+    if world == 1:
+        # the project's autotuner picks the flux tile depth and kernel on this
+        # state (restored after every trial), outside the timed region
+        reset()
+        best, best_ms = dev.autotune(steps=2, **dict(base, react=gpu.REACT_SURROGATE))
+        tuned = {"setting": best, "ms_per_step": best_ms}
     timing, profs, statuses, clocks = {}, {}, {}, None
     for name, react in forms.items():
         reset()
@@ -448,7 +509,8 @@ def run_ours(a, rank, world, local):
                    "parallelism": (f"{world} x slabs of {n_loc} cells (NCCL halo send/recv, all-reduce MIN of dt)"
                                    if world > 1 else "1 GPU"),
                    "l2": "state ~12 GB per GPU >> 126 MB L2 (no flush needed)",
-                   "graph": "one CUDA graph per step" if world == 1 else "per-op launches (halo exchanges between)"},
+                   "graph": "one CUDA graph per step" if world == 1 else "per-op launches (halo exchanges between)",
+                   "autotuned": tuned},
         "integrator": {"imex_value": integ["imex"], "adaptive_value": integ["adaptive"],
                        "ratio_vs_imex": value / integ["imex"], "ratio_vs_adaptive": value / integ["adaptive"],
                        "ms_per_step": {k: timing[k] / a.steps for k in timing},
@@ -469,6 +531,7 @@ def run_ours(a, rank, world, local):
                     for f in profs},
         "roofline": rf,
         "roofline_other_kernels": rf_more,
+        "roofline_chemistry": chem_roofline(profs, statuses, fluid, a.steps + W, a.steps),
         "status": {k: st[k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")},
     }
     if clocks:
@@ -486,6 +549,10 @@ def run_ours(a, rank, world, local):
     if not a.no_e2e:
         reset()
         out["e2e"] = run_e2e(dev, stepper(dict(base, react=gpu.REACT_SURROGATE)), a.steps, cells, torch, world, dist)
+        if world == 1:
+            reset()
+            out["e2e_state_through_host"] = run_e2e_host_state(dev, dict(base, react=gpu.REACT_SURROGATE),
+                                                               max(a.steps // 2, 2), cells, torch)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     dev.close()
@@ -531,6 +598,36 @@ def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
                         "so the host copies are amortised over the K steps and the value depends on K"}
 
 
+def run_e2e_host_state(dev, step, K, cells, torch):
+    """The host-array calling convention of the reference (its state lives in
+    host arrays between calls): every step uploads CS, T, E from pinned host
+    memory, decodes, steps and downloads CS and T.  Reported beside e2e."""
+    one = step if callable(step) else (lambda: dev.step(**step))
+    shapes = {n: dev.shape(n) for n in ("CS", "T", "E")}
+    host = {n: torch.empty(s, dtype=torch.float64, pin_memory=True).numpy() for n, s in shapes.items()}
+    for n in host:
+        dev.download(n, host[n])
+    stream = torch.cuda.ExternalStream(dev.stream)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(K):
+        for n in ("CS", "T", "E"):
+            dev.upload(n, host[n])
+        dev.update_after_cs()
+        one()
+        dev.download("CS", host["CS"])
+        dev.download("T", host["T"])
+    ev1.record(stream)
+    dev.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    h2d = sum(host[n].nbytes for n in ("CS", "T", "E"))
+    d2h = host["CS"].nbytes + host["T"].nbytes
+    return {"value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms": ms,
+            "protocol": "every step: upload CS,T,E (pinned), decode, one eu3d_step, download CS,T"}
+
+
 def workload_name(ni, nj, nk):
     return (f"3D oblique detonation {ni}x{nj}x{nk} (ODW, Mach 7 H2-air 0.1 atm 300 K, 25 deg wedge, "
             f"1 % seeded inflow density perturbation)")
@@ -558,6 +655,353 @@ def run_reference(a, rank, world):
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# ------------------------------------------------- the other configurations
+def _line(metric, value, unit, K, W, ms, dtype, config, **extra):
+    out = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": K, "warmup": W,
+           "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+           "data": "synthetic", "config": config}
+    out.update(extra)
+    return out
+
+
+def _case_run(dev, forms, K, W, torch, cells, units, pb, value_form, clocks_form=None):
+    """Times each form (eu3d_step keyword sets) K steps after W warm-up from
+    the state `reset` puts back; per-kernel profile, roofline of the value
+    form's top kernel, clocks during the value form's timed steps."""
+    hbm, tfl, src = peaks()
+    timing, profs, stats, clocks = {}, {}, {}, None
+    for name, (reset, step) in forms.items():
+        reset()
+        ms, clk = timed_steps(dev, step, K, W, torch, 1, None, clocks=(name == (clocks_form or value_form)))
+        if clk:
+            clocks = clk
+        timing[name] = ms
+        stats[name] = dev.status()
+        reset()
+        profs[name] = profiled(dev, step, K)
+    prof = profs[value_form]
+    rf = roofline(prof, units, hbm, tfl, src, pb=pb)
+    rates = {k: cells * K / (v * 1e-3) / 1e6 for k, v in timing.items()}
+    return timing, profs, stats, clocks, rf, rates
+
+
+def _kernel_table(profs):
+    return {f: {k: {"ms_avg": v[0] / v[1], "share": v[0] / sum(x[0] for x in pr.values()), "launches": v[1]}
+                for k, v in sorted(pr.items(), key=lambda kv: -kv[1][0])} for f, pr in profs.items()}
+
+
+def _port_baseline(make, step, steps, label):
+    """The oracle (the C restatement of the reference's path) on one host
+    core: `make()` builds it, `step(o)` advances it one step."""
+    o, cells = make()
+    step(o)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step(o)
+    dt = time.perf_counter() - t0
+    return {"value": cells * steps / dt / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{label}: {steps} steps after one warm-up step on one host core", "seconds": dt}
+
+
+def run_znd(a):
+    """C1: the 1D ZND detonation at its full size, FP64 throughout, SSP-RK2,
+    CFL 0.3 (at 0.5 the reference's own arithmetic goes non-finite in the
+    first step at the driver interface).  Value: the reference's one-step
+    IMEX; beside it the FP64 adaptive chemistry.  The fixed-policy adaptive
+    trapezoid (the configuration's chemistry) goes non-finite at its 12th step
+    in the reference's arithmetic, so it is not timed."""
+    import torch
+    from eu3d_b200 import gpu
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.cases import upload_primitive_state, znd_case
+    from eu3d_b200.readers import load_h2_ja919
+    mech = load_h2_ja919()
+    g, st = znd_case(mech)
+    dev = gpu.DeviceFlowfield(mech, g, quirks=gpu.QUIRKS_FIXED, flux_bits=64)
+    dev.set_elements(S.atoms_matrix(mech))
+
+    def reset():
+        upload_primitive_state(dev, st)
+        dev.set_time(0.0)
+        dev.reset_status()
+
+    base = dict(timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_TRANSMISSIVE, cfl=0.3, final_time=1.0)
+    forms = {"imex": (reset, dict(base, react=gpu.REACT_IMEX)), "adaptive": (reset, dict(base, react=gpu.REACT_ADAPTIVE))}
+    K, W = max(a.steps, 500), max(a.warmup, 20)
+    cells = g.ni * g.nj * g.nk
+    units = {k: cells for k in kernel_work(8)}
+    timing, profs, stats, clocks, rf, rates = _case_run(dev, forms, K, W, torch, cells, units, 8, "imex")
+    reset()
+    e2e = run_e2e(dev, forms["imex"][1], K, cells, torch)
+    dev.close()
+
+    def make():
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from pyoracle import Oracle
+        o = Oracle(mech, g, gpu.QUIRKS_FIXED)
+        for n in ("U", "V", "W", "P", "T", "Yi"):
+            o.view(n)[...] = st[n]
+        o.prims_from_state()
+        return o, cells
+
+    cb = _port_baseline(make, lambda o: o.step(gpu.REACT_IMEX, 0, gpu.ADV_SSPRK2, gpu.DIFF_MUSCL2, 0.3, 1.0,
+                                                gpu.BC_TRANSMISSIVE), 20,
+                        "the oracle on the whole 4000x2x2 case, SSP-RK2 + IMEX, CFL 0.3")
+    return _line("Mcell-steps/s, 1D ZND detonation 4000x2x2, FP64", rates["imex"], UNIT, K, W, timing["imex"], "f64",
+                 {"workload": "1D ZND detonation 4000x2x2 cells on 0.1 m: stoichiometric H2-air 300 K 1 atm, "
+                              "H2O/N2 driver 3000 K 30 atm for x < 5 mm, transmissive ends",
+                  "cells": cells, "chemistry": "FP64 IMEX (the reference's); adaptive FP64 beside",
+                  "flux": "MUSCL_2/minmod + AUSM, FP64", "time": "SSP-RK2, CFL 0.3", "graph": "one CUDA graph per step",
+                  "l2": "the whole state fits L2: steps are latency- and launch-bound"},
+                 rates={k: v for k, v in rates.items()}, ms_per_step_forms={k: v / K for k, v in timing.items()},
+                 kernels=_kernel_table(profs), roofline=rf, clocks=clocks, e2e=e2e, cpu_baseline=cb,
+                 gpu_launches=int(sum(v[1] for v in profs["imex"].values())),
+                 status={k: stats["imex"][k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")})
+
+
+def run_odw2d(a):
+    """C2: the 2D oblique detonation 1024x512 from a developed state (1000
+    SSP-RK2 steps of FP64 adaptive chemistry): IMEX with FP64 and with FP32
+    reconstruction/AUSM (FP64 state); the FP64 adaptive chemistry with one
+    thread per cell and on the persistent queue (one cell per lane, refill).
+    The reference's IMEX has the same work in every cell, so the queue is
+    measured on the integrator whose substep counts vary from cell to cell."""
+    import torch
+    from eu3d_b200 import gpu
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.cases import extrude_state, odw_case, setup_odw
+    from eu3d_b200.readers import load_h2_ja919
+    mech = load_h2_ja919()
+    ni, nj = 1024, 512
+    case = odw_case(mech, ni, nj, 2)
+    src = gpu.DeviceFlowfield(mech, case.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=32)
+    setup_odw(src, case)
+    src.set_elements(S.atoms_matrix(mech))
+    src.run(1000, react=gpu.REACT_ADAPTIVE, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
+    src.synchronize()
+    cells = ni * nj * 2
+    fluid = fluid_cells(case)
+    out_forms, profs_all, timing_all, rates_all = {}, {}, {}, {}
+    K, W = max(a.steps, 50), max(a.warmup, 5)
+    base = dict(timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_ODM, cfl=CFL, final_time=1.0)
+    results = {}
+    for bits in (64, 32):
+        dev = gpu.DeviceFlowfield(mech, case.grid, quirks=gpu.QUIRKS_FIXED, flux_bits=bits)
+        setup_odw(dev, case)
+        dev.set_elements(S.atoms_matrix(mech))
+
+        def reset(q=None, dev=dev):
+            extrude_state(src, dev)
+            dev.set_time(0.0)
+            dev.reset_status()
+            if q is not None:
+                dev.set_tuning(adapt_queue=q)
+
+        forms = {f"imex_fp{bits}": (lambda dev=dev: reset(0, dev), dict(base, react=gpu.REACT_IMEX))}
+        if bits == 32:
+            forms["adaptive_thread_per_cell"] = (lambda dev=dev: reset(0, dev), dict(base, react=gpu.REACT_ADAPTIVE))
+            forms["adaptive_queue"] = (lambda dev=dev: reset(1, dev), dict(base, react=gpu.REACT_ADAPTIVE))
+        units = {k: fluid for k in kernel_work(bits // 8)}
+        timing, profs, stats, clocks, rf, rates = _case_run(dev, forms, K, W, torch, cells, units, bits // 8,
+                                                            f"imex_fp{bits}")
+        results[bits] = (rf, clocks, stats)
+        timing_all.update(timing)
+        profs_all.update(profs)
+        rates_all.update(rates)
+        if bits == 32:
+            reset(0)
+            e2e = run_e2e(dev, forms["imex_fp32"][1], K, cells, torch)
+        dev.close()
+    src.close()
+    rf, clocks, stats = results[32]
+    chem = {f: sum(v[0] for k, v in profs_all[f].items() if k in CHEM_KERNELS | {"adapt_list", "adapt_queue"}) / K
+            for f in ("adaptive_thread_per_cell", "adaptive_queue")}
+    cb = cpu_baseline(slab=(64, 32, 2))
+    return _line("Mcell-steps/s, 2D ODW 1024x512, FP32 flux / FP64 state, IMEX", rates_all["imex_fp32"], UNIT, K, W,
+                 timing_all["imex_fp32"], "f32 (reconstruction, AUSM, residual) + f64 (state, decode, chemistry)",
+                 {"workload": "2D oblique detonation 1024x512x2 (L = 0.2 m, Mach 7 H2-air 0.1 atm 300 K, 25 deg "
+                              "wedge), developed by 1000 steps of FP64 adaptive chemistry",
+                  "cells": cells, "fluid_cells": fluid, "time": f"SSP-RK2, CFL {CFL}", "graph": "one CUDA graph per step",
+                  "l2": "state ~0.4 GB > 126 MB L2"},
+                 rates=rates_all, ms_per_step_forms={k: v / K for k, v in timing_all.items()},
+                 fp64_vs_fp32_speedup=rates_all["imex_fp32"] / rates_all["imex_fp64"],
+                 adaptive_chemistry_ms_per_step={"thread_per_cell": chem["adaptive_thread_per_cell"],
+                                                 "persistent_queue": chem["adaptive_queue"]},
+                 kernels=_kernel_table(profs_all), roofline=rf, clocks=clocks, e2e=e2e, cpu_baseline=cb,
+                 gpu_launches=int(sum(v[1] for v in profs_all["imex_fp32"].values())),
+                 status={k: stats["imex_fp32"][k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")})
+
+
+def run_rsbi(a):
+    """C3: the 3D reactive shock-bubble interaction at 256^3, SSP-RK2, IMEX,
+    RSBI (mirror) ghost fill, CFL 0.5, one CUDA graph per step; FP32
+    reconstruction/AUSM/residual (value) and FP64 beside, and the FP32 run's
+    errors against the FP64 one after `--accuracy-steps`/20 steps from the same
+    initial state (pointwise rho, p, T; Y_k against each species' scale)."""
+    import torch
+    from eu3d_b200 import gpu
+    from eu3d_b200.cases import rsbi_case, upload_primitive_state
+    from eu3d_b200.readers import load_h2_ja919
+    from eu3d_b200.validate import field_errors
+    mech = load_h2_ja919()
+    t0 = time.time()
+    case = rsbi_case(mech, n=256)
+    setup_s = time.time() - t0
+    g = case.grid
+    cells = g.ni * g.nj * g.nk
+    base = dict(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, diff=gpu.DIFF_MUSCL2, bc_kind=gpu.BC_RSBI, cfl=CFL,
+                final_time=1.0)
+    K, W = max(a.steps, 10), max(a.warmup, 3)
+    nerr = max(a.accuracy_steps // 20, 10)
+    rates, timing_all, profs_all, fields = {}, {}, {}, {}
+    rf = clocks = e2e = stats32 = None
+    for bits in (64, 32):
+        dev = gpu.DeviceFlowfield(mech, g, quirks=gpu.QUIRKS_FIXED, flux_bits=bits)
+
+        def reset(dev=dev):
+            upload_primitive_state(dev, case.state)
+            dev.set_time(0.0)
+            dev.reset_status()
+
+        units = {k: cells for k in kernel_work(bits // 8)}
+        timing, profs, stats, clk, r, rt = _case_run(dev, {f"fp{bits}": (reset, base)}, K, W, torch, cells, units,
+                                                     bits // 8, f"fp{bits}")
+        rates.update(rt)
+        timing_all.update(timing)
+        profs_all.update(profs)
+        reset()
+        dev.run(nerr, **base)
+        dev.synchronize()
+        b = g.bc
+        fields[bits] = {n: dev.download(n)[b:-b, b:-b, b:-b].copy() for n in ("T", "P", "D", "Yi")}
+        if bits == 32:
+            rf, clocks, stats32 = r, clk, stats["fp32"]
+            reset()
+            e2e = run_e2e(dev, base, K, cells, torch)
+        dev.close()
+    err = field_errors(fields[64], fields[32], np.ones((g.ni, g.nj, g.nk), bool), mech.species)
+    cb = cpu_baseline(slab=(32, 32, 8))
+    return _line("Mcell-steps/s, 3D reactive shock-bubble 256^3, FP32 flux / FP64 state, IMEX", rates["fp32"], UNIT, K,
+                 W, timing_all["fp32"], "f32 (reconstruction, AUSM, residual) + f64 (state, decode, chemistry)",
+                 {"workload": "3D reactive shock-bubble interaction 256^3 on a 0.1 m cube: Mach 2 shock in air "
+                              "(300 K, 1 atm) from x = 0.01 m into a stoichiometric H2-O2 bubble of radius 25 mm at "
+                              "the centre, tanh interface 2 cells wide, seeded radial perturbation 0.02 R on "
+                              "spherical harmonics l <= 8",
+                  "cells": cells, "time": f"SSP-RK2, CFL {CFL}", "chemistry": "FP64 IMEX", "boundary": "RSBI (mirror)",
+                  "graph": "one CUDA graph per step", "l2": "state ~6 GB >> 126 MB L2", "setup_s": setup_s},
+                 rates=rates, fp32_vs_fp64_speedup=rates["fp32"] / rates["fp64"],
+                 fp32_flux_errors_vs_fp64={"steps": nerr, "errors": err,
+                                           "measures": "rho, p, T: pointwise relative; Y_k: |dY_k| / max Y_k"},
+                 kernels=_kernel_table(profs_all), roofline=rf, clocks=clocks, e2e=e2e, cpu_baseline=cb,
+                 gpu_launches=int(sum(v[1] for v in profs_all["fp32"].values())),
+                 status={k: stats32[k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")})
+
+
+def run_surrogate(a):
+    """C4: the learned chemistry standalone on 2^22 states (T 300-3500 K, log p
+    in [0.05, 50] atm, compositions at the element ratios of stoichiometric
+    H2-air, dt log-uniform in [1e-9, 1e-7] s): FP64 labels from the adaptive
+    integrator, Adam training steps (batch 8192) on the tensor-core kernels,
+    and inference of all states with the fused tensor-core kernel.  Value:
+    inference, in million states per second; the roofline is the inference
+    kernel's (71 168 FLOP a state)."""
+    import torch
+    from eu3d_b200 import gpu
+    from eu3d_b200 import surrogate as S
+    from eu3d_b200.readers import load_h2_ja919
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    mech = load_h2_ja919()
+    n = 1 << 22
+    from eu3d_b200.readers import make_grid
+    grid = make_grid(8, 0, 1, 8, 0, 1, 2, 0, 1, 2, fixed_ghosts=True)
+    dev = gpu.DeviceFlowfield(mech, grid, quirks=gpu.QUIRKS_FIXED, flux_bits=32)
+    sur = gpu.DeviceSurrogate(dev, n, S.atoms_matrix(mech))
+    env = (300.0, 3500.0, np.log(0.05), np.log(50.0), np.log(1e-9), np.log(1e-7))
+    sur.add_random(n, env, S.species_index(mech), 7)
+    # labels and training are synchronous calls on the surrogate's own stream:
+    # timed on the host around them, the device idle on both sides
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nv = sur.label(gpu.REACT_ADAPTIVE, cap=4096)
+    label_ms = (time.perf_counter() - t0) * 1e3
+    X, Lb = sur.dataset()
+    model = S.SurrogateModel.load(a.model)
+    sur.set_norm(model.norm)
+    sur.set_params(model.params)
+    batch, steps = 8192, max(a.steps, 200)
+    sur.train(20, batch, 1e-4, 1e-5, 1, 3)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sur.train(steps, batch, 1e-4, 1e-5, 1, 5)
+    torch.cuda.synchronize()
+    train_ms = (time.perf_counter() - t0) * 1e3
+    feats = torch.from_numpy(np.ascontiguousarray(S.features(X, model.norm), dtype=np.float32)).cuda()
+    out = torch.empty((n, 16), dtype=torch.float32, device="cuda")
+    cur = torch.cuda.current_stream()
+    for _ in range(max(a.warmup, 3)):
+        sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
+    K = max(a.steps, 10)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    clk = ClockSampler(0)
+    clk.__enter__()
+    ev[0].record(cur)
+    for _ in range(K):
+        sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
+    ev[1].record(cur)
+    torch.cuda.synchronize()
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+    infer_ms = ev[0].elapsed_time(ev[1]) / K
+    hbm, tfl, src = peaks()
+    flop = kernel_work(4)["sur_mlp"][1]
+    ach = flop * n / (infer_ms * 1e-3) / 1e12
+    rf = {"bound": "tensor", "kernel": "sur_mlp (array source)", "achieved": ach, "peak": tfl, "unit": "TFLOP/s",
+          "frac": ach / tfl, "traffic": None, "per_cell": f"{flop} FLOP", "cells": n, "avg_ms": infer_ms,
+          "peak_source": src}
+    train_flop = 3 * flop * batch * steps
+    # host baseline: the oracle's FP64 forward pass (numpy) on a bounded sample
+    from mlp_oracle import forward
+    m = 1 << 16
+    f64 = S.features(X[:m], model.norm).astype(np.float64)
+    t0 = time.perf_counter()
+    forward(model.params.astype(np.float64), f64, quantize=False)
+    cpu_s = time.perf_counter() - t0
+    cb = {"value": m / cpu_s / 1e6, "unit": "Mstates/s", "cores": os.cpu_count() or 1, "kind": "port",
+          "sample": f"the oracle's FP64 forward pass (numpy, BLAS threads) on {m} of the states", "seconds": cpu_s}
+    # e2e: host features in, host outputs back, every pass
+    host_in = torch.from_numpy(np.ascontiguousarray(S.features(X, model.norm), dtype=np.float32)).pin_memory()
+    host_out = torch.empty((n, 16), dtype=torch.float32).pin_memory()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    for _ in range(3):
+        feats.copy_(host_in, non_blocking=True)
+        sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
+        host_out.copy_(out, non_blocking=True)
+    e1.record(cur)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / 3
+    sur.close()
+    dev.close()
+    return _line("Mstates/s, chemistry surrogate inference on 2^22 states", n / (infer_ms * 1e-3) / 1e6, "Mstates/s",
+                 K, max(a.warmup, 3), infer_ms * K, "bf16 (weights, activations) + f32 (accumulation)",
+                 {"workload": "2^22 random thermochemical states (T 300-3500 K, p 0.05-50 atm, stoichiometric H2-air "
+                              "element ratios, dt 1e-9-1e-7 s); MLP 12 -> 3x128 GELU -> 10",
+                  "states": n, "labels": "FP64 adaptive integrator (cap 4096 substeps)",
+                  "training": f"Adam, batch {batch}, {steps} steps", "l2": "inputs 268 MB > 126 MB L2"},
+                 labels={"valid": nv, "ms": label_ms, "Mstates_per_s": n / (label_ms * 1e-3) / 1e6},
+                 training={"steps": steps, "batch": batch, "ms": train_ms,
+                           "samples_per_s": batch * steps / (train_ms * 1e-3),
+                           "tflops_forward_backward": train_flop / (train_ms * 1e-3) / 1e12,
+                           "flop_note": "3 x 71 168 FLOP per sample (forward and the two backward GEMMs)"},
+                 roofline=rf, clocks=clocks, cpu_baseline=cb,
+                 e2e={"value": n / (e2e_ms * 1e-3) / 1e6, "unit": "Mstates/s", "h2d_bytes_per_step": n * 64,
+                      "d2h_bytes_per_step": n * 64, "ms": e2e_ms,
+                      "protocol": "pinned host features -> device, inference, outputs -> pinned host, per pass"},
+                 gpu_launches=K)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -567,6 +1011,13 @@ def main():
         out = run_reference(a, rank, world)
         if out is not None:
             print(json.dumps(out), flush=True)
+        return
+    if a.config != "odw3d":
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            fn = {"znd": run_znd, "odw2d": run_odw2d, "rsbi": run_rsbi, "surrogate": run_surrogate}[a.config]
+            print(json.dumps(fn(a)), flush=True)
         return
     if world > 1:
         import datetime

@@ -38,7 +38,7 @@ def main(argv=None):
     d.set_tuning(flux_stage=a.flux_stage)
     if a.kz:
         d.set_tuning(flux_kz=a.kz)
-    S.SurrogateModel.load(S.DEFAULT_MODEL).attach(d, 0)
+    S.SurrogateModel.load(S.DEFAULT_MODEL).attach(d, 0, gate=S.GATE)
     kw = dict(timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.5, final_time=1.0)
     for react, n in ((gpu.REACT_IMEX, a.imex), (gpu.REACT_SURROGATE, a.surrogate), (gpu.REACT_ADAPTIVE, a.adaptive)):
         if n:
