@@ -614,7 +614,7 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
 //  M_RK3_STAGE2/3 SSP-RK3 stage updates (new)
 //  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
 template <class P, int MODE, bool SPEC>
-__global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
+__device__ __forceinline__ void cell_body(const CellArgs &a, P *__restrict__ q)
 {
     const Layout &L = a.L;
     const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
@@ -761,6 +761,22 @@ __global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
     store_prims<P>(o, q, fs, c);
     warp_count(&a.st->newton_capped, capped_any != 0);
     warp_count(&a.st->nonfinite, !(isfinite(o.D) && isfinite(o.T)));
+}
+
+template <class P, int MODE, bool SPEC>
+__global__ void __launch_bounds__(128, 3) k_cell(CellArgs a, P *__restrict__ q)
+{
+    cell_body<P, MODE, SPEC>(a, q);
+}
+
+// The same cell update compiled for NB resident blocks of 128 threads per SM
+// (fewer registers a thread): the memory-bound SSP-RK2 stage updates, whose
+// decode otherwise holds 167 registers and leaves 12 warps per SM to cover
+// the HBM latency (tuning cell_blocks).
+template <class P, int MODE, bool SPEC, int NB>
+__global__ void __launch_bounds__(128, NB) k_cell_nb(CellArgs a, P *__restrict__ q)
+{
+    cell_body<P, MODE, SPEC>(a, q);
 }
 
 // Bin offsets of the adaptive-trapezoid queue, heaviest bin first (one warp).

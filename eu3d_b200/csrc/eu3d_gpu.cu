@@ -92,6 +92,7 @@ struct eu3d_handle {
     int sur_fused = 0;     // surrogate: network and apply in one kernel (1) or two kernels (0, faster)
     unsigned wait_tries = 1u << 19;  // bound of the flux ring's copy waits (eu3d_set_wait_limit)
     int adapt_queue = 0;   // FP64 adaptive chemistry on the persistent queue (1) or one thread per cell (0)
+    int cell_blocks = 3;   // resident blocks per SM of the FP32-path SSP-RK2 stage updates (3, 4 or 6)
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
@@ -214,6 +215,20 @@ void launch_cell_t(eu3d_handle *h, int mode)
                                   "cell_rk1",    "cell_rk2",   "cell_nochem",        "cell_trap1_predict",
                                   "cell_adapt",  "cell_rk3_2", "cell_rk3_3"};
     ProfScope ps(h, names[mode]);
+    if constexpr (sizeof(P) == 4) {
+        // SSP-RK2 stage updates of the FP32-flux path at the tuned occupancy
+        if ((mode == M_RK_STAGE1 || mode == M_RK_STAGE2) && h->cell_blocks != 3) {
+            const bool s1 = mode == M_RK_STAGE1;
+            if (h->cell_blocks == 4) {
+                if (s1) k_cell_nb<P, M_RK_STAGE1, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
+                else k_cell_nb<P, M_RK_STAGE2, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
+            } else {
+                if (s1) k_cell_nb<P, M_RK_STAGE1, SPEC, 6><<<g, 128, 0, h->st>>>(a, q);
+                else k_cell_nb<P, M_RK_STAGE2, SPEC, 6><<<g, 128, 0, h->st>>>(a, q);
+            }
+            return;
+        }
+    }
     switch (mode) {
     case M_DECODE: k_cell<P, M_DECODE, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
     case M_ADV: k_cell<P, M_ADV, SPEC><<<g, 128, 0, h->st>>>(a, q); break;
@@ -1918,6 +1933,9 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
     h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
     h->sur_fused = t->sur_fused ? 1 : 0;
+    if (t->cell_blocks != 3 && t->cell_blocks != 4 && t->cell_blocks != 6)
+        return fail(EU3D_ERR_ARG, "cell_blocks must be 3, 4 or 6");
+    h->cell_blocks = t->cell_blocks;
     h->adapt_queue = t->adapt_queue ? 1 : 0;
     if (h->adapt_queue) {
         int rc = ensure_cell_list(h);
@@ -1947,6 +1965,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
     t->flux_stage = h->flux_stage;
     t->sur_fused = h->sur_fused;
     t->adapt_queue = h->adapt_queue;
+    t->cell_blocks = h->cell_blocks;
     return EU3D_OK;
 }
 
@@ -1955,7 +1974,8 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     if (!h || !s) return fail(EU3D_ERR_ARG, "null argument");
     if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
     CK(cudaSetDevice(h->dev));
-    const eu3d_tuning start{h->flux_kz, h->chem_queue, h->queue_blocks, h->flux_stage, h->sur_fused, h->adapt_queue};
+    const eu3d_tuning start{h->flux_kz,   h->chem_queue,  h->queue_blocks, h->flux_stage,
+                            h->sur_fused, h->adapt_queue, h->cell_blocks};
     // the trials advance the state: keep a copy and put it back after each
     const size_t fs = (size_t)h->L.fs;
     const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
@@ -1981,17 +2001,23 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     std::vector<eu3d_tuning> cands;
     const bool q = s->react == EU3D_REACT_TRAPEZOID && s->type == 1;
     const bool aq = s->react == EU3D_REACT_ADAPTIVE;
+    const bool rk2 = s->timeadv == EU3D_ADV_SSPRK2 && h->flux_bits == 32;
     for (int fst : {0, 1, 2})
         for (int kz : {4, 8, 16, 32, 64})
             for (int cq : {0, 1})
                 for (int qb : {2, 3, 4})
-                    for (int ad : {0, 1}) {
-                        if (h->flux_bits == 64 && fst != start.flux_stage) continue;
-                        if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
-                        if (q && cq == 0 && qb != start.queue_blocks) continue;
-                        if (!aq && ad != start.adapt_queue) continue;
-                        cands.push_back({kz, cq, qb, fst, start.sur_fused, ad});
-                    }
+                    for (int ad : {0, 1})
+                        for (int cb : {3, 4, 6}) {
+                            if (h->flux_bits == 64 && fst != start.flux_stage) continue;
+                            if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
+                            if (q && cq == 0 && qb != start.queue_blocks) continue;
+                            if (!aq && ad != start.adapt_queue) continue;
+                            if (!rk2 && cb != start.cell_blocks) continue;
+                            // the stage occupancy is tuned at the default flux setting
+                            if (rk2 && cb != start.cell_blocks && (fst != start.flux_stage || kz != start.flux_kz))
+                                continue;
+                            cands.push_back({kz, cq, qb, fst, start.sur_fused, ad, cb});
+                        }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);

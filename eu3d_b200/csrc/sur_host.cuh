@@ -258,11 +258,8 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
         }
         {
             ProfScope ps(h, "sur_apply");
-            int sms = 148;
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->dev);
-            const long long need = (n + 127) / 128;
-            k_sur_apply_list<P><<<(unsigned)std::max<long long>(1, std::min<long long>(need, 7LL * sms)), 128, 0,
-                                  h->st>>>(a, q, h->sur_active, acount);
+            k_sur_apply_list<P><<<(unsigned)std::max<long long>(1, (n + 127) / 128), 128, 0, h->st>>>(
+                a, q, h->sur_active, acount);
         }
     } else if (h->sur_fused) {
         // network and apply in one kernel (outputs stay on chip)

@@ -891,25 +891,24 @@ __global__ void __launch_bounds__(256) k_list_fluid(CellArgs a, SurQueue qu)
     sur_push(qu, true, (int)L.at(i, j, k), 0.0);
 }
 
-// The apply of the listed cells (grid-stride over the list, whose length is
-// on the device); network outputs by list position.
+// The apply of the listed cells: one thread per list position, launched
+// for the largest possible list (the length is on the device); network
+// outputs by list position.
 template <class P>
 __global__ void __launch_bounds__(128, 7) k_sur_apply_list(SurApplyArgs s, P *__restrict__ q,
                                                            const int *__restrict__ list, const int *__restrict__ count)
 {
     const Layout &L = s.a.L;
-    const long long total = min((long long)*count, s.n);
+    const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= min((long long)*count, s.n)) return;
     const int plane = L.NJ * L.px;
-    for (long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x; pos < total;
-         pos += (long long)gridDim.x * blockDim.x) {
-        const int c = list[pos];
-        const int k = c / plane, r = c - k * plane;
-        const int j = r / L.px, i = r - j * L.px;
-        float o[SUR_NOUT];
+    const int c = list[pos];
+    const int k = c / plane, r = c - k * plane;
+    const int j = r / L.px, i = r - j * L.px;
+    float o[SUR_NOUT];
 #pragma unroll
-        for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
-        sur_apply_cell<P>(s, q, i, j, k, o);
-    }
+    for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
+    sur_apply_cell<P>(s, q, i, j, k, o);
 }
 
 // The MLP kernel's source for the fused form: features from the flowfield

@@ -88,7 +88,7 @@ class Status(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int), ("flux_stage", C.c_int),
-                ("sur_fused", C.c_int), ("adapt_queue", C.c_int)]
+                ("sur_fused", C.c_int), ("adapt_queue", C.c_int), ("cell_blocks", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -442,8 +442,10 @@ class DeviceFlowfield:
         return t.as_dict()
 
     def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None, sur_fused=None,
-                   adapt_queue=None):
+                   adapt_queue=None, cell_blocks=None):
         t = Tuning(**self.tuning())
+        if cell_blocks is not None:
+            t.cell_blocks = int(cell_blocks)
         if adapt_queue is not None:
             t.adapt_queue = 1 if adapt_queue else 0
         if flux_kz is not None:

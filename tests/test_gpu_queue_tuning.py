@@ -48,7 +48,7 @@ def test_autotune_restores_state_and_sets_best(mech):
     T0 = a.download("T").copy()
     best, ms = a.autotune(steps=2, react=gpu.REACT_TRAPEZOID, type_=1, bc_kind=gpu.BC_RSBI)
     assert ms > 0
-    assert best["flux_kz"] in (4, 8, 16, 32, 64) and best["chem_queue"] in (0, 1)
+    assert best["flux_kz"] in (4, 8, 16, 32, 64) and best["chem_queue"] in (0, 1) and best["cell_blocks"] == 3
     assert a.tuning() == best
     assert np.array_equal(a.download("CS"), cs0) and np.array_equal(a.download("T"), T0)
     st = a.status()
@@ -176,3 +176,29 @@ def test_flux_kernels_with_wedge_match_oracle(mech, stage):
         d.advection(gpu.ADV_EE, gpu.DIFF_MUSCL2)
         assert np.array_equal(interior(d.download("RHS"))[fluid], res[32][fluid])
         d.close()
+
+
+def test_stage_update_occupancy_gives_the_same_bits(mech):
+    """The SSP-RK2 stage updates compiled for 3, 4 and 6 resident blocks per
+    SM (tuning cell_blocks) are the same arithmetic: identical state after a
+    few steps of the ODW with its wedge."""
+    from eu3d_b200.cases import odw_case, setup_odw
+    case = odw_case(mech, 96, 48, 4, L=0.2 * 95 / 511.0)
+    out = []
+    for cb in (3, 4, 6):
+        d = gpu.DeviceFlowfield(mech, case.grid, QUIRKS_FIXED, flux_bits=32)
+        setup_odw(d, case)
+        d.set_tuning(cell_blocks=cb)
+        assert d.tuning()["cell_blocks"] == cb
+        d.run(8, react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.5)
+        d.synchronize()
+        out.append({f: d.download(f) for f in ("CS", "T", "P")})
+        d.close()
+    for f in ("CS", "T", "P"):
+        assert np.array_equal(out[0][f], out[1][f]) and np.array_equal(out[0][f], out[2][f]), f
+    with pytest.raises(gpu.Eu3dError):
+        d2 = gpu.DeviceFlowfield(mech, case.grid, QUIRKS_FIXED, flux_bits=32)
+        try:
+            d2.set_tuning(cell_blocks=5)
+        finally:
+            d2.close()
