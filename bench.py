@@ -12,13 +12,17 @@ extruded along z.  Inputs (~12 GB of state) are far larger than L2 (126 MB),
 so no flush is needed between steps.
 
 Metric: Mcell-steps/s = interior cells x steps / device time, with the
-learned chemistry surrogate (value); the same steps with the plain FP64 IMEX
-integrator and with the FP64 adaptive integrator (the surrogate's teacher)
-are timed on the same GPU and state and reported beside it, with the
-coupled accuracy of a 2D run (peak T, detonation front) against the FP64
-runs.
+learned chemistry surrogate (value; its frozen-chemistry gate on, launch
+settings from the project's autotuner); the same steps with the plain FP64
+IMEX integrator and with the FP64 adaptive integrator (the surrogate's
+teacher) are timed on the same GPU and state and reported beside it, with
+the per-step split of chemistry and the rest, and the coupled accuracy of
+the FP32-flux, surrogate and IMEX forms against the all-FP64 run (errors in
+rho, p, T and each Y_k, peak T, detonation front) on the 2D case and a
+spanwise slice of the 3D one.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+    python bench.py --config {znd,odw2d,rsbi,surrogate}   (the other configurations, one GPU)
 
 --gpus N (under torchrun, one rank per GPU): the same case split into N x
 slabs (strong scaling), halos exchanged by NCCL send/recv and dt reduced by
