@@ -25,8 +25,10 @@ EXE = os.path.join(HOST, "eu3d_dropin")
 
 
 def build_driver():
+    """Links the driver against the in-tree library (built by
+    __graft_entry__.build / python -m eu3d_b200.build)."""
     from eu3d_b200 import build as b
-    b.build()
+    assert os.path.exists(b.LIB), "libeu3d_gpu.so missing: python -m eu3d_b200.build"
     subprocess.run(["make", "-s", "-C", HOST], check=True)
     return EXE
 
