@@ -178,8 +178,12 @@ class Slab:
         c = self.counts
         self.dlb_alloc(sum(c[t] for t in self.mine), sum(c[t] for t in self.theirs))
         self.dlb_pack()
-        yield "dlb_out"
+        # the packets travel while this rank integrates the cells it kept (the
+        # reference overlaps its non-blocking sends the same way,
+        # src/Euler.cpp:488-518); the guest work waits for them
+        yield "dlb_out_start"
         self.part(gpu.PART_CHEM_WORK, spec)
+        yield "dlb_out_wait"
         self.dlb_guest([c[t] for t in self.theirs])
         yield "dlb_back"
         self.dlb_unpack()
@@ -223,6 +227,9 @@ class DeviceSlab(Slab):
         self._recv = {s: torch.empty(nb, dtype=torch.uint8, device=f"cuda:{dev.device}") for s in (0, 1)}
         self._dt = torch.as_tensor(_CudaArray(dev.dt_device_ptr), device=f"cuda:{dev.device}")
         self.stream = torch.cuda.ExternalStream(dev.stream, device=f"cuda:{dev.device}")
+        # load-balancing packets travel on this stream while the handle's
+        # stream integrates the rank's own cells
+        self.side = torch.cuda.Stream(device=f"cuda:{dev.device}")
 
     def cfl_local(self, cfl, final_time):
         self.d.cfl_local(cfl, final_time)
@@ -344,13 +351,16 @@ class LoopbackTransport:
     def _by_rank(self, slabs):
         return {s.rank: s for s in slabs}
 
-    def dlb_out(self, slabs):
+    def dlb_out_start(self, slabs):
         self._sync(slabs)
         by = self._by_rank(slabs)
         for t, (snd, rcv, _) in enumerate(slabs[0].plan):
             if by[rcv].counts[t]:
                 by[rcv].in_seg(t).copy_(by[snd].out_seg(t))
         self._sync(slabs)
+
+    def dlb_out_wait(self, slabs):
+        pass  # the copies above are complete
 
     def dlb_back(self, slabs):
         self._sync(slabs)
@@ -419,28 +429,47 @@ class TorchTransport:
             self.dist.all_reduce(v, op=self.dist.ReduceOp.SUM, group=self.group)
         s.counts = [int(x) for x in v.tolist()]
 
-    def _p2p(self, s, sends, recvs):
+    def _p2p(self, s, sends, recvs, side=False):
+        """Posts the sends and receives; returns their requests.  side: on
+        a device slab, issue them on the slab's side stream (after the
+        packets are packed on its own stream), so that the slab's stream runs
+        on while they travel."""
         dist = self.dist
+        ops = [dist.P2POp(dist.isend, buf, peer, group=self.group) for buf, peer in sends]
+        ops += [dist.P2POp(dist.irecv, buf, peer, group=self.group) for buf, peer in recvs]
+        if not ops:
+            return []
+        if side and isinstance(s, DeviceSlab):
+            s.side.wait_stream(s.stream)
+            with s.torch.cuda.stream(s.side):
+                return dist.batch_isend_irecv(ops)
         with self._ctx(s):
-            ops = [dist.P2POp(dist.isend, buf, peer, group=self.group) for buf, peer in sends]
-            ops += [dist.P2POp(dist.irecv, buf, peer, group=self.group) for buf, peer in recvs]
-            if ops:
-                for req in dist.batch_isend_irecv(ops):
-                    req.wait()
+            return dist.batch_isend_irecv(ops)
 
-    def dlb_out(self, slabs):
+    def _wait(self, s, reqs):
+        # NCCL: the slab's stream waits for the transfers; gloo: the host waits
+        with self._ctx(s):
+            for req in reqs:
+                req.wait()
+
+    def dlb_out_start(self, slabs):
         (s,) = slabs
         plan = s.plan
         sends = [(s.out_seg(t), plan[t][1]) for t in s.mine if s.counts[t]]
         recvs = [(s.in_seg(t), plan[t][0]) for t in s.theirs if s.counts[t]]
-        self._p2p(s, sends, recvs)
+        s._dlb_reqs = self._p2p(s, sends, recvs, side=True)
+
+    def dlb_out_wait(self, slabs):
+        (s,) = slabs
+        self._wait(s, getattr(s, "_dlb_reqs", []))
+        s._dlb_reqs = []
 
     def dlb_back(self, slabs):
         (s,) = slabs
         plan = s.plan
         sends = [(s.guest_seg(t), plan[t][0]) for t in s.theirs if s.counts[t]]
         recvs = [(s.back_seg(t), plan[t][1]) for t in s.mine if s.counts[t]]
-        self._p2p(s, sends, recvs)
+        self._wait(s, self._p2p(s, sends, recvs))
 
 
 class SlabRun:
