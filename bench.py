@@ -476,7 +476,7 @@ def run_ours(a, rank, world, local):
     steps_run = a.steps + W
     net_cells = (st["surrogate_cells"] + st["surrogate_fallback"] + st["surrogate_audited"]) // max(steps_run, 1)
     units = {k: fluid for k in kernel_work(4)}
-    units["sur_mlp"] = units["sur_mlp_apply"] = net_cells
+    units["sur_mlp"] = units["sur_mlp_apply"] = units["sur_apply"] = net_cells
     pb = 4 if a.flux_bits == 32 else 8
     rf = roofline(prof, units, hbm, tfl, src, pb=pb)
     rf_more = {k: {f: r[f] for f in ("achieved", "unit", "frac", "avg_ms", "cells", "per_cell")}

@@ -92,7 +92,7 @@ struct eu3d_handle {
     int sur_fused = 0;     // surrogate: network and apply in one kernel (1) or two kernels (0, faster)
     unsigned wait_tries = 1u << 19;  // bound of the flux ring's copy waits (eu3d_set_wait_limit)
     int adapt_queue = 0;   // FP64 adaptive chemistry on the persistent queue (1) or one thread per cell (0)
-    int cell_blocks = 3;   // resident blocks per SM of the FP32-path SSP-RK2 stage updates (3, 4 or 6)
+    int cell_blocks = 3;   // resident blocks per SM of the FP32-path SSP-RK2 stage updates (3 or 4)
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
@@ -217,15 +217,9 @@ void launch_cell_t(eu3d_handle *h, int mode)
     ProfScope ps(h, names[mode]);
     if constexpr (sizeof(P) == 4) {
         // SSP-RK2 stage updates of the FP32-flux path at the tuned occupancy
-        if ((mode == M_RK_STAGE1 || mode == M_RK_STAGE2) && h->cell_blocks != 3) {
-            const bool s1 = mode == M_RK_STAGE1;
-            if (h->cell_blocks == 4) {
-                if (s1) k_cell_nb<P, M_RK_STAGE1, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
-                else k_cell_nb<P, M_RK_STAGE2, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
-            } else {
-                if (s1) k_cell_nb<P, M_RK_STAGE1, SPEC, 6><<<g, 128, 0, h->st>>>(a, q);
-                else k_cell_nb<P, M_RK_STAGE2, SPEC, 6><<<g, 128, 0, h->st>>>(a, q);
-            }
+        if ((mode == M_RK_STAGE1 || mode == M_RK_STAGE2) && h->cell_blocks == 4) {
+            if (mode == M_RK_STAGE1) k_cell_nb<P, M_RK_STAGE1, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
+            else k_cell_nb<P, M_RK_STAGE2, SPEC, 4><<<g, 128, 0, h->st>>>(a, q);
             return;
         }
     }
@@ -1933,8 +1927,9 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
     h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
     h->sur_fused = t->sur_fused ? 1 : 0;
-    if (t->cell_blocks != 3 && t->cell_blocks != 4 && t->cell_blocks != 6)
-        return fail(EU3D_ERR_ARG, "cell_blocks must be 3, 4 or 6");
+    // (a build for 6 blocks, at 85 registers, scheduled the decode's
+    // arithmetic differently and changed results in the last bits: left out)
+    if (t->cell_blocks != 3 && t->cell_blocks != 4) return fail(EU3D_ERR_ARG, "cell_blocks must be 3 or 4");
     h->cell_blocks = t->cell_blocks;
     h->adapt_queue = t->adapt_queue ? 1 : 0;
     if (h->adapt_queue) {
@@ -2007,7 +2002,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
             for (int cq : {0, 1})
                 for (int qb : {2, 3, 4})
                     for (int ad : {0, 1})
-                        for (int cb : {3, 4, 6}) {
+                        for (int cb : {3, 4}) {
                             if (h->flux_bits == 64 && fst != start.flux_stage) continue;
                             if (!q && (cq != start.chem_queue || qb != start.queue_blocks)) continue;
                             if (q && cq == 0 && qb != start.queue_blocks) continue;

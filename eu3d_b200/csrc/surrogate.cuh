@@ -703,13 +703,18 @@ __device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int valu
 // energy balance at the predicted temperature, then applied to the species
 // and decoded in FP64.  Rejected cells (and audited ones) go to the fallback
 // list untouched.  (i, j, k): ghosted indices; net: the cell's network outputs.
-template <class P>
-__device__ __forceinline__ void sur_apply_cell(const SurApplyArgs &s, P *__restrict__ q, int i, int j, int k,
-                                               const float net[SUR_NOUT])
+// Outcome bits of sur_apply_cell, in the order of the status counters it
+// feeds: accepted, fallen back, then the rejection reasons (envelope,
+// network output, energy residual, failed decode).
+constexpr int SUR_NFLAGS = 6;
+
+template <class P, bool COUNT = true>
+__device__ __forceinline__ unsigned sur_apply_cell(const SurApplyArgs &s, P *__restrict__ q, int i, int j, int k,
+                                                   const float net[SUR_NOUT])
 {
     const CellArgs &a = s.a;
     const Layout &L = a.L;
-    if (solid_cell(a, i, j)) return;
+    if (solid_cell(a, i, j)) return 0u;
     const long long c = L.at(i, j, k);
     const long long fs = L.fs;
     const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
@@ -799,13 +804,45 @@ __device__ __forceinline__ void sur_apply_cell(const SurApplyArgs &s, P *__restr
         }
     }
     sur_push(s.qu, !ok || audit, (int)((unsigned)c | (audit ? SUR_AUDIT : 0u)), audit ? o.T : 0.0);
-    warp_count(&a.st->sur_cells, ok && !audit);
-    warp_count(&a.st->sur_fallback, !ok);
-    warp_count(&a.st->sur_reject[0], !ok_env);
-    warp_count(&a.st->sur_reject[1], ok_env && !ok_out);
-    warp_count(&a.st->sur_reject[2], ok_out && !ok_res);
-    warp_count(&a.st->sur_reject[3], ok_res && !ok);
+    const unsigned flags = (ok && !audit ? 1u : 0u) | (!ok ? 2u : 0u) | (!ok_env ? 4u : 0u) |
+                           (ok_env && !ok_out ? 8u : 0u) | (ok_out && !ok_res ? 16u : 0u) | (ok_res && !ok ? 32u : 0u);
+    if (COUNT) {
+        warp_count(&a.st->sur_cells, flags & 1u);
+        warp_count(&a.st->sur_fallback, flags & 2u);
+        warp_count(&a.st->sur_reject[0], flags & 4u);
+        warp_count(&a.st->sur_reject[1], flags & 8u);
+        warp_count(&a.st->sur_reject[2], flags & 16u);
+        warp_count(&a.st->sur_reject[3], flags & 32u);
+    }
+    return flags;
 }
+
+// Block-level counting: each warp adds its lanes' flags to shared counters,
+// then one thread per counter adds the block's sums to the status -- one
+// global atomic per counter and block instead of per warp (the counters are
+// a few hot addresses).  All threads of the block must call both.
+template <int N>
+struct BlockCount {
+    unsigned long long *sm;  // N shared counters
+    __device__ __forceinline__ void init() const
+    {
+        if (threadIdx.x < N) sm[threadIdx.x] = 0ull;
+        __syncthreads();
+    }
+    __device__ __forceinline__ void add(unsigned flags) const
+    {
+#pragma unroll
+        for (int b = 0; b < N; b++) {
+            const unsigned m = __ballot_sync(0xffffffffu, (flags >> b) & 1u);
+            if ((threadIdx.x & 31) == 0 && m) atomicAdd(&sm[b], (unsigned long long)__popc(m));
+        }
+    }
+    __device__ __forceinline__ void flush(unsigned long long *const dst[N]) const
+    {
+        __syncthreads();
+        if (threadIdx.x < N && sm[threadIdx.x]) atomicAdd(dst[threadIdx.x], sm[threadIdx.x]);
+    }
+};
 
 // One thread per interior cell: the network outputs from the MLP kernel's
 // output buffer.
@@ -843,40 +880,54 @@ struct SurGate {
 };
 
 template <class P>
-__global__ void __launch_bounds__(256) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g, SurQueue qu)
+__global__ void __launch_bounds__(512) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g, SurQueue qu)
 {
     const Layout &L = a.L;
     const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = L.bc + blockIdx.y;
     const int k = L.bc + blockIdx.z;
-    if (i >= L.ni + L.bc) return;
-    if (solid_cell(a, i, j)) return;
-    const long long c = L.at(i, j, k);
-    const double T = a.T[c];
-    bool frozen = T < g.T_frozen;
-    if (frozen && g.mask) {
-        double y = 0.0;
+    const bool fluid = i < L.ni + L.bc && !solid_cell(a, i, j);
+    const long long c = L.at(min(i, L.ni + L.bc - 1), j, k);
+    bool frozen = false;
+    double T = 0.0;
+    if (fluid) {
+        T = a.T[c];
+        frozen = T < g.T_frozen;
+        if (frozen && g.mask) {
+            double y = 0.0;
 #pragma unroll
-        for (int s = 0; s < NS; s++)
-            if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c], 0.0);
-        frozen = y <= g.y_max;
-    }
-    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
-    const bool audit = frozen && g.audit_stride > 0 && ((unsigned)idx % (unsigned)g.audit_stride) == 0;
-    {
-        // warp-aggregated append of the active cells, in lane order
-        const unsigned act = __activemask();
-        const unsigned m = __ballot_sync(act, !frozen);
-        if (m) {
-            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
-            int base = 0;
-            if (lane == leader) base = atomicAdd(g.acount, __popc(m));
-            base = __shfl_sync(act, base, leader);
-            if (!frozen) g.active[base + __popc(m & ((1u << lane) - 1u))] = (int)c;
+            for (int s = 0; s < NS; s++)
+                if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c], 0.0);
+            frozen = y <= g.y_max;
         }
     }
+    const bool active = fluid && !frozen;
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    const bool audit = frozen && g.audit_stride > 0 && ((unsigned)idx % (unsigned)g.audit_stride) == 0;
+    // block-aggregated append of the active cells, in thread order: one
+    // global atomic for the list and one for the frozen count per block
+    __shared__ int wact[16], wfrz[16], base_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned ma = __ballot_sync(0xffffffffu, active), mf = __ballot_sync(0xffffffffu, frozen);
+    if (lane == 0) {
+        wact[w] = __popc(ma);
+        wfrz[w] = __popc(mf);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ta = 0, tf = 0;
+        for (int v = 0; v < nw; v++) {
+            const int n = wact[v];
+            wact[v] = ta;  // exclusive offsets
+            ta += n;
+            tf += wfrz[v];
+        }
+        base_s = ta ? atomicAdd(g.acount, ta) : 0;
+        if (tf) atomicAdd(&a.st->sur_frozen, (unsigned long long)tf);
+    }
+    __syncthreads();
+    if (active) g.active[base_s + wact[w] + __popc(ma & ((1u << lane) - 1u))] = (int)c;
     sur_push(qu, audit, (int)((unsigned)c | SUR_FROZEN_AUDIT), T);
-    warp_count(&a.st->sur_frozen, frozen);
 }
 
 // Lists every fluid interior cell (the queued adaptive chemistry's work).
@@ -899,16 +950,26 @@ __global__ void __launch_bounds__(128, 7) k_sur_apply_list(SurApplyArgs s, P *__
                                                            const int *__restrict__ list, const int *__restrict__ count)
 {
     const Layout &L = s.a.L;
+    __shared__ unsigned long long cnt[SUR_NFLAGS];
+    const BlockCount<SUR_NFLAGS> bc{cnt};
+    bc.init();
     const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= min((long long)*count, s.n)) return;
-    const int plane = L.NJ * L.px;
-    const int c = list[pos];
-    const int k = c / plane, r = c - k * plane;
-    const int j = r / L.px, i = r - j * L.px;
-    float o[SUR_NOUT];
+    unsigned flags = 0u;
+    if (pos < min((long long)*count, s.n)) {
+        const int plane = L.NJ * L.px;
+        const int c = list[pos];
+        const int k = c / plane, r = c - k * plane;
+        const int j = r / L.px, i = r - j * L.px;
+        float o[SUR_NOUT];
 #pragma unroll
-    for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
-    sur_apply_cell<P>(s, q, i, j, k, o);
+        for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
+        flags = sur_apply_cell<P, false>(s, q, i, j, k, o);
+    }
+    bc.add(flags);
+    Status *st = s.a.st;
+    unsigned long long *const dst[SUR_NFLAGS] = {&st->sur_cells,     &st->sur_fallback,  &st->sur_reject[0],
+                                                 &st->sur_reject[1], &st->sur_reject[2], &st->sur_reject[3]};
+    bc.flush(dst);
 }
 
 // The MLP kernel's source for the fused form: features from the flowfield

@@ -278,10 +278,10 @@ int eu3d_dlb_unpack(eu3d_handle *h, const double *dev_back);
    (default, faster on B200): two kernels; the same decisions either way.
    adapt_queue 1: the FP64 adaptive chemistry (EU3D_REACT_ADAPTIVE) lists the
    fluid cells and integrates them on the persistent queue, one cell per lane
-   with refill; 0 (default): one thread per cell.  cell_blocks (3, default;
-   4 or 6): resident blocks of 128 threads per SM the SSP-RK2 stage updates
-   of the FP32-flux path are compiled for (more blocks, fewer registers a
-   thread).  Changing them drops the recorded step graphs. */
+   with refill; 0 (default): one thread per cell.  cell_blocks (3, default,
+   or 4): resident blocks of 128 threads per SM the SSP-RK2 stage updates of
+   the FP32-flux path are compiled for (more blocks, fewer registers a
+   thread; the same results).  Changing them drops the recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
@@ -306,7 +306,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t);
    {4, 8, 16, 32, 64}, the three FP32 flux kernels; for the adaptive
    trapezoid also the queue on/off and 2..4 blocks per SM; for the FP64
    adaptive chemistry adapt_queue on/off; for SSP-RK2 with FP32 flux the
-   stage updates' cell_blocks 3, 4, 6) on the handle's current state,
+   stage updates' cell_blocks 3, 4) on the handle's current state,
    restoring the state after
    each trial, and keeps the fastest.  best / best_ms may be NULL.  Needs
    temporary device memory for one copy of the state. */

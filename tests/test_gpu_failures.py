@@ -23,17 +23,21 @@ HOT = dict(tlo=1100.0, thi=2600.0)
 
 
 def test_newton_cap_is_counted_and_matches_the_reference_iterate(mech):
-    """Cells whose internal energy belongs to 13 500 K, decoded from a 300 K
-    start: the inversion uses all ten iterations (|dT| is still above 1e-6 K)
-    and keeps the tenth iterate, as Get_temp does; the status counts every
-    such cell and nothing goes non-finite."""
+    """Cells of stoichiometric H2-air at rest whose internal energy belongs to
+    9500 K, decoded from a 300 K start: beyond the polynomials' range the
+    Newton inversion overshoots, is still moving by thousands of kelvin at
+    its tenth iteration and keeps that iterate, as Get_temp does (the host
+    restatement of the iteration, oracle/opcount.py, shows the same for
+    starts 0.1 K either side, so the count is not a rounding accident).  The
+    status counts every such cell, nothing goes non-finite, and the iterate
+    agrees with the oracle's."""
+    from eu3d_b200.readers import stoichiometric_h2_air
     o, g = make_oracle(mech, seed=31, quirks=QUIRKS_FIXED, **HOT)
     sl = (slice(3, 6), slice(2, 5), slice(2, 4))  # 18 interior cells
-    cs = o.view("CS")
-    Y = o.view("Yi")[sl]
-    hot = complete_state(mech, o.view("P")[sl], np.full(Y.shape[:-1], 13500.0), o.view("U")[sl], o.view("V")[sl],
-                         o.view("W")[sl], Y)
-    cs[sl] = hot["CS"]
+    Y = np.broadcast_to(stoichiometric_h2_air(mech), o.view("Yi")[sl].shape)
+    z = np.zeros(Y.shape[:-1])
+    hot = complete_state(mech, z + 101325.0, z + 9500.0, z, z, z, Y)
+    o.view("CS")[sl] = hot["CS"]
     o.view("T")[sl] = 300.0
     d = gpu.DeviceFlowfield(mech, g, QUIRKS_FIXED, flux_bits=64)
     d.upload_state(o)
@@ -43,10 +47,9 @@ def test_newton_cap_is_counted_and_matches_the_reference_iterate(mech):
     st = d.status()
     assert st["newton_capped"] == 18, st
     assert st["nonfinite_cells"] == 0
-    T = interior(d.download("T"))
-    assert np.all(np.isfinite(T))
-    assert np.all(np.abs(d.download("T")[sl] - 13500.0) < 1.0)  # close, not converged to 1e-6 K
-    assert rel_err(T, interior(o.view("T"))) < 1e-9
+    T = d.download("T")[sl]
+    assert np.all(np.isfinite(T)) and np.all(T > 20000.0)  # far from 9500 K: not converged
+    assert np.max(np.abs(T / o.view("T")[sl] - 1.0)) < 1e-8
     d.close()
 
 

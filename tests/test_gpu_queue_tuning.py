@@ -142,7 +142,7 @@ def test_flux_kernels_with_wedge_match_oracle(mech, stage):
     x = g.xnode[2:-2][:, None, None]
     y = g.ynode[2:-2][None, :, None]
     fluid = np.broadcast_to(~((x > wedge[0]) & (y - wedge[1] < (x - wedge[0]) * wedge[2])), (g.ni, g.nj, g.nk))
-    assert (~fluid).sum() > 0.3 * fluid.size
+    assert (~fluid).sum() > 0.25 * fluid.size
     o.boundary(gpu.BC_RSBI, wedge)
     o.dt = 2e-8
     o.advection(0, gpu.DIFF_MUSCL2)
@@ -179,13 +179,13 @@ def test_flux_kernels_with_wedge_match_oracle(mech, stage):
 
 
 def test_stage_update_occupancy_gives_the_same_bits(mech):
-    """The SSP-RK2 stage updates compiled for 3, 4 and 6 resident blocks per
-    SM (tuning cell_blocks) are the same arithmetic: identical state after a
+    """The SSP-RK2 stage updates compiled for 3 and 4 resident blocks per SM
+    (tuning cell_blocks) are the same arithmetic: identical state after a
     few steps of the ODW with its wedge."""
     from eu3d_b200.cases import odw_case, setup_odw
     case = odw_case(mech, 96, 48, 4, L=0.2 * 95 / 511.0)
     out = []
-    for cb in (3, 4, 6):
+    for cb in (3, 4):
         d = gpu.DeviceFlowfield(mech, case.grid, QUIRKS_FIXED, flux_bits=32)
         setup_odw(d, case)
         d.set_tuning(cell_blocks=cb)
@@ -195,10 +195,10 @@ def test_stage_update_occupancy_gives_the_same_bits(mech):
         out.append({f: d.download(f) for f in ("CS", "T", "P")})
         d.close()
     for f in ("CS", "T", "P"):
-        assert np.array_equal(out[0][f], out[1][f]) and np.array_equal(out[0][f], out[2][f]), f
+        assert np.array_equal(out[0][f], out[1][f]), f
     with pytest.raises(gpu.Eu3dError):
         d2 = gpu.DeviceFlowfield(mech, case.grid, QUIRKS_FIXED, flux_bits=32)
         try:
-            d2.set_tuning(cell_blocks=5)
+            d2.set_tuning(cell_blocks=6)
         finally:
             d2.close()
