@@ -302,7 +302,8 @@ def roofline(prof, units, hbm, tflops, src, pb=4, kernel=None):
     (the fluid cells for the flux and cell kernels, which leave the wedge's
     solid cells out; the listed cells for the network)."""
     kw = kernel_work(pb)
-    cand = [(k, v) for k, v in prof.items() if k in kw]
+    # the chemistry kernels are FP64-bound: their rooflines are chem_roofline's
+    cand = [(k, v) for k, v in prof.items() if k in kw and k not in ("cell_imex", "cell_adapt")]
     k, v = (kernel, prof[kernel]) if kernel else max(cand, key=lambda kv: kv[1][0])
     avg_ms = v[0] / v[1]
     bound, work = kw[k]
@@ -325,13 +326,14 @@ def roofline(prof, units, hbm, tflops, src, pb=4, kernel=None):
                                else "(MEASURED_PEAKS.json absent: the pool's earlier cuBLAS measurement, 1590 TFLOP/s)")}
 
 
-# DRAM bytes per cell of a launch (ncu dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch on the 256 x 128 x 64 ODW, 2.10 M cells, with the benchmark's 64
-# z planes per block: the full 33.5 M-cell case is too large to capture under
-# the profiling rule), scaled to a launch by cells; the flux kernel's traffic
-# grows with cells (one pass; the tile halos add 3 % of reads)
-TRAFFIC_PER_CELL = {"advection": (168.854016e6 + 81.255936e6) / 2097152}
-TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on a 2.10 M-cell case, per cell, times the fluid cells"}
+# DRAM bytes of a flux launch per fluid cell (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch of k_flux_ring on the 256 x 128 x 64 ODW,
+# 2.10 M cells of which 1.30 M fluid, all-solid tiles skipped; the full
+# 33.5 M-cell case is too large to capture under the profiling rule, and the
+# kernel's traffic grows with the fluid cells): 125.7 MB read + 50.4 MB written
+TRAFFIC_PER_CELL = {"advection": (125739008 + 50361600) / 1303488}
+TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on a 2.10 M-cell case (1.30 M fluid), per fluid cell, "
+                             "times the fluid cells"}
 
 
 def fluid_cells(case, i0=0, n_loc=None):
@@ -685,6 +687,9 @@ def _case_run(dev, forms, K, W, torch, cells, units, pb, value_form, clocks_form
         profs[name] = profiled(dev, step, K)
     prof = profs[value_form]
     rf = roofline(prof, units, hbm, tfl, src, pb=pb)
+    if "cell_imex" in prof:
+        fluid = units.get("cell_rk1", cells)
+        rf["chemistry"] = chem_roofline({"imex": prof}, {}, fluid, 1, K).get("cell_imex")
     rates = {k: cells * K / (v * 1e-3) / 1e6 for k, v in timing.items()}
     return timing, profs, stats, clocks, rf, rates
 
@@ -878,12 +883,16 @@ def run_rsbi(a):
         dev.synchronize()
         b = g.bc
         fields[bits] = {n: dev.download(n)[b:-b, b:-b, b:-b].copy() for n in ("T", "P", "D", "Yi")}
+        fields[bits]["nonfinite"] = dev.status()["nonfinite_cells"]
         if bits == 32:
             rf, clocks, stats32 = r, clk, stats["fp32"]
             reset()
             e2e = run_e2e(dev, base, K, cells, torch)
         dev.close()
-    err = field_errors(fields[64], fields[32], np.ones((g.ni, g.nj, g.nk), bool), mech.species)
+    finite = np.isfinite(fields[64]["T"]) & np.isfinite(fields[32]["T"])
+    err = field_errors(fields[64], fields[32], finite, mech.species)
+    err["cells_compared"] = int(finite.sum())
+    err["nonfinite_cells"] = {"fp64": fields[64]["nonfinite"], "fp32": fields[32]["nonfinite"]}
     cb = cpu_baseline(slab=(32, 32, 8))
     return _line("Mcell-steps/s, 3D reactive shock-bubble 256^3, FP32 flux / FP64 state, IMEX", rates["fp32"], UNIT, K,
                  W, timing_all["fp32"], "f32 (reconstruction, AUSM, residual) + f64 (state, decode, chemistry)",
@@ -941,7 +950,11 @@ def run_surrogate(a):
     train_ms = (time.perf_counter() - t0) * 1e3
     feats = torch.from_numpy(np.ascontiguousarray(S.features(X, model.norm), dtype=np.float32)).cuda()
     out = torch.empty((n, 16), dtype=torch.float32, device="cuda")
-    cur = torch.cuda.current_stream()
+    # a stream of its own (the legacy default stream's handle is 0, which the
+    # library reads as "the surrogate's stream", where these events would
+    # not see the kernels)
+    cur = torch.cuda.Stream()
+    torch.cuda.synchronize()
     for _ in range(max(a.warmup, 3)):
         sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
     K = max(a.steps, 10)
@@ -978,12 +991,13 @@ def run_surrogate(a):
     host_out = torch.empty((n, 16), dtype=torch.float32).pin_memory()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(cur)
-    for _ in range(3):
-        feats.copy_(host_in, non_blocking=True)
-        sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
-        host_out.copy_(out, non_blocking=True)
-    e1.record(cur)
+    with torch.cuda.stream(cur):
+        e0.record(cur)
+        for _ in range(3):
+            feats.copy_(host_in, non_blocking=True)
+            sur.infer_device(feats.data_ptr(), n, out.data_ptr(), cur.cuda_stream)
+            host_out.copy_(out, non_blocking=True)
+        e1.record(cur)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / 3
     sur.close()

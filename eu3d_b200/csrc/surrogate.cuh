@@ -879,55 +879,78 @@ struct SurGate {
     int *acount;       // list length
 };
 
+// One block takes GATE_ROWS x rows of up to 512 cells; each thread keeps the
+// loads of its GATE_ROWS cells in flight together (the kernel is bound by
+// memory latency, not bandwidth), and the block appends its active cells
+// with one global atomic.
+constexpr int GATE_ROWS = 4, GATE_THREADS = 512;
+
 template <class P>
-__global__ void __launch_bounds__(512) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g, SurQueue qu)
+__global__ void __launch_bounds__(GATE_THREADS) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g,
+                                                           SurQueue qu)
 {
     const Layout &L = a.L;
-    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = L.bc + blockIdx.y;
-    const int k = L.bc + blockIdx.z;
-    const bool fluid = i < L.ni + L.bc && !solid_cell(a, i, j);
-    const long long c = L.at(min(i, L.ni + L.bc - 1), j, k);
-    bool frozen = false;
-    double T = 0.0;
-    if (fluid) {
-        T = a.T[c];
-        frozen = T < g.T_frozen;
-        if (frozen && g.mask) {
+    // rows of GATE_ROWS (j, k) in blockIdx.x (no 65535 limit), x chunks in blockIdx.y
+    const int i = L.bc + blockIdx.y * blockDim.x + threadIdx.x;
+    const int rows = L.nj * L.nk;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    bool fluid[GATE_ROWS], frozen[GATE_ROWS];
+    long long c[GATE_ROWS], idx[GATE_ROWS];
+    double T[GATE_ROWS];
+#pragma unroll
+    for (int m = 0; m < GATE_ROWS; m++) {
+        const int r = blockIdx.x * GATE_ROWS + m;
+        const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
+        fluid[m] = r < rows && i < L.ni + L.bc && !solid_cell(a, i, j);
+        c[m] = L.at(min(i, L.ni + L.bc - 1), min(j, L.nj + L.bc - 1), min(k, L.nk + L.bc - 1));
+        idx[m] = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+        T[m] = fluid[m] ? a.T[c[m]] : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < GATE_ROWS; m++) {
+        frozen[m] = fluid[m] && T[m] < g.T_frozen;
+        if (frozen[m] && g.mask) {
             double y = 0.0;
 #pragma unroll
             for (int s = 0; s < NS; s++)
-                if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c], 0.0);
-            frozen = y <= g.y_max;
+                if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c[m]], 0.0);
+            frozen[m] = y <= g.y_max;
         }
     }
-    const bool active = fluid && !frozen;
-    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
-    const bool audit = frozen && g.audit_stride > 0 && ((unsigned)idx % (unsigned)g.audit_stride) == 0;
-    // block-aggregated append of the active cells, in thread order: one
-    // global atomic for the list and one for the frozen count per block
-    __shared__ int wact[16], wfrz[16], base_s;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const unsigned ma = __ballot_sync(0xffffffffu, active), mf = __ballot_sync(0xffffffffu, frozen);
-    if (lane == 0) {
-        wact[w] = __popc(ma);
-        wfrz[w] = __popc(mf);
+    // block-aggregated append in (row, thread) order
+    __shared__ int wact[GATE_ROWS][GATE_THREADS / 32], base_s;
+    __shared__ unsigned long long nfrz;
+    if (threadIdx.x == 0) nfrz = 0ull;
+    unsigned ma[GATE_ROWS];
+    int myfrz = 0;
+#pragma unroll
+    for (int m = 0; m < GATE_ROWS; m++) {
+        ma[m] = __ballot_sync(0xffffffffu, fluid[m] && !frozen[m]);
+        myfrz += __popc(__ballot_sync(0xffffffffu, frozen[m]));
+        if (lane == 0) wact[m][w] = __popc(ma[m]);
     }
     __syncthreads();
+    if (lane == 0 && myfrz) atomicAdd(&nfrz, (unsigned long long)myfrz);
     if (threadIdx.x == 0) {
-        int ta = 0, tf = 0;
-        for (int v = 0; v < nw; v++) {
-            const int n = wact[v];
-            wact[v] = ta;  // exclusive offsets
-            ta += n;
-            tf += wfrz[v];
-        }
+        int ta = 0;
+        for (int m = 0; m < GATE_ROWS; m++)
+            for (int v = 0; v < nw; v++) {
+                const int n = wact[m][v];
+                wact[m][v] = ta;  // exclusive offsets
+                ta += n;
+            }
         base_s = ta ? atomicAdd(g.acount, ta) : 0;
-        if (tf) atomicAdd(&a.st->sur_frozen, (unsigned long long)tf);
     }
     __syncthreads();
-    if (active) g.active[base_s + wact[w] + __popc(ma & ((1u << lane) - 1u))] = (int)c;
-    sur_push(qu, audit, (int)((unsigned)c | SUR_FROZEN_AUDIT), T);
+    if (threadIdx.x == 0 && nfrz) atomicAdd(&a.st->sur_frozen, nfrz);
+#pragma unroll
+    for (int m = 0; m < GATE_ROWS; m++) {
+        if (fluid[m] && !frozen[m])
+            g.active[base_s + wact[m][w] + __popc(ma[m] & ((1u << lane) - 1u))] = (int)c[m];
+        const bool audit =
+            frozen[m] && g.audit_stride > 0 && ((unsigned)idx[m] % (unsigned)g.audit_stride) == 0;
+        sur_push(qu, audit, (int)((unsigned)c[m] | SUR_FROZEN_AUDIT), T[m]);
+    }
 }
 
 // Lists every fluid interior cell (the queued adaptive chemistry's work).
@@ -950,12 +973,14 @@ __global__ void __launch_bounds__(128, 7) k_sur_apply_list(SurApplyArgs s, P *__
                                                            const int *__restrict__ list, const int *__restrict__ count)
 {
     const Layout &L = s.a.L;
+    const long long total = min((long long)*count, s.n);
+    if ((long long)blockIdx.x * blockDim.x >= total) return;  // a whole block past the list
     __shared__ unsigned long long cnt[SUR_NFLAGS];
     const BlockCount<SUR_NFLAGS> bc{cnt};
     bc.init();
     const long long pos = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned flags = 0u;
-    if (pos < min((long long)*count, s.n)) {
+    if (pos < total) {
         const int plane = L.NJ * L.px;
         const int c = list[pos];
         const int k = c / plane, r = c - k * plane;

@@ -114,7 +114,8 @@ def _front_stats(Tref, Tx, per):
     return {f"front_{per}_both": int(both.sum()), f"front_{per}_one_only": int((np.isfinite(fa) ^ np.isfinite(fx)).sum()),
             "front_abs_diff_cells_median": float(np.median(d)) if d.size else None,
             "front_abs_diff_cells_p95": float(np.percentile(d, 95)) if d.size else None,
-            "front_abs_diff_cells_max": float(d.max()) if d.size else None}
+            "front_abs_diff_cells_max": float(d.max()) if d.size else None,
+            f"front_{per}_over_1_cell": int((d > 1.0).sum())}
 
 
 def accuracy(mech, model, steps, ni=512, nj=256, nk=16, cfl=0.5, runs=("adaptive_fp32", "surrogate", "imex"),
