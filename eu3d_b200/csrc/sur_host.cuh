@@ -247,8 +247,8 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
         int *acount = h->sur_count + 2;
         {
             ProfScope ps(h, "sur_gate");
-            const SurGate g{h->gate_T, h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, acount};
-            const dim3 gg((L.nj * L.nk + GATE_ROWS - 1) / GATE_ROWS, (L.ni + GATE_THREADS - 1) / GATE_THREADS);
+            const SurGate g{h->gate_T, (float)h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, acount};
+            const dim3 gg(L.nj * L.nk, (L.ni + GATE_THREADS - 1) / GATE_THREADS);
             k_sur_gate<P><<<gg, GATE_THREADS, 0, h->st>>>(cell_args(h), q, g, qu);
         }
         const SurSrcList<P> lsrc{L, h->T, q, h->scal, h->sur_out, h->sur_active, acount, n};

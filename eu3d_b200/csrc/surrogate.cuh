@@ -867,90 +867,78 @@ __global__ void __launch_bounds__(128, 7) k_sur_apply(SurApplyArgs s, P *__restr
 // its chemistry changes nothing the FP64 integrator would resolve (cold
 // H2-air ahead of the shock has ignition delays of seconds against steps of
 // tens of nanoseconds).  The other fluid cells are listed for the network.
-// Every audit_stride-th frozen cell (by interior index) is also sent to the
-// fallback queue, whose FP64 integrator records the largest temperature
-// change the gate ignored.
+// About one frozen cell in audit_stride (a fixed hash sample of the interior
+// index, gate_sample) is also sent to the fallback queue, whose FP64
+// integrator records the largest temperature change the gate ignored.
 struct SurGate {
     double T_frozen;
-    double y_max;
+    float y_max_f;  // compared with the FP32 sum of the radicals' mass fractions
     unsigned mask;
     int audit_stride;  // 0: no audit
     int *active;       // listed cells (ghosted indices)
     int *acount;       // list length
 };
 
-// One block takes GATE_ROWS x rows of up to 512 cells; each thread keeps the
-// loads of its GATE_ROWS cells in flight together (the kernel is bound by
-// memory latency, not bandwidth), and the block appends its active cells
-// with one global atomic.
-constexpr int GATE_ROWS = 4, GATE_THREADS = 512;
+// One block of GATE_THREADS threads per x row (of up to GATE_THREADS cells),
+// blocks over the (j, k) rows in blockIdx.x (no 65535 limit); the block
+// appends its active cells with one global atomic.  The kernel is bound by
+// instruction issue, so the per-cell work is kept small: the radical test in
+// FP32 (the primitives' precision of the benchmark path) and the audit
+// sample drawn by a multiplicative hash instead of a division.
+constexpr int GATE_THREADS = 512;
+
+// deterministic sample of about one cell in `stride` (Knuth's multiplicative hash)
+__device__ __forceinline__ bool gate_sample(long long idx, unsigned stride)
+{
+    return stride > 0 && (unsigned)idx * 2654435761u < 0xFFFFFFFFu / stride;
+}
 
 template <class P>
 __global__ void __launch_bounds__(GATE_THREADS) k_sur_gate(CellArgs a, const P *__restrict__ q, SurGate g,
                                                            SurQueue qu)
 {
     const Layout &L = a.L;
-    // rows of GATE_ROWS (j, k) in blockIdx.x (no 65535 limit), x chunks in blockIdx.y
     const int i = L.bc + blockIdx.y * blockDim.x + threadIdx.x;
-    const int rows = L.nj * L.nk;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    bool fluid[GATE_ROWS], frozen[GATE_ROWS];
-    long long c[GATE_ROWS], idx[GATE_ROWS];
-    double T[GATE_ROWS];
-#pragma unroll
-    for (int m = 0; m < GATE_ROWS; m++) {
-        const int r = blockIdx.x * GATE_ROWS + m;
-        const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
-        fluid[m] = r < rows && i < L.ni + L.bc && !solid_cell(a, i, j);
-        c[m] = L.at(min(i, L.ni + L.bc - 1), min(j, L.nj + L.bc - 1), min(k, L.nk + L.bc - 1));
-        idx[m] = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
-        T[m] = fluid[m] ? a.T[c[m]] : 0.0;
-    }
-#pragma unroll
-    for (int m = 0; m < GATE_ROWS; m++) {
-        frozen[m] = fluid[m] && T[m] < g.T_frozen;
-        if (frozen[m] && g.mask) {
-            double y = 0.0;
+    const int r = blockIdx.x;
+    const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
+    const bool fluid = i < L.ni + L.bc && !solid_cell(a, i, j);
+    const long long c = L.at(min(i, L.ni + L.bc - 1), j, k);
+    bool frozen = false;
+    double T = 0.0;
+    if (fluid) {
+        T = a.T[c];
+        frozen = T < g.T_frozen;
+        if (frozen && g.mask) {
+            float y = 0.f;
 #pragma unroll
             for (int s = 0; s < NS; s++)
-                if ((g.mask >> s) & 1u) y += fmax((double)q[(PY + s) * L.fs + c[m]], 0.0);
-            frozen[m] = y <= g.y_max;
+                if ((g.mask >> s) & 1u) y += fmaxf((float)q[(PY + s) * L.fs + c], 0.f);
+            frozen = y <= g.y_max_f;
         }
     }
-    // block-aggregated append in (row, thread) order
-    __shared__ int wact[GATE_ROWS][GATE_THREADS / 32], base_s;
-    __shared__ unsigned long long nfrz;
-    if (threadIdx.x == 0) nfrz = 0ull;
-    unsigned ma[GATE_ROWS];
-    int myfrz = 0;
-#pragma unroll
-    for (int m = 0; m < GATE_ROWS; m++) {
-        ma[m] = __ballot_sync(0xffffffffu, fluid[m] && !frozen[m]);
-        myfrz += __popc(__ballot_sync(0xffffffffu, frozen[m]));
-        if (lane == 0) wact[m][w] = __popc(ma[m]);
-    }
+    const bool active = fluid && !frozen;
+    __shared__ int wact[GATE_THREADS / 32], base_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned ma = __ballot_sync(0xffffffffu, active), mf = __ballot_sync(0xffffffffu, frozen);
+    __shared__ int nfrz;
+    if (threadIdx.x == 0) nfrz = 0;
+    if (lane == 0) wact[w] = __popc(ma);
     __syncthreads();
-    if (lane == 0 && myfrz) atomicAdd(&nfrz, (unsigned long long)myfrz);
+    if (lane == 0 && mf) atomicAdd(&nfrz, __popc(mf));
     if (threadIdx.x == 0) {
         int ta = 0;
-        for (int m = 0; m < GATE_ROWS; m++)
-            for (int v = 0; v < nw; v++) {
-                const int n = wact[m][v];
-                wact[m][v] = ta;  // exclusive offsets
-                ta += n;
-            }
+        for (int v = 0; v < nw; v++) {
+            const int n = wact[v];
+            wact[v] = ta;  // exclusive offsets
+            ta += n;
+        }
         base_s = ta ? atomicAdd(g.acount, ta) : 0;
     }
     __syncthreads();
-    if (threadIdx.x == 0 && nfrz) atomicAdd(&a.st->sur_frozen, nfrz);
-#pragma unroll
-    for (int m = 0; m < GATE_ROWS; m++) {
-        if (fluid[m] && !frozen[m])
-            g.active[base_s + wact[m][w] + __popc(ma[m] & ((1u << lane) - 1u))] = (int)c[m];
-        const bool audit =
-            frozen[m] && g.audit_stride > 0 && ((unsigned)idx[m] % (unsigned)g.audit_stride) == 0;
-        sur_push(qu, audit, (int)((unsigned)c[m] | SUR_FROZEN_AUDIT), T[m]);
-    }
+    if (threadIdx.x == 0 && nfrz) atomicAdd(&a.st->sur_frozen, (unsigned long long)nfrz);
+    if (active) g.active[base_s + wact[w] + __popc(ma & ((1u << lane) - 1u))] = (int)c;
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    sur_push(qu, frozen && gate_sample(idx, (unsigned)g.audit_stride), (int)((unsigned)c | SUR_FROZEN_AUDIT), T);
 }
 
 // Lists every fluid interior cell (the queued adaptive chemistry's work).

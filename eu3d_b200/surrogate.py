@@ -225,7 +225,7 @@ class SurrogateModel:
 # Frozen-chemistry gate of the coupled runs: fluid cells below 600 K whose
 # radical pool (H, O, OH, HO2, H2O2) is at most 1e-6 by mass keep their flux
 # update (cold H2-air: ignition delays of seconds at 600 K against flow steps
-# of tens of nanoseconds); every 4099th of them is re-run by the FP64
+# of tens of nanoseconds); about one in 4099 of them is re-run by the FP64
 # integrator, which records the largest temperature change ignored.
 GATE = dict(t_frozen=600.0, y_max=1e-6, species=("H", "O", "OH", "HO2", "H2O2"), audit_stride=4099)
 

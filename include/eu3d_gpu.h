@@ -460,10 +460,11 @@ int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride);
    species_mask (bit s = species s; 0: no composition test) are at most y_max
    keeps the state of its flux update and decode -- over one flow step its
    chemistry is below what the FP64 integrator resolves -- and only the other
-   cells go through the network and its apply.  Every audit_stride-th gated
-   cell (0: none) is integrated by the FP64 fallback as well, which keeps its
-   result and records the largest temperature change the gate ignored
-   (eu3d_status.frozen_audit_max_dT).  t_frozen = 0 (the default) turns the
+   cells go through the network and its apply.  The radicals' mass fractions
+   are summed in FP32.  About one gated cell in audit_stride (0: none; a
+   fixed hash sample of the interior cell index) is integrated by the FP64
+   fallback as well, which keeps its result and records the largest
+   temperature change the gate ignored (eu3d_status.frozen_audit_max_dT).  t_frozen = 0 (the default) turns the
    gate off: every fluid cell takes the network.  With the gate on, sur_fused
    is ignored. */
 int eu3d_set_surrogate_gate(eu3d_handle *h, double t_frozen, double y_max, unsigned species_mask, int audit_stride);

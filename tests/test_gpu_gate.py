@@ -102,12 +102,13 @@ def test_frozen_cells_keep_the_flux_update_and_are_audited(mech):
     (g, st, T0), (n, _, _) = res["gated"], res["stages"]
     fluid = _fluid(case)
     # the gate's decision from the state the stages leave: T below 600 K and
-    # the radicals' mass fractions (FP32 primitives, summed in FP64) <= 1e-6
-    rad = [mech.species.index(r) for r in gate["species"]]
-    yr = np.zeros(n["T"].shape)
+    # the radicals' mass fractions (FP32 primitives, summed in FP32 in species
+    # order) <= 1e-6
+    rad = sorted(mech.species.index(r) for r in gate["species"])
+    yr = np.zeros(n["T"].shape, np.float32)
     for r in rad:
-        yr = yr + np.maximum(n["Yi"][..., r], 0.0)
-    frozen = fluid & (n["T"] < gate["t_frozen"]) & (yr <= gate["y_max"])
+        yr = yr + np.maximum(n["Yi"][..., r].astype(np.float32), np.float32(0))
+    frozen = fluid & (n["T"] < gate["t_frozen"]) & (yr <= np.float32(gate["y_max"]))
     assert frozen.sum() > 0.2 * fluid.sum()
     assert st["surrogate_frozen"] == frozen.sum(), (st["surrogate_frozen"], frozen.sum())
     # every fluid cell counted once
@@ -118,8 +119,10 @@ def test_frozen_cells_keep_the_flux_update_and_are_audited(mech):
     # frozen cells keep the stages' state bit for bit (audited ones are
     # integrated by the fallback, which keeps its result)
     ni, nj, nk = case.grid.ni, case.grid.nj, case.grid.nk
-    idx = np.arange(ni * nj * nk).reshape(nk, nj, ni).transpose(2, 1, 0)
-    keep = frozen & (idx % gate["audit_stride"] != 0)
+    idx = np.arange(ni * nj * nk, dtype=np.uint64).reshape(nk, nj, ni).transpose(2, 1, 0)
+    sampled = ((idx * np.uint64(2654435761)) & np.uint64(0xFFFFFFFF)) < np.uint64(0xFFFFFFFF // gate["audit_stride"])
+    assert st["frozen_audited"] == (frozen & sampled).sum()
+    keep = frozen & ~sampled
     for f in ("CS", "T"):
         assert np.array_equal(g[f][keep], n[f][keep]), f
     assert st["nonfinite_cells"] == 0
