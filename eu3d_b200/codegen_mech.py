@@ -179,7 +179,19 @@ def gen(mech) -> str:
     w("                                                  double MD[NS])")
     w("{")
     w("    double Wi[NS];")
-    w("    const double iDi[NS] = {" + ", ".join(f"(Di[{s}] == 0.0 ? 0.0 : 1.0 / Di[{s}])" for s in range(NS)) + "};")
+    # The reference divides each term by Di (src/Reaction.cpp:798); here
+    # the term is multiplied by 1/Di.  Below 2^-1022 (a subnormal partial
+    # density, which trace species reach in cold air) 1/Di overflows, so such a
+    # Di is scaled by 2^64 and its numerator with it: both scalings are exact,
+    # and a normal Di keeps the scale 1.
+    w("    // 1/Di, with a subnormal Di (and its numerator) scaled by 2^64 so that the")
+    w("    // reciprocal stays finite; the scalings are exact")
+    w("    double iDi[NS], sDi[NS];")
+    w("#pragma unroll")
+    w("    for (int s = 0; s < NS; s++) {")
+    w("        sDi[s] = fabs(Di[s]) < 0x1p-1022 ? 0x1p+64 : 1.0;")
+    w("        iDi[s] = Di[s] == 0.0 ? 0.0 : 1.0 / (Di[s] * sDi[s]);")
+    w("    }")
     w("    const double tdep = 1.0 / (RU_CAL * (p.T * p.T));")
     w("#pragma unroll")
     w("    for (int s = 0; s < NS; s++) { Wi[s] = 0.0; MD[s] = 0.0; }")
@@ -207,7 +219,7 @@ def gen(mech) -> str:
             if wj.startswith("- "):
                 wj = "-" + wj[2:]
             tbterm = f" + rr * {lit(tb[s, r] / mech.mw[s])}" if tb[s, r] != 0 else ""
-            w(f"        MD[{s}] += {lit(nu)} * ((({wj}) * iDi[{s}] + wjh2 * PT[{s}]) * tb{tbterm});")
+            w(f"        MD[{s}] += {lit(nu)} * (((({wj}) * sDi[{s}]) * iDi[{s}] + wjh2 * PT[{s}]) * tb{tbterm});")
         w("    }")
     w("#pragma unroll")
     w("    for (int s = 0; s < NS; s++) {")

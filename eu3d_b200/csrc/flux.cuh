@@ -110,6 +110,22 @@ __device__ __forceinline__ float recon_right<float, EU3D_DIFF_MUSCL2>(float b, f
 __device__ __forceinline__ double pdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float pdiv(float a, float b) { return __fdividef(a, b); }
 
+// the hardware's approximate reciprocal square root and reciprocal (PTX
+// rsqrt.approx / rcp.approx, subnormals flushed: the FP32 flux never meets
+// them in a sound speed)
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Upwind-side MUSCL_2 state in one formula for both sides, FP32.  For the
 // left state pass (far, ctr, oth) = f(a-1), f(a), f(a+1) and seps = +1e-12;
 // for the right state f(a+2), f(a+1), f(a) and seps = -1e-12.  Negating both
@@ -149,10 +165,16 @@ __device__ __forceinline__ void face_flux_src(const Src &src, bool zspec, float 
     both(PP, PL, PR);
     both(PG, GL, GR);
     both(FN, NL, NR);
-    const float CL = sqrtf(__fdividef(__fmul_rn(GL, PL), DL));
-    const float CR = sqrtf(__fdividef(__fmul_rn(GR, PR), DR));
+    // sound speeds sqrt(g p / D) = x rsqrt(x D) with x = g p: one approximate
+    // reciprocal square root (relative error below 2^-22) in place of a
+    // division and a correctly rounded square root with its special-case
+    // path; one reciprocal of CI serves both Mach numbers
+    const float xL = __fmul_rn(GL, PL), xR = __fmul_rn(GR, PR);
+    const float CL = __fmul_rn(xL, rsqrt_approx(__fmul_rn(xL, DL)));
+    const float CR = __fmul_rn(xR, rsqrt_approx(__fmul_rn(xR, DR)));
     const float CI = __fmul_rn(0.5f, CL + CR);
-    const float MaL = __fdividef(NL, CI), MaR = __fdividef(NR, CI);
+    const float rCI = rcp_approx(CI);
+    const float MaL = __fmul_rn(NL, rCI), MaR = __fmul_rn(NR, rCI);
     // both branches of the split Mach numbers are evaluated and one is
     // selected (the unused one may divide by ~0; its result is dropped)
     float B1, G1, B2, G2;
@@ -500,8 +522,11 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
 //    primitives, 27 KB) arrives by one TMA box load into a ring of three
 //    shared-memory buffers: while plane c is processed, planes c and c+1 are
 //    resident and c+2 is in flight, so no thread computes load addresses;
-//  * a z face reads cells c and c+1 from the ring and only c-1 and c+2 from
-//    global memory (L2);
+//  * the ring holds planes c, c+1 and c+2 while plane c is processed (c+2
+//    is copied during the plane before and waited for only after the x and
+//    y faces, which need plane c alone), and each thread keeps its own cell
+//    of plane c-1 in a private shared-memory slot, so the z face above the
+//    cell reads its four cells c-1 .. c+2 from shared memory;
 //  * a cell's right x face is its right neighbour's left face, passed by a
 //    warp shuffle (row ends through shared memory from the face warp);
 //  * the upwind side is reconstructed without branches (face_flux_src).
@@ -513,25 +538,28 @@ struct FluxRing {
     static constexpr uint32_t PLANE_BYTES = PLANE * 4;  // bytes of one TMA box (27648)
     static constexpr int FY = (FR_TY + 1) * FT_X * NV;  // y-face fluxes
     static constexpr int FXE = FR_TY * NV;              // the last x face of each row
-    static constexpr size_t BYTES = FR_NBUF * PLANE_BYTES + 4 * (FY + FXE) + 8 * FR_NBUF;
-    static constexpr size_t SMEM = BYTES + 1024;        // slack to align the ring to 1 KB
+    static constexpr int CORE = NPRIM * FT_X * FR_TY;   // each cell thread's cell of plane c-1
+    static constexpr size_t BYTES = FR_NBUF * PLANE_BYTES + 4 * (FY + FXE + CORE) + 8 * FR_NBUF;
+    // slack to align the ring to 128 B; two blocks (with the 1 KB the
+    // hardware reserves for each) fit the SM's 228 KB
+    static constexpr size_t SMEM = BYTES + 128;
     // TMA box {x, y, z, field}
     static constexpr unsigned BOX[4] = {FR_HX, FR_HY, 1, NPRIM};
 };
 
-// Source of the z face between planes c and c+1 of one column: cells c-1
-// and c+2 from global memory, c and c+1 from the ring.
+// Source of the z face between planes c and c+1 of one column: cell c-1
+// from the thread's private slot (fields FT_X * FR_TY floats apart), c, c+1
+// and c+2 from the ring.
 struct ZSrc {
-    const float *gm, *gp;  // cell (i, j, c-1) and (i, j, c+2), field 0
-    const float *sc, *sn;  // the cell in the staged planes c and c+1, field 0
-    int fs;                // global field stride
+    const float *cm;          // the cell of plane c-1, field 0
+    const float *sc, *sn, *sp;  // the cell in the staged planes c, c+1, c+2, field 0
     __device__ __forceinline__ float v(int f, int n) const
     {
-        return n == 0 ? __ldg(gm + f * fs) : n == 1 ? sc[f * FR_PL] : n == 2 ? sn[f * FR_PL] : __ldg(gp + f * fs);
+        return n == 0 ? cm[f * (FT_X * FR_TY)] : n == 1 ? sc[f * FR_PL] : n == 2 ? sn[f * FR_PL] : sp[f * FR_PL];
     }
     __device__ __forceinline__ void up3(int f, bool left, float &far, float &ctr, float &oth) const
     {
-        far = __ldg((left ? gm : gp) + f * fs);
+        far = left ? cm[f * (FT_X * FR_TY)] : sp[f * FR_PL];
         ctr = (left ? sc : sn)[f * FR_PL];
         oth = (left ? sn : sc)[f * FR_PL];
     }
@@ -547,11 +575,12 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     constexpr int TY = FR_TY, HX = FR_HX, PL = FR_PL;
     extern __shared__ unsigned char fr_raw[];
     const uint32_t raw_s = tc::smem_u32(fr_raw);
-    float *ring = reinterpret_cast<float *>(fr_raw + (((raw_s + 1023u) & ~1023u) - raw_s));
+    float *ring = reinterpret_cast<float *>(fr_raw + (((raw_s + 127u) & ~127u) - raw_s));
     auto fy = reinterpret_cast<float(*)[FT_X][NV]>(ring + FR_NBUF * FluxRing::PLANE);
     auto fxe = reinterpret_cast<float(*)[NV]>(ring + FR_NBUF * FluxRing::PLANE + FluxRing::FY);
+    float *core = ring + FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE;
     const uint32_t ring_s = tc::smem_u32(ring);
-    const uint32_t mb_s = ring_s + 4u * (FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE);
+    const uint32_t mb_s = ring_s + 4u * (FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE + FluxRing::CORE);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FT_X + tx;
     const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
     const int kb = L.bc + blockIdx.z * kz;
@@ -563,9 +592,10 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     // an all-solid tile leaves before its barriers and copies exist
     if (!__syncthreads_or(act && !wedge.solid(xn[i], yn[j]))) return;
     const int fs = (int)L.fs, sz = L.px * L.NJ;
-    // plane kb + p into buffer p % 3; the block loads planes kb .. kb + np
-    // (the last one only feeds the top z face).  x = i0 - 2 = 32 blockIdx.x
-    // keeps the box start on a 16-byte boundary.
+    // plane kb + p into buffer p % 3; the block loads planes kb .. kb + np + 1
+    // (the last two only feed the top z face; kb + np + 1 <= nk + bc + 1 is
+    // the last ghost plane).  x = i0 - 2 = 32 blockIdx.x keeps the box start
+    // on a 16-byte boundary.
     auto issue = [&](int p) {
         const uint32_t b = (uint32_t)(p % FR_NBUF);
         tc::mbar_expect_tx(mb_s + 8u * b, FluxRing::PLANE_BYTES);
@@ -576,7 +606,7 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         tc::fence_mbar_init();
     }
     __syncthreads();
-    int issued = min(FR_NBUF, np + 1);
+    int issued = min(FR_NBUF, np + 2);
     if (tid == 0)
         for (int p = 0; p < issued; p++) issue(p);
     const double dt = *dtp;
@@ -586,28 +616,30 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     float qb[NV], qa[NV], fo[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) qb[v] = qa[v] = fo[v] = 0.f;
-    // the z face below the first plane, from global memory
-    if (act) face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
-    const float *gcol = q + (act ? L.at(i, j, kb) : 0);
+    // the z face below the first plane from global memory, and the cell of
+    // plane kb - 1 into the thread's slot
+    float *slot = core + (cellw ? tid : 0);
+    if (act) {
+        face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
+        const float *g = q + L.at(i, j, kb) - sz;
+#pragma unroll
+        for (int f = 0; f < NPRIM; f++) slot[f * (FT_X * FR_TY)] = __ldg(g + (long long)f * fs);
+    }
     const int so = (ty + 2) * HX + tx + 2;  // the cell inside a staged field plane
     bool ok = true;
     int p = 0;
     for (; p < np; p++) {
-        const int b0 = p % FR_NBUF, b1 = (p + 1) % FR_NBUF;
+        const int b0 = p % FR_NBUF, b1 = (p + 1) % FR_NBUF, b2 = (p + 2) % FR_NBUF;
         if (p == 0) ok = tc::mbar_wait(mb_s + 8u * b0, 0, wait_tries) && ok;
         ok = tc::mbar_wait(mb_s + 8u * b1, ((p + 1) / FR_NBUF) & 1, wait_tries) && ok;
         const float *S0 = ring + b0 * FluxRing::PLANE, *S1 = ring + b1 * FluxRing::PLANE;
+        const float *S2 = ring + b2 * FluxRing::PLANE;
         const int k = kb + p;
         // y face g = ty of column i, between b = j0+g-1 and b+1 (staged rows
         // g .. g+3): faces 0..7 by the cell warps, face 8 by warp TY
         if (ty <= TY && i <= ilast && j0 + ty - 1 <= jlast)
             face_flux_src<2, DIFF>(StridedSrc<false>{S0 + ty * HX + tx + 2, PL, HX}, species_quirk && i >= L.ni,
                                    fy[ty][tx]);
-        // z face above the cell (between planes k and k+1)
-        if (act) {
-            const ZSrc zsrc{gcol + (long long)(p - 1) * sz, gcol + (long long)(p + 2) * sz, S0 + so, S1 + so, fs};
-            face_flux_src<3, DIFF>(zsrc, zs_cell, qa);
-        }
         // x face f of row r, between a = i0+f-1 and a+1 (staged columns
         // f .. f+3): f = tx by the cell warps, f = 32 of row tx by warp TY+1
         {
@@ -621,6 +653,15 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
 #pragma unroll
                     for (int v = 0; v < NV; v++) fxe[r][v] = fo[v];
             }
+        }
+        // z face above the cell (between planes k and k+1): plane k+2 was
+        // copied during the previous plane; then the cell of plane k replaces
+        // that of plane k-1 in the slot
+        ok = tc::mbar_wait(mb_s + 8u * b2, ((p + 2) / FR_NBUF) & 1, wait_tries) && ok;
+        if (act) {
+            face_flux_src<3, DIFF>(ZSrc{slot, S0 + so, S1 + so, S2 + so}, zs_cell, qa);
+#pragma unroll
+            for (int f = 0; f < NPRIM; f++) slot[f * (FT_X * FR_TY)] = S0[so + f * PL];
         }
         if (__syncthreads_or(!ok)) break;
         if (cellw) {
@@ -641,7 +682,7 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
             }
         }
         __syncthreads();
-        if (p + FR_NBUF <= np) {
+        if (p + FR_NBUF <= np + 1) {
             if (tid == 0) issue(p + FR_NBUF);
             issued++;
         }

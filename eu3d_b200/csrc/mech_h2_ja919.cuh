@@ -184,7 +184,14 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
                                                   double MD[NS])
 {
     double Wi[NS];
-    const double iDi[NS] = {(Di[0] == 0.0 ? 0.0 : 1.0 / Di[0]), (Di[1] == 0.0 ? 0.0 : 1.0 / Di[1]), (Di[2] == 0.0 ? 0.0 : 1.0 / Di[2]), (Di[3] == 0.0 ? 0.0 : 1.0 / Di[3]), (Di[4] == 0.0 ? 0.0 : 1.0 / Di[4]), (Di[5] == 0.0 ? 0.0 : 1.0 / Di[5]), (Di[6] == 0.0 ? 0.0 : 1.0 / Di[6]), (Di[7] == 0.0 ? 0.0 : 1.0 / Di[7]), (Di[8] == 0.0 ? 0.0 : 1.0 / Di[8])};
+    // 1/Di, with a subnormal Di (and its numerator) scaled by 2^64 so that the
+    // reciprocal stays finite; the scalings are exact
+    double iDi[NS], sDi[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        sDi[s] = fabs(Di[s]) < 0x1p-1022 ? 0x1p+64 : 1.0;
+        iDi[s] = Di[s] == 0.0 ? 0.0 : 1.0 / (Di[s] * sDi[s]);
+    }
     const double tdep = 1.0 / (RU_CAL * (p.T * p.T));
 #pragma unroll
     for (int s = 0; s < NS; s++) { Wi[s] = 0.0; MD[s] = 0.0; }
@@ -201,13 +208,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.b5be07fcb923ap+15 * tdep);
         Wi[0] += 0x1.0000000000000p+0 * tb * rr;
-        MD[0] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[4] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[4] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[4] + wjh2 * PT[4]) * tb);
+        MD[4] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb);
         Wi[5] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[5] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[5] + wjh2 * PT[5]) * tb);
+        MD[5] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[5]) * iDi[5] + wjh2 * PT[5]) * tb);
         Wi[7] += 0x1.0000000000000p+0 * tb * rr;
-        MD[7] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 2
@@ -222,13 +229,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.06a537e90ff97p+14 * tdep);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[1] += 0x1.0000000000000p+0 * tb * rr;
-        MD[1] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[3] += 0x1.0000000000000p+0 * tb * rr;
-        MD[3] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[4] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[4] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[4] + wjh2 * PT[4]) * tb);
+        MD[4] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb);
     }
     {
         // reaction 3
@@ -243,13 +250,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.0000000000000p+0 * p.tm1 + 0x1.1647837b4a234p+13 * tdep);
         Wi[0] += 0x1.0000000000000p+0 * tb * rr;
-        MD[0] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[1] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[1] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[3] += 0x1.0000000000000p+0 * tb * rr;
-        MD[3] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[5] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[5] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[5] + wjh2 * PT[5]) * tb);
+        MD[5] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[5]) * iDi[5] + wjh2 * PT[5]) * tb);
     }
     {
         // reaction 4
@@ -264,13 +271,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.420d8e8a71de7p+12 * tdep);
         Wi[0] += 0x1.0000000000000p+0 * tb * rr;
-        MD[0] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb);
         Wi[3] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[3] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[5] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[5] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[5] + wjh2 * PT[5]) * tb);
+        MD[5] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[5]) * iDi[5] + wjh2 * PT[5]) * tb);
     }
     {
         // reaction 5
@@ -285,11 +292,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.10a6b1c432ca5p+10 * tdep);
         Wi[1] += 0x1.0000000000000p+0 * tb * rr;
-        MD[1] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb);
         Wi[3] += (-0x1.0000000000000p+1) * tb * rr;
-        MD[3] += (-0x1.0000000000000p+1) * (((kf * 0x1.0000000000000p+1 * rf) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += (-0x1.0000000000000p+1) * ((((kf * 0x1.0000000000000p+1 * rf) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
     }
     {
         // reaction 6
@@ -304,11 +311,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * ((-0x1.0000000000000p+1) * p.tm1);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb + rr * 0x1.550b381dd224bp-2);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb + rr * 0x1.550b381dd224bp-2);
         Wi[3] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[3] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
+        MD[3] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
     }
     {
         // reaction 7
@@ -323,9 +330,9 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * ((-0x1.0000000000000p+0) * p.tm1);
         Wi[0] += (-0x1.0000000000000p+1) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+1) * (((kf * 0x1.0000000000000p+1 * rf) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
+        MD[0] += (-0x1.0000000000000p+1) * ((((kf * 0x1.0000000000000p+1 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
         Wi[5] += 0x1.0000000000000p+0 * tb * rr;
-        MD[5] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[5] + wjh2 * PT[5]) * tb + rr * 0x1.fbf77c89c7e90p-1);
+        MD[5] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[5]) * iDi[5] + wjh2 * PT[5]) * tb + rr * 0x1.fbf77c89c7e90p-1);
     }
     {
         // reaction 8
@@ -340,11 +347,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * ((-0x1.3333333333333p-1) * p.tm1);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
         Wi[1] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[1] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[1] + wjh2 * PT[1]) * tb + rr * 0x1.0002752b5049bp-4);
+        MD[1] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb + rr * 0x1.0002752b5049bp-4);
         Wi[3] += 0x1.0000000000000p+0 * tb * rr;
-        MD[3] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
+        MD[3] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
     }
     {
         // reaction 9
@@ -359,11 +366,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * ((-0x1.f446e2eb1c433p+9) * tdep);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb + rr * 0x1.fbf77c89c7e90p-1);
         Wi[4] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[4] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[4] + wjh2 * PT[4]) * tb + rr * 0x1.0002752b5049bp-5);
+        MD[4] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb + rr * 0x1.0002752b5049bp-5);
         Wi[7] += 0x1.0000000000000p+0 * tb * rr;
-        MD[7] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[7] + wjh2 * PT[7]) * tb + rr * 0x1.f0622ad29be6cp-6);
+        MD[7] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb + rr * 0x1.f0622ad29be6cp-6);
     }
     {
         // reaction 10
@@ -378,9 +385,9 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * ((-0x1.c23fcd35a8588p+10) * tdep);
         Wi[1] += (-0x1.0000000000000p+1) * tb * rr;
-        MD[1] += (-0x1.0000000000000p+1) * (((kf * 0x1.0000000000000p+1 * rf) * iDi[1] + wjh2 * PT[1]) * tb + rr * 0x1.0002752b5049bp-4);
+        MD[1] += (-0x1.0000000000000p+1) * ((((kf * 0x1.0000000000000p+1 * rf) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb + rr * 0x1.0002752b5049bp-4);
         Wi[4] += 0x1.0000000000000p+0 * tb * rr;
-        MD[4] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[4] + wjh2 * PT[4]) * tb + rr * 0x1.0002752b5049bp-5);
+        MD[4] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb + rr * 0x1.0002752b5049bp-5);
     }
     {
         // reaction 11
@@ -395,11 +402,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.0e25c5d638866p+10 * tdep);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[3] += 0x1.0000000000000p+1 * tb * rr;
-        MD[3] += 0x1.0000000000000p+1 * (((-kb * 0x1.0000000000000p+1 * rb) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += 0x1.0000000000000p+1 * ((((-kb * 0x1.0000000000000p+1 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[7] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[7] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 12
@@ -414,13 +421,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.0e25c5d638866p+10 * tdep);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[1] += 0x1.0000000000000p+0 * tb * rr;
-        MD[1] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb);
         Wi[7] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[7] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 13
@@ -435,13 +442,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.db42b367a0f91p+9 * tdep);
         Wi[1] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[1] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[3] += 0x1.0000000000000p+0 * tb * rr;
-        MD[3] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[4] += 0x1.0000000000000p+0 * tb * rr;
-        MD[4] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[4] + wjh2 * PT[4]) * tb);
+        MD[4] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb);
         Wi[7] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[7] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 14
@@ -456,13 +463,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0.0);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb);
         Wi[3] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[3] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[4] += 0x1.0000000000000p+0 * tb * rr;
-        MD[4] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[4] + wjh2 * PT[4]) * tb);
+        MD[4] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb);
         Wi[7] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[7] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 15
@@ -477,11 +484,11 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0.0);
         Wi[4] += 0x1.0000000000000p+0 * tb * rr;
-        MD[4] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[4] + wjh2 * PT[4]) * tb);
+        MD[4] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[4]) * iDi[4] + wjh2 * PT[4]) * tb);
         Wi[6] += 0x1.0000000000000p+0 * tb * rr;
-        MD[6] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[6] + wjh2 * PT[6]) * tb);
+        MD[6] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[6]) * iDi[6] + wjh2 * PT[6]) * tb);
         Wi[7] += (-0x1.0000000000000p+1) * tb * rr;
-        MD[7] += (-0x1.0000000000000p+1) * (((kf * 0x1.0000000000000p+1 * rf) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += (-0x1.0000000000000p+1) * ((((kf * 0x1.0000000000000p+1 * rf) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 16
@@ -496,13 +503,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.c23fcd35a8588p+11 * tdep);
         Wi[0] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[0] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[0] + wjh2 * PT[0]) * tb);
+        MD[0] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[0]) * iDi[0] + wjh2 * PT[0]) * tb);
         Wi[5] += 0x1.0000000000000p+0 * tb * rr;
-        MD[5] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[5] + wjh2 * PT[5]) * tb);
+        MD[5] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[5]) * iDi[5] + wjh2 * PT[5]) * tb);
         Wi[6] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[6] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[6] + wjh2 * PT[6]) * tb);
+        MD[6] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[6]) * iDi[6] + wjh2 * PT[6]) * tb);
         Wi[7] += 0x1.0000000000000p+0 * tb * rr;
-        MD[7] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 17
@@ -517,13 +524,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.9038b6ae7d567p+12 * tdep);
         Wi[1] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[1] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[1] + wjh2 * PT[1]) * tb);
+        MD[1] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[1]) * iDi[1] + wjh2 * PT[1]) * tb);
         Wi[3] += 0x1.0000000000000p+0 * tb * rr;
-        MD[3] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[6] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[6] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[6] + wjh2 * PT[6]) * tb);
+        MD[6] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[6]) * iDi[6] + wjh2 * PT[6]) * tb);
         Wi[7] += 0x1.0000000000000p+0 * tb * rr;
-        MD[7] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 18
@@ -538,13 +545,13 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.65b3212d77319p+10 * tdep);
         Wi[2] += 0x1.0000000000000p+0 * tb * rr;
-        MD[2] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[2] + wjh2 * PT[2]) * tb);
+        MD[2] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[2]) * iDi[2] + wjh2 * PT[2]) * tb);
         Wi[3] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[3] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[3] + wjh2 * PT[3]) * tb);
+        MD[3] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb);
         Wi[6] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[6] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[6] + wjh2 * PT[6]) * tb);
+        MD[6] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[6]) * iDi[6] + wjh2 * PT[6]) * tb);
         Wi[7] += 0x1.0000000000000p+0 * tb * rr;
-        MD[7] += 0x1.0000000000000p+0 * (((-kb * 0x1.0000000000000p+0 * rb) * iDi[7] + wjh2 * PT[7]) * tb);
+        MD[7] += 0x1.0000000000000p+0 * ((((-kb * 0x1.0000000000000p+0 * rb) * sDi[7]) * iDi[7] + wjh2 * PT[7]) * tb);
     }
     {
         // reaction 19
@@ -559,9 +566,9 @@ __device__ __forceinline__ void diagonalized_spec(const TPow &p, const double G[
         const double rr = kf * rf - kb * rb;
         const double wjh2 = rr * (0x1.63aa6b923a29cp+15 * tdep);
         Wi[3] += 0x1.0000000000000p+1 * tb * rr;
-        MD[3] += 0x1.0000000000000p+1 * (((-kb * 0x1.0000000000000p+1 * rb) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
+        MD[3] += 0x1.0000000000000p+1 * ((((-kb * 0x1.0000000000000p+1 * rb) * sDi[3]) * iDi[3] + wjh2 * PT[3]) * tb + rr * 0x1.e1aca45c4cb5ep-5);
         Wi[6] += (-0x1.0000000000000p+0) * tb * rr;
-        MD[6] += (-0x1.0000000000000p+0) * (((kf * 0x1.0000000000000p+0 * rf) * iDi[6] + wjh2 * PT[6]) * tb + rr * 0x1.e1aca45c4cb5ep-6);
+        MD[6] += (-0x1.0000000000000p+0) * ((((kf * 0x1.0000000000000p+0 * rf) * sDi[6]) * iDi[6] + wjh2 * PT[6]) * tb + rr * 0x1.e1aca45c4cb5ep-6);
     }
 #pragma unroll
     for (int s = 0; s < NS; s++) {

@@ -130,6 +130,73 @@ def test_chemistry_call_parity(mech, quirks, react, typ):
         assert np.array_equal(interior(d.download("Nchem")), interior(o.view("Nchem")).astype(np.float64))
 
 
+SUBNORMAL = ((0, 5e-320), (3, 2e-306), (6, 3e-310), (7, 1.1e-309))  # (species, partial density kg/m^3)
+
+
+def _subnormal_traces(o, rng):
+    """Cells whose H, OH, H2O2 and HO2 partial densities are subnormal once
+    in g/cm^3 (below 2^-1022 after the factor 1e-3): the state that cold air
+    ahead of a reaction front reaches after a few chemistry calls.  The
+    oracle's state is decoded again (its partial densities, concentrations
+    and temperature derivatives are the previous decode's)."""
+    cs = o.view("CS")
+    sl = (slice(2, 9), slice(2, 6), slice(2, 5))
+    for s, v in SUBNORMAL:
+        cs[sl + (s,)] = v * rng.uniform(0.5, 2.0, cs[sl + (s,)].shape)
+    o.update_after_cs()
+    o.partial_t()
+    return sl
+
+
+def test_chemistry_with_subnormal_trace_species(mech):
+    """The implicit diagonal divides each term by the species' partial density
+    Di (src/Reaction.cpp:798), which the specialised kernels multiply by 1/Di
+    instead: for a subnormal Di that reciprocal overflows unless it is scaled.
+    One IMEX call on cold cells with subnormal radicals: finite, and equal to
+    the oracle within 1e-10 per variable.  The FP64 adaptive chemistry (same
+    diagonal) on those cells: finite, and close to the state reached with
+    those radicals raised by 2^60 into the normal range (each diagonal term is
+    the rate over Di with the rate proportional to Di, continuous as Di goes
+    to zero from above; but products of subnormal concentrations lose digits
+    or underflow to zero, so the two runs agree only to about 1e-8)."""
+    from eu3d_b200 import surrogate as S
+    rng = np.random.default_rng(62)
+    o, g = make_oracle(mech, seed=61, quirks=QUIRKS_FIXED, tlo=450.0, thi=700.0, radicals=1e-6)
+    sl = _subnormal_traces(o, rng)
+    d = to_gpu(o, g, QUIRKS_FIXED)
+    for x in (o, d):
+        x.boundary(gpu.BC_RSBI)
+        x.dt = 2e-7
+        x.advection(0, 1)
+        x.imex()
+    T = d.download("T")
+    assert np.all(np.isfinite(interior(T))) and d.status()["nonfinite_cells"] == 0
+    assert np.max(np.abs(T[sl] / o.view("T")[sl] - 1.0)) < 1e-12
+    e, errs = worst(d, o)
+    assert e < TOL_FN * 100, errs
+    d.close()
+
+    out = []
+    for raise_ in (False, True):
+        o, g = make_oracle(mech, seed=61, quirks=QUIRKS_FIXED, tlo=1100.0, thi=1400.0, radicals=1e-6)
+        sl = _subnormal_traces(o, np.random.default_rng(62))
+        if raise_:
+            for s, _ in SUBNORMAL:
+                o.view("CS")[sl + (s,)] *= 2.0 ** 60
+        d = to_gpu(o, g, QUIRKS_FIXED)
+        d.upload("RHS", np.zeros(d.shape("RHS")))
+        d.set_elements(S.atoms_matrix(mech))
+        d.dt = 2e-7
+        d.react_adaptive()
+        assert d.status()["nonfinite_cells"] == 0
+        out.append({f: interior(d.download(f)) for f in ("CS", "T", "P")})
+        d.close()
+    errs = {f: rel_err(out[0][f], out[1][f]) for f in ("CS", "T", "P")}
+    for f in ("CS", "T", "P"):
+        assert np.all(np.isfinite(out[0][f])), f
+    assert errs["CS"] < 1e-6 and errs["T"] < 1e-8 and errs["P"] < 1e-8, errs
+
+
 @pytest.mark.parametrize("quirks", [QUIRKS_FIXED, QUIRKS_REF], ids=["fixed", "ref"])
 def test_cfl_parity(mech, quirks):
     o, g = make_oracle(mech, seed=8, quirks=quirks, **policy(quirks))

@@ -18,9 +18,9 @@ from pyoracle import Oracle, RefCase, copy_state
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
-REF_INPUT = os.environ.get("EU3D_REF", "/root/reference") + "/input"
-
 import golden.make_golden as mg  # noqa: E402
+
+REF_INPUT = os.path.join(mg.REF_DIR, "input")  # the reference's input tables, when its tree is present
 
 
 @pytest.mark.parametrize("case", mg.CASES, ids=[c[0] for c in mg.CASES])
