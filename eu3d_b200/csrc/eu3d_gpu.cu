@@ -391,8 +391,12 @@ void launch_adv_t(eu3d_handle *h)
         if (h->flux_stage == 2 && h->tq_ok) {
             dim3 gs((L.ni + FT_X - 1) / FT_X, (L.nj + FR_TY - 1) / FR_TY, (L.nk + kz - 1) / kz);
             dim3 bs(FT_X, FR_TY + 2);
-            k_flux_ring<DIFF><<<gs, bs, FluxRing::SMEM, h->st>>>(h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs,
-                                                                 sq, kz, h->status, wedge, h->wait_tries);
+            if (sq)
+                k_flux_ring<DIFF, true><<<gs, bs, FluxRing::SMEM, h->st>>>(
+                    h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs, kz, h->status, wedge, h->wait_tries);
+            else
+                k_flux_ring<DIFF, false><<<gs, bs, FluxRing::SMEM, h->st>>>(
+                    h->tq, L, qf, h->xn, h->yn, h->zn, h->scal, (float *)h->rhs, kz, h->status, wedge, h->wait_tries);
             return;
         }
         if (h->flux_stage) {
@@ -423,9 +427,10 @@ void launch_adv(eu3d_handle *h, int diff)
 template <int DIFF>
 void flux_attributes()
 {
-    cudaFuncSetAttribute(k_flux_ring<DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FluxRing::SMEM);
-    cudaFuncSetAttribute(k_flux_ring<DIFF>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         (int)cudaSharedmemCarveoutMaxShared);
+    for (auto k : {k_flux_ring<DIFF, false>, k_flux_ring<DIFF, true>}) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FluxRing::SMEM);
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+    }
     cudaFuncSetAttribute(k_flux_stage<DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FluxStage::SMEM);
     cudaFuncSetAttribute(k_flux_tile<float, DIFF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)FluxTile<float>::SMEM);

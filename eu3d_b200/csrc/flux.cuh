@@ -516,61 +516,202 @@ __global__ void __launch_bounds__(FT_X *(FS_TY + 2), 2) k_flux_stage(
     }
 }
 
-// FP32 flux kernel fed by TMA.  Same tile (32 x 8 cells plus two face
-// warps), face ownership and residual order as k_flux_stage.  Differences:
+// FP32 flux kernel fed by TMA (k_flux_ring).  Same tile (32 x 8 cells plus
+// two face warps), face ownership and residual order as k_flux_stage.
+// Differences:
 //  * each z plane of the tile with its two-cell halo (36 x 12 cells x 16
 //    primitives, 27 KB) arrives by one TMA box load into a ring of three
 //    shared-memory buffers: while plane c is processed, planes c and c+1 are
-//    resident and c+2 is in flight, so no thread computes load addresses;
-//  * the ring holds planes c, c+1 and c+2 while plane c is processed (c+2
-//    is copied during the plane before and waited for only after the x and
-//    y faces, which need plane c alone), and each thread keeps its own cell
-//    of plane c-1 in a private shared-memory slot, so the z face above the
-//    cell reads its four cells c-1 .. c+2 from shared memory;
+//    resident and c+2 is resident or in flight (it is waited for only after
+//    the x and y faces, which need plane c alone), so no thread computes
+//    load addresses;
+//  * each cell thread keeps its own cell of plane c-1 in a private
+//    shared-memory slot, so the z face above the cell reads its four cells
+//    c-1 .. c+2 from shared memory;
 //  * a cell's right x face is its right neighbour's left face, passed by a
 //    warp shuffle (row ends through shared memory from the face warp);
-//  * the upwind side is reconstructed without branches (face_flux_src).
+//  * faces are evaluated by face_flux_pk: the left/right pairs of the AUSM
+//    arithmetic, two upwind fields at a time, the species fluxes and the
+//    residual in packed FP32 pairs, the upwind side picked by pointer
+//    selection, not branches -- bit for bit face_flux_src's result;
+//  * the cell warps evaluate their three faces with no per-lane condition
+//    (lanes past a ragged tile edge compute on staged values and store
+//    nothing), so the faces share one basic block;
+//  * dt/dz of the next plane is formed by one thread of the y-face warp
+//    while the others work (two-entry buffer); the species-face quirk is a
+//    template switch (SQ), so the default build carries no test for it.
 // Every wait on the ring is bounded: when one runs out the block counts a
 // timeout in the status, waits (bounded) for its copies in flight and stops.
 constexpr int FR_TY = 8, FR_HX = FT_X + 4, FR_HY = FR_TY + 4, FR_PL = FR_HX * FR_HY, FR_NBUF = 3;
+constexpr int FR_CS = FT_X * FR_TY;  // field stride of the plane c-1 slots
+
+// Packed FP32 pairs: Blackwell's two-lane add, multiply and fused
+// multiply-add (CUDA's __fadd2_rn / __fmul2_rn / __ffma2_rn).  Each lane is
+// rounded once, to nearest, exactly as the scalar __fadd_rn / __fmul_rn /
+// __fmaf_rn of the same operands; a - b is fma(b, -1, a), the exact a - b
+// rounded once, as the scalar subtraction.
+__device__ __forceinline__ float2 pk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// up_muscl2 of two fields on the same side at once: lane by lane the scalar
+// up_muscl2 (differences, epsilon, product and the final fma in pairs; the
+// comparisons and selections per lane)
+__device__ __forceinline__ float2 up_muscl2_x2(float2 far, float2 ctr, float2 oth, float2 seps)
+{
+    const float2 A0 = sub2(ctr, far), A1 = sub2(oth, ctr);
+    const float2 d = add2(A0, seps);
+    const float2 pr = mul2(A1, d);
+    const float2 h = pk(fabsf(A1.x) >= fabsf(d.x) ? A0.x : A1.x, fabsf(A1.y) >= fabsf(d.y) ? A0.y : A1.y);
+    const float2 r = fma2(pk(0.5f, 0.5f), h, ctr);
+    return pk(pr.x > 0.f ? r.x : ctr.x, pr.y > 0.f ? r.y : ctr.y);
+}
+
+// The upwind triple of a face (cells far, ctr, oth of field 0), chosen once
+// per face; the fields follow at FR_PL floats (the staged planes' stride).
+struct UpBase {
+    const float *f, *c, *o;
+};
+
+// x or y face inside one staged plane: cells a-1 .. a+2, ST floats apart
+// from qc (cell a-1, field 0)
+template <int ST>
+struct PlaneSrc {
+    const float *qc;
+    __device__ __forceinline__ float v(int f, int n) const { return qc[f * FR_PL + n * ST]; }
+    __device__ __forceinline__ UpBase side(bool left) const
+    {
+        return left ? UpBase{qc, qc + ST, qc + 2 * ST} : UpBase{qc + 3 * ST, qc + 2 * ST, qc + ST};
+    }
+    __device__ __forceinline__ float far(const UpBase &b, bool, int f) const { return b.f[f * FR_PL]; }
+};
+
+// z face between planes c and c+1 of one column: cell c-1 from the thread's
+// slot (fields FR_CS floats apart), c, c+1, c+2 from the ring.  The far cell
+// of the upwind triple is the slot's (left) or plane c+2's (right): the two
+// strides differ, so both are read and one is selected.
+struct ZColSrc {
+    const float *cm;            // the cell of plane c-1, field 0
+    const float *sc, *sn, *sp;  // the cell in the staged planes c, c+1, c+2, field 0
+    __device__ __forceinline__ float v(int f, int n) const
+    {
+        return n == 0 ? cm[f * FR_CS] : n == 1 ? sc[f * FR_PL] : n == 2 ? sn[f * FR_PL] : sp[f * FR_PL];
+    }
+    __device__ __forceinline__ UpBase side(bool left) const
+    {
+        return left ? UpBase{nullptr, sc, sn} : UpBase{nullptr, sn, sc};
+    }
+    __device__ __forceinline__ float far(const UpBase &, bool left, int f) const
+    {
+        const float a = cm[f * FR_CS], b = sp[f * FR_PL];
+        return left ? a : b;
+    }
+};
+
+// AUSM face flux of the ring kernel: face_flux_src's arithmetic with the
+// left/right pairs of the sound speeds and split Mach numbers, the upwind
+// reconstruction of two fields at a time and the species fluxes in packed
+// pairs; the result equals face_flux_src's bit for bit.
+template <int DIR, int DIFF, class Src>
+__device__ __forceinline__ void face_flux_pk(const Src &src, bool zspec, float out[NV])
+{
+    auto both = [&](int f, float &L, float &R) {
+        const float v0 = src.v(f, 0), v1 = src.v(f, 1), v2 = src.v(f, 2), v3 = src.v(f, 3);
+        L = recon_left<float, DIFF>(v0, v1, v2);
+        R = recon_right<float, DIFF>(v1, v2, v3);
+    };
+    constexpr int FN = DIR == 1 ? PU : DIR == 2 ? PV : PW;
+    float DL, DR, PL, PR, GL, GR, NL, NR;
+    both(PD, DL, DR);
+    both(PP, PL, PR);
+    both(PG, GL, GR);
+    both(FN, NL, NR);
+    // sound speeds x rsqrt(x D), x = g p: left and right in one pair
+    const float2 X = mul2(pk(GL, GR), pk(PL, PR));
+    const float2 Y = mul2(X, pk(DL, DR));
+    const float2 C = mul2(X, pk(rsqrt_approx(Y.x), rsqrt_approx(Y.y)));
+    const float CI = __fmul_rn(0.5f, C.x + C.y);
+    const float rCI = rcp_approx(CI);
+    const float2 M = mul2(pk(NL, NR), pk(rCI, rCI));  // (MaL, MaR)
+    // split Mach numbers: lane x the "+" split of MaL, lane y the "-" split
+    // of MaR, each in face_flux_src's operation order
+    const float2 MP = add2(M, pk(1.0f, -1.0f));  // MaL + 1, MaR - 1
+    const float2 M2 = fma2(M, M, pk(-1.0f, -1.0f));
+    const float2 MP2 = mul2(MP, MP), M22 = mul2(M2, M2);
+    const float2 BSUB = fma2(pk(0.125f, -0.125f), M22, mul2(pk(0.25f, -0.25f), MP2));
+    const float2 TWO = fma2(M, pk(-1.0f, 1.0f), pk(2.0f, 2.0f));  // 2 - MaL, 2 + MaR
+    const float2 GSUB = fma2(mul2(pk(0.1875f, -0.1875f), M), M22, mul2(mul2(pk(0.25f, 0.25f), MP2), TWO));
+    const float2 BSUP = mul2(pk(0.5f, 0.5f), pk(M.x + fabsf(M.x), M.y - fabsf(M.y)));
+    const bool subL = fabsf(M.x) < 1.0f, subR = fabsf(M.y) < 1.0f;
+    const float B1 = subL ? BSUB.x : BSUP.x, G1 = subL ? GSUB.x : __fdividef(BSUP.x, M.x);
+    const float B2 = subR ? BSUB.y : BSUP.y, G2 = subR ? GSUB.y : __fdividef(BSUP.y, M.y);
+    const float VI = __fmul_rn(B1 + B2, CI);
+    const bool left = VI >= 0.0f;
+    const float seps = left ? 1e-12f : -1e-12f;
+    const UpBase ub = src.side(left);
+    auto up2 = [&](int f, int g) -> float2 {
+        const float2 far = pk(src.far(ub, left, f), src.far(ub, left, g));
+        const float2 ctr = pk(ub.c[f * FR_PL], ub.c[g * FR_PL]);
+        const float2 oth = pk(ub.o[f * FR_PL], ub.o[g * FR_PL]);
+        if (DIFF == EU3D_DIFF_MUSCL1) return ctr;
+        if (DIFF == EU3D_DIFF_WENO) return pk(weno3(far.x, ctr.x, oth.x), weno3(far.y, ctr.y, oth.y));
+        return up_muscl2_x2(far, ctr, oth, pk(seps, seps));
+    };
+    constexpr int T1 = DIR == 1 ? PV : PU, T2 = DIR == 3 ? PV : PW;  // the tangential velocities
+    const float2 TT = up2(T1, T2);
+    const float2 HY = up2(PH, PY);
+    const float Ds = left ? DL : DR, Ns = left ? NL : NR;
+    const float Us = DIR == 1 ? Ns : TT.x;
+    const float Vs = DIR == 2 ? Ns : DIR == 1 ? TT.x : TT.y;
+    const float Ws = DIR == 3 ? Ns : TT.y;
+    const float VD = __fmul_rn(VI, Ds);
+    const float zf = __fmul_rn(0.0f, VD);
+    out[0] = zspec ? zf : __fmul_rn(VD, HY.y);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float2 o = mul2(pk(VD, VD), up2(PY + 1 + 2 * q, PY + 2 + 2 * q));
+        out[1 + 2 * q] = zspec ? zf : o.x;
+        out[2 + 2 * q] = zspec ? zf : o.y;
+    }
+    const float pn = __fmaf_rn(G2, PR, __fmul_rn(G1, PL));
+    out[NS] = DIR == 1 ? __fmaf_rn(VD, Us, pn) : __fmul_rn(VD, Us);
+    out[NS + 1] = DIR == 2 ? __fmaf_rn(VD, Vs, pn) : __fmul_rn(VD, Vs);
+    out[NS + 2] = DIR == 3 ? __fmaf_rn(VD, Ws, pn) : __fmul_rn(VD, Ws);
+    const float q2 = __fmaf_rn(Ws, Ws, __fmaf_rn(Vs, Vs, __fmul_rn(Us, Us)));
+    out[NS + 3] = __fmul_rn(VI, __fmaf_rn(__fmul_rn(0.5f, Ds), q2, __fmul_rn(Ds, HY.x)));
+}
+
+// residual() of two conserved variables at once (the same roundings per lane)
+__device__ __forceinline__ float2 residual2(float2 ax, float2 nby, float2 ncz, float2 xr, float2 xl, float2 yt,
+                                            float2 yb, float2 za, float2 zb)
+{
+    const float2 r = fma2(nby, sub2(yt, yb), mul2(ax, sub2(xr, xl)));
+    return fma2(ncz, sub2(za, zb), r);
+}
+
 struct FluxRing {
     static constexpr int PLANE = NPRIM * FR_PL;         // floats of one staged plane
     static constexpr uint32_t PLANE_BYTES = PLANE * 4;  // bytes of one TMA box (27648)
     static constexpr int FY = (FR_TY + 1) * FT_X * NV;  // y-face fluxes
     static constexpr int FXE = FR_TY * NV;              // the last x face of each row
-    static constexpr int CORE = NPRIM * FT_X * FR_TY;   // each cell thread's cell of plane c-1
-    static constexpr size_t BYTES = FR_NBUF * PLANE_BYTES + 4 * (FY + FXE + CORE) + 8 * FR_NBUF;
+    static constexpr int CORE = NPRIM * FR_CS;          // each cell thread's cell of plane c-1
+    static constexpr int CZ = 2;                        // dt/dz of the current and the next plane
+    static constexpr size_t BYTES = FR_NBUF * PLANE_BYTES + 4 * (FY + FXE + CORE + CZ) + 8 * FR_NBUF;
     // slack to align the ring to 128 B; two blocks (with the 1 KB the
     // hardware reserves for each) fit the SM's 228 KB
     static constexpr size_t SMEM = BYTES + 128;
     // TMA box {x, y, z, field}
     static constexpr unsigned BOX[4] = {FR_HX, FR_HY, 1, NPRIM};
 };
+static_assert(2 * (FluxRing::SMEM + 1024) <= 228 * 1024, "two ring blocks must fit one SM");
 
-// Source of the z face between planes c and c+1 of one column: cell c-1
-// from the thread's private slot (fields FT_X * FR_TY floats apart), c, c+1
-// and c+2 from the ring.
-struct ZSrc {
-    const float *cm;          // the cell of plane c-1, field 0
-    const float *sc, *sn, *sp;  // the cell in the staged planes c, c+1, c+2, field 0
-    __device__ __forceinline__ float v(int f, int n) const
-    {
-        return n == 0 ? cm[f * (FT_X * FR_TY)] : n == 1 ? sc[f * FR_PL] : n == 2 ? sn[f * FR_PL] : sp[f * FR_PL];
-    }
-    __device__ __forceinline__ void up3(int f, bool left, float &far, float &ctr, float &oth) const
-    {
-        far = left ? cm[f * (FT_X * FR_TY)] : sp[f * FR_PL];
-        ctr = (left ? sc : sn)[f * FR_PL];
-        oth = (left ? sn : sc)[f * FR_PL];
-    }
-};
-
-template <int DIFF>
+template <int DIFF, bool SQ>
 __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     const __grid_constant__ CUtensorMap tq, Layout L, const float *__restrict__ q, const double *__restrict__ xn,
     const double *__restrict__ yn, const double *__restrict__ zn, const double *__restrict__ dtp,
-    float *__restrict__ rhs, int species_quirk, int kz, Status *__restrict__ stat, FluxSolid wedge,
-    unsigned wait_tries)
+    float *__restrict__ rhs, int kz, Status *__restrict__ stat, FluxSolid wedge, unsigned wait_tries)
 {
     constexpr int TY = FR_TY, HX = FR_HX, PL = FR_PL;
     extern __shared__ unsigned char fr_raw[];
@@ -579,8 +720,10 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
     auto fy = reinterpret_cast<float(*)[FT_X][NV]>(ring + FR_NBUF * FluxRing::PLANE);
     auto fxe = reinterpret_cast<float(*)[NV]>(ring + FR_NBUF * FluxRing::PLANE + FluxRing::FY);
     float *core = ring + FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE;
+    float *czb = core + FluxRing::CORE;
     const uint32_t ring_s = tc::smem_u32(ring);
-    const uint32_t mb_s = ring_s + 4u * (FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE + FluxRing::CORE);
+    const uint32_t mb_s =
+        ring_s + 4u * (FR_NBUF * FluxRing::PLANE + FluxRing::FY + FluxRing::FXE + FluxRing::CORE + FluxRing::CZ);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * FT_X + tx;
     const int i0 = L.bc + blockIdx.x * FT_X, j0 = L.bc + blockIdx.y * TY;
     const int kb = L.bc + blockIdx.z * kz;
@@ -601,18 +744,23 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         tc::mbar_expect_tx(mb_s + 8u * b, FluxRing::PLANE_BYTES);
         tc::tma_load_4d(ring_s + b * FluxRing::PLANE_BYTES, &tq, i0 - 2, j0 - 2, kb + p, 0, mb_s + 8u * b);
     };
+    const double dt = *dtp;
+    // dt/dz of plane kb + p, formed by one thread of the y-face warp
+    const bool czw = tid == TY * FT_X;
+    auto cz_of = [&](int p) { return (float)(dt / (zn[kb + p] - zn[kb + p - 1])); };
     if (tid == 0) {
         for (int b = 0; b < FR_NBUF; b++) tc::mbar_init(mb_s + 8u * b, 1);
         tc::fence_mbar_init();
     }
+    if (czw) czb[0] = cz_of(0);
     __syncthreads();
     int issued = min(FR_NBUF, np + 2);
     if (tid == 0)
         for (int p = 0; p < issued; p++) issue(p);
-    const double dt = *dtp;
-    const bool zs_cell = species_quirk && i >= L.ni;
+    const bool zs_cell = SQ && i >= L.ni;
     const float ax = (float)(act ? -dt / (xn[i] - xn[i - 1]) : 0.0);
     const float by = (float)(act ? dt / (yn[j] - yn[j - 1]) : 0.0);
+    const float2 ax2 = pk(ax, ax), nby2 = pk(-by, -by);
     float qb[NV], qa[NV], fo[NV];
 #pragma unroll
     for (int v = 0; v < NV; v++) qb[v] = qa[v] = fo[v] = 0.f;
@@ -623,9 +771,16 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         face_flux_up<float, 3, DIFF>(q + L.at(i, j, kb) - 2 * (long long)sz, fs, sz, zs_cell, qb);
         const float *g = q + L.at(i, j, kb) - sz;
 #pragma unroll
-        for (int f = 0; f < NPRIM; f++) slot[f * (FT_X * FR_TY)] = __ldg(g + (long long)f * fs);
+        for (int f = 0; f < NPRIM; f++) slot[f * FR_CS] = __ldg(g + (long long)f * fs);
     }
     const int so = (ty + 2) * HX + tx + 2;  // the cell inside a staged field plane
+    // x faces: cell warps own face tx of row ty (cells i-2 .. i+1); the last
+    // face warp lanes 0..7 own face 32 of row tx (lanes 8..31 repeat row
+    // tx & 7 and store nothing)
+    const int xr_row = cellw ? ty : (tx & (TY - 1));
+    const int xr_col = cellw ? tx : FT_X;
+    const bool xs_face = SQ && (i0 + xr_col - 1) >= L.ni;
+    float *out = rhs + L.at(min(i, ilast), min(j, jlast), kb);
     bool ok = true;
     int p = 0;
     for (; p < np; p++) {
@@ -634,58 +789,72 @@ __global__ void __launch_bounds__(FT_X *(FR_TY + 2), 2) k_flux_ring(
         ok = tc::mbar_wait(mb_s + 8u * b1, ((p + 1) / FR_NBUF) & 1, wait_tries) && ok;
         const float *S0 = ring + b0 * FluxRing::PLANE, *S1 = ring + b1 * FluxRing::PLANE;
         const float *S2 = ring + b2 * FluxRing::PLANE;
-        const int k = kb + p;
-        // y face g = ty of column i, between b = j0+g-1 and b+1 (staged rows
-        // g .. g+3): faces 0..7 by the cell warps, face 8 by warp TY
-        if (ty <= TY && i <= ilast && j0 + ty - 1 <= jlast)
-            face_flux_src<2, DIFF>(StridedSrc<false>{S0 + ty * HX + tx + 2, PL, HX}, species_quirk && i >= L.ni,
-                                   fy[ty][tx]);
-        // x face f of row r, between a = i0+f-1 and a+1 (staged columns
-        // f .. f+3): f = tx by the cell warps, f = 32 of row tx by warp TY+1
-        {
-            const bool xw = cellw || (ty == TY + 1 && tx < TY);
-            const int r = cellw ? ty : tx;
-            const int f = cellw ? tx : FT_X;
-            const int a = i0 + f - 1;
-            if (xw && j0 + r <= jlast && a <= ilast) {
-                face_flux_src<1, DIFF>(StridedSrc<false>{S0 + (r + 2) * HX + f, PL, 1}, species_quirk && a >= L.ni, fo);
-                if (!cellw)
+        if (czw && p + 1 < np) czb[(p + 1) & 1] = cz_of(p + 1);
+        // y face g of column i, between rows j0+g-1 and j0+g (staged rows
+        // g .. g+3); x face f of row r, between columns i0+f-1 and i0+f
+        // (staged columns f .. f+3).  A cell warp evaluates both in one
+        // block of code (its y face g = ty, its x face f = tx); warp TY the
+        // y faces g = 8, warp TY+1 the x faces f = 32.
+        if (cellw) {
+            face_flux_pk<2, DIFF>(PlaneSrc<HX>{S0 + ty * HX + tx + 2}, SQ && i >= L.ni, fy[ty][tx]);
+            face_flux_pk<1, DIFF>(PlaneSrc<1>{S0 + (ty + 2) * HX + tx}, xs_face, fo);
+        } else if (ty == TY) {
+            face_flux_pk<2, DIFF>(PlaneSrc<HX>{S0 + ty * HX + tx + 2}, SQ && i >= L.ni, fy[ty][tx]);
+        } else {
+            face_flux_pk<1, DIFF>(PlaneSrc<1>{S0 + (xr_row + 2) * HX + FT_X}, xs_face, fo);
+            if (tx < TY)
 #pragma unroll
-                    for (int v = 0; v < NV; v++) fxe[r][v] = fo[v];
-            }
+                for (int v = 0; v < NV; v++) fxe[tx][v] = fo[v];
         }
         // z face above the cell (between planes k and k+1): plane k+2 was
-        // copied during the previous plane; then the cell of plane k replaces
-        // that of plane k-1 in the slot
+        // copied during the previous plane; then the cell of plane k
+        // replaces that of plane k-1 in the slot
         ok = tc::mbar_wait(mb_s + 8u * b2, ((p + 2) / FR_NBUF) & 1, wait_tries) && ok;
-        if (act) {
-            face_flux_src<3, DIFF>(ZSrc{slot, S0 + so, S1 + so, S2 + so}, zs_cell, qa);
+        if (cellw) {
+            face_flux_pk<3, DIFF>(ZColSrc{slot, S0 + so, S1 + so, S2 + so}, zs_cell, qa);
 #pragma unroll
-            for (int f = 0; f < NPRIM; f++) slot[f * (FT_X * FR_TY)] = S0[so + f * PL];
+            for (int f = 0; f < NPRIM; f++) slot[f * FR_CS] = S0[so + f * PL];
         }
         if (__syncthreads_or(!ok)) break;
-        if (cellw) {
-            // every lane of a cell warp evaluates (inactive lanes on values
-            // that are never stored): only the stores are predicated
-            // The right x face comes from the next lane; lane 31's (face 32
-            // of the row) is sent by lane 0 from the face warp's slot.
-            const float cz = (float)(dt / (zn[k] - zn[k - 1]));
-            float *out = rhs + L.at(min(i, ilast), min(j, jlast), k);
-#pragma unroll
-            for (int v = 0; v < NV; v++) {
-                float send = fo[v];
-                if (tx == 0) send = fxe[ty][v];
-                const float fr = __shfl_sync(0xffffffffu, send, (tx + 1) & (FT_X - 1));
-                const float val = residual(ax, by, cz, fr, fo[v], fy[ty + 1][tx][v], fy[ty][tx][v], qa[v], qb[v]);
-                if (act) out[v * L.fs] = val;
-                qb[v] = qa[v];
-            }
-        }
-        __syncthreads();
+        // nothing reads plane p (buffer b0) after the barrier: plane p + 3
+        // goes into it while the residuals are formed
         if (p + FR_NBUF <= np + 1) {
             if (tid == 0) issue(p + FR_NBUF);
             issued++;
         }
+        if (cellw) {
+            // every lane of a cell warp evaluates (inactive lanes on values
+            // that are never stored): only the stores are predicated.  The
+            // right x face comes from the next lane; lane 31's (face 32 of
+            // the row) is sent by lane 0 from the face warp's slot.
+            const float cz = czb[p & 1];
+            const float2 ncz2 = pk(-cz, -cz);
+            float fr[NV];
+#pragma unroll
+            for (int v = 0; v < NV; v++) {
+                float send = fo[v];
+                if (tx == 0) send = fxe[ty][v];
+                fr[v] = __shfl_sync(0xffffffffu, send, (tx + 1) & (FT_X - 1));
+            }
+#pragma unroll
+            for (int v = 0; v + 1 < NV; v += 2) {
+                const float2 r = residual2(ax2, nby2, ncz2, pk(fr[v], fr[v + 1]), pk(fo[v], fo[v + 1]),
+                                           pk(fy[ty + 1][tx][v], fy[ty + 1][tx][v + 1]),
+                                           pk(fy[ty][tx][v], fy[ty][tx][v + 1]), pk(qa[v], qa[v + 1]),
+                                           pk(qb[v], qb[v + 1]));
+                if (act) {
+                    out[v * (long long)fs] = r.x;
+                    out[(v + 1) * (long long)fs] = r.y;
+                }
+            }
+            const float rl = residual(ax, by, cz, fr[NV - 1], fo[NV - 1], fy[ty + 1][tx][NV - 1], fy[ty][tx][NV - 1],
+                                      qa[NV - 1], qb[NV - 1]);
+            if (act) out[(NV - 1) * (long long)fs] = rl;
+#pragma unroll
+            for (int v = 0; v < NV; v++) qb[v] = qa[v];
+            out += sz;
+        }
+        __syncthreads();
     }
     if (p < np) {
         // a wait ran out: count it, let the copies in flight land (with the

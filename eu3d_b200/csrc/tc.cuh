@@ -79,28 +79,46 @@ __device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity)
     return ok != 0;
 }
 
-// potentially blocking test: the thread is suspended until the phase
-// completes or about hint_ns pass (then false)
-__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity, uint32_t hint_ns)
+// potentially blocking test without a suspend-time hint: the hardware
+// resumes the thread when the phase completes (or after its own time limit,
+// then false)
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity)
 {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
         : "=r"(ok)
-        : "r"(mbar), "r"(parity), "r"(hint_ns)
+        : "r"(mbar), "r"(parity)
         : "memory");
     return ok != 0;
 }
 
-// bounded wait on an mbarrier phase (under a second): false when the bound
-// ran out, so that no caller can spin forever.  Waiting threads sleep in
-// the barrier instead of issuing test instructions.
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait on an mbarrier phase: false when the bound ran out, so that
+// no caller can spin forever.  The bound is max_tries attempts and at most
+// one second of the global timer, whichever ends first.  Waiting threads
+// block in try_wait, which the hardware ends as soon as the phase completes;
+// a suspend-time hint is not given (with one, a wait that found the copy
+// still in flight slept out the hint, which set the pace of the flux ring).
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32_t max_tries = (1u << 19))
 {
-    for (uint32_t t = 0; t < max_tries; t++)
-        if (mbar_try(mbar, parity, 1000u)) return true;
+    uint64_t t0 = 0;
+    for (uint32_t t = 0; t < max_tries; t++) {
+        if (mbar_try(mbar, parity)) return true;
+        const uint64_t now = global_ns();
+        if (t == 0)
+            t0 = now;
+        else if (now - t0 > 1000000000ull)
+            return false;
+    }
     return false;
 }
 
