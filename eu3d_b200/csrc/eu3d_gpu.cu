@@ -113,6 +113,8 @@ struct eu3d_handle {
     float *sur_out = nullptr;
     int *sur_list = nullptr, *sur_count = nullptr;
     double *sur_audit = nullptr;
+    double *sur_res = nullptr;  // fallback results per list slot ((NS + 1) x sur_cap)
+    int *sur_info = nullptr;    // fallback substep counts and flags per list slot
     long long sur_cap = 0;
     int sur_audit_stride = 0;
     int *sur_active = nullptr;  // cells the frozen-chemistry gate passes to the network
@@ -744,7 +746,8 @@ void free_handle(eu3d_handle *h)
                     h->nchem,   h->xn,     h->yn,     h->zn,      h->scal,      h->partial,
                     h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
                     h->sur_audit, h->qlist,   h->qbins,  h->wedge_band, h->dlb_rowload, h->g_cs,
-                    h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim, h->sur_active};
+                    h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim, h->sur_active,
+                    h->sur_res, h->sur_info};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->writer.joinable()) h->writer.join();
@@ -806,18 +809,22 @@ int ensure_cell_list(eu3d_handle *h)
     if (h->L.fs > (long long)SUR_CELL_MASK) return fail(EU3D_ERR_ARG, "grid too large for the cell list");
     if (h->sur_cap < n) {
         CK(cudaStreamSynchronize(h->st));
-        void *ptrs[] = {h->sur_out, h->sur_list, h->sur_audit, h->sur_active};
+        void *ptrs[] = {h->sur_out, h->sur_list, h->sur_audit, h->sur_active, h->sur_res, h->sur_info};
         for (void *q : ptrs)
             if (q) cudaFree(q);
         h->sur_out = nullptr;
         h->sur_list = nullptr;
         h->sur_audit = nullptr;
         h->sur_active = nullptr;
+        h->sur_res = nullptr;
+        h->sur_info = nullptr;
         h->sur_cap = 0;
         CK(cudaMalloc(&h->sur_out, (size_t)n * SUR_NOUT * sizeof(float)));
         CK(cudaMalloc(&h->sur_list, (size_t)n * sizeof(int)));
         CK(cudaMalloc(&h->sur_audit, (size_t)n * sizeof(double)));
         CK(cudaMalloc(&h->sur_active, (size_t)n * sizeof(int)));
+        CK(cudaMalloc(&h->sur_res, (size_t)n * (NS + 1) * sizeof(double)));
+        CK(cudaMalloc(&h->sur_info, (size_t)n * sizeof(int)));
         h->sur_cap = n;
     }
     if (!h->sur_count) CK(cudaMalloc(&h->sur_count, 4 * sizeof(int)));
@@ -835,13 +842,14 @@ void adapt_queue_t(eu3d_handle *h, bool decoded)
     P *q = (P *)h->prim;
     cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
-    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, L.interior_cells()};
+    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, L.interior_cells(), h->sur_res, h->sur_info};
     {
         ProfScope ps(h, "adapt_list");
         k_list_fluid<<<cell_grid(L, 256), 256, 0, h->st>>>(cell_args(h), qu);
     }
     ProfScope ps(h, "adapt_queue");
     k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+    k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
 }
 
 int adapt_queue_op(eu3d_handle *h, bool decoded)

@@ -237,7 +237,7 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     // split step: the flux update and its decode first (Update_after_Adv),
     // unless the time scheme left the state decoded with the update in
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
-    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n};
+    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n, h->sur_res, h->sur_info};
     SurApplyArgs a{cell_args(h), s->norm_d, h->sur_out, n, qu, h->sur_audit_stride};
     const SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
     const long long ntiles = src.ntiles();
@@ -283,6 +283,7 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     {
         ProfScope ps(h, "sur_fallback");
         k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+        k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
     }
 }
 

@@ -666,7 +666,11 @@ struct SurQueue {
     int *count;     // [0] list length, [1] work cursor
     double *audit;  // per list slot: the temperature to judge for audited cells
     long long cap;
+    double *res;    // per list slot, field-major (cap apart): the integrated species and T
+    int *info;      // per list slot: substeps | SUR_CAPPED | SUR_FORCED
 };
+constexpr int SUR_CAPPED = 1 << 24;  // a Newton iteration ran into its cap
+constexpr int SUR_FORCED = 1 << 25;  // the substep cap lengthened a substep
 
 struct SurApplyArgs {
     CellArgs a;
@@ -1014,8 +1018,12 @@ struct SurSrcFieldApply : SurSrcField<P> {
 // the slowest of a batch.  Each cell runs the FP64 adaptive split step the
 // network was trained on (adapt_split_step with the flux update applied
 // already: chem_increment, then the species update and a decode), one
-// substep per pass.  For audited cells the surrogate's temperature is
-// compared with the integrator's and the largest difference recorded.
+// substep per pass.  The loop holds the substeps only: a finished cell's
+// integrated species, T and counts go to its list slot, and
+// k_sur_fallback_finish does the projection, update, decode and stores with
+// one thread per slot -- run inside the loop, that work was executed by the
+// warp in nearly every pass (some lane finishes a cell in most passes), and
+// its code competed with the substep's for the instruction cache.
 template <class P, bool SPEC>
 __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restrict__ q, SurQueue qu)
 {
@@ -1027,9 +1035,7 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
     const AdaptCfg cfg = a.acfg;
     const double hmin = dt / cfg.nmax;
     int slot = -1;  // list slot of the lane's cell; -1: needs one; >= total: none left
-    bool audit = false, faudit = false;
-    long long c = 0;
-    double cs0[NV], cs[NV];  // the cell's state before the chemistry; the integrator's copy
+    double cs[NV];  // the integrator's copy of the cell's state
     double T = 0.0, Esub = 0.0, trem = 0.0;
     int k = 0, capped = 0, forced = 0;
     Decoded o;
@@ -1044,22 +1050,17 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
             if (need) {
                 slot = base + __popc(m & ((1u << lane) - 1u));
                 if (slot < total) {
-                    const unsigned ent = (unsigned)qu.list[slot];
-                    audit = (ent & SUR_AUDIT) != 0;
-                    faudit = (ent & SUR_FROZEN_AUDIT) != 0;
-                    c = (long long)(ent & (unsigned)SUR_CELL_MASK);
-                    load_cs(a.cs, fs, c, cs0);
+                    const long long c = (long long)((unsigned)qu.list[slot] & (unsigned)SUR_CELL_MASK);
+                    load_cs(a.cs, fs, c, cs);
                     // the decoded state (adapt_split_step without the flux
                     // update): the integrator runs at its energy from its T
                     double D = 0.0;
 #pragma unroll
-                    for (int s = 0; s < NS; s++) D += cs0[s];
+                    for (int s = 0; s < NS; s++) D += cs[s];
                     const double iD = 1.0 / D;
-                    const double U = cs0[NS] * iD, V = cs0[NS + 1] * iD, W = cs0[NS + 2] * iD;
-                    Esub = (cs0[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) * iD;
+                    const double U = cs[NS] * iD, V = cs[NS + 1] * iD, W = cs[NS + 2] * iD;
+                    Esub = (cs[NS + 3] - 0.5 * D * (U * U + V * V + W * W)) * iD;
                     T = a.T[c];
-#pragma unroll
-                    for (int v = 0; v < NV; v++) cs[v] = cs0[v];
                     trem = dt;
                     k = 0;
                     capped = 0;
@@ -1071,44 +1072,79 @@ __global__ void __launch_bounds__(128, 3) k_sur_fallback(CellArgs a, P *__restri
         if (slot < total) {
             if (trem > 0.0 && k < cfg.nmax) adapt_substep<SPEC>(cs, T, Esub, qk, trem, k, hmin, cfg, o, capped, forced);
             if (!(trem > 0.0 && k < cfg.nmax)) {
-                // chem_increment's projection, then adapt_split_step's update and decode
-                double D0 = 0.0, Dn = 0.0;
 #pragma unroll
-                for (int s = 0; s < NS; s++) {
-                    D0 += cs0[s];
-                    Dn += cs[s];
-                }
-                double Y0[NS], dY[NS];
-#pragma unroll
-                for (int s = 0; s < NS; s++) {
-                    Y0[s] = cs0[s] / D0;
-                    dY[s] = cs[s] / Dn - Y0[s];
-                }
-                elem_project(Y0, dY, a.proj_eps);
-                const double Tc = T;
-                const double iD = 1.0 / D0;
-#pragma unroll
-                for (int s = 0; s < NS; s++) cs0[s] = fmax(D0 * (cs0[s] * iD + dY[s]), 0.0);
-                int cp = 0;
-                decode(cs0, Tc, Esub, qk, o, cp);
-                capped |= cp;
-                atomicAdd(&a.st->substeps, (unsigned long long)k);
-                store_cs(a.cs, fs, c, cs0);
-                a.T[c] = o.T;
-                a.E[c] = o.E;
-                store_prims<P>(o, q, fs, c);
-                if (capped) atomicAdd(&a.st->newton_capped, 1ull);
-                if (forced) atomicAdd(&a.st->substep_capped, 1);
-                if (!(isfinite(o.D) && isfinite(o.T))) atomicAdd(&a.st->nonfinite, 1ull);
-                if (audit || faudit) {
-                    const double d = fabs(qu.audit[slot] - o.T);
-                    unsigned long long *mx = audit ? &a.st->audit_max_dT_bits : &a.st->frozen_audit_max_dT_bits;
-                    atomicAdd(audit ? &a.st->audit_cells : &a.st->frozen_audit_cells, 1ull);
-                    if (isfinite(d)) atomicMax(mx, (unsigned long long)__double_as_longlong(d));
-                    else atomicMax(mx, 0x7ff0000000000000ull);
-                }
+                for (int sp = 0; sp < NS; sp++) qu.res[sp * qu.cap + slot] = cs[sp];
+                qu.res[NS * qu.cap + slot] = T;
+                qu.info[slot] = k | (capped ? SUR_CAPPED : 0) | (forced ? SUR_FORCED : 0);
                 slot = -1;
             }
+        }
+    }
+}
+
+// The end of each fallback cell's split step, one thread per list slot:
+// chem_increment's element projection of the integrated change, then
+// adapt_split_step's species update and decode at the cell's density and
+// energy, the stores, and the status counts (audits compared with the
+// surrogate's temperature).  The same arithmetic as the end of
+// adapt_split_step, on the state k_sur_fallback left in the slot.
+constexpr int FALLBACK_FINISH_BLOCKS = 148 * 8;  // grid of k_sur_fallback_finish (grid-stride over the slots)
+
+template <class P, bool SPEC>
+__global__ void __launch_bounds__(128) k_sur_fallback_finish(CellArgs a, P *__restrict__ q, SurQueue qu)
+{
+    const int total = (int)min((long long)*qu.count, qu.cap);
+    const long long fs = a.L.fs;
+    const unsigned qk = a.quirks;
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < total; slot += gridDim.x * blockDim.x) {
+        const unsigned ent = (unsigned)qu.list[slot];
+        const bool audit = (ent & SUR_AUDIT) != 0, faudit = (ent & SUR_FROZEN_AUDIT) != 0;
+        const long long c = (long long)(ent & (unsigned)SUR_CELL_MASK);
+        double cs0[NV];
+        load_cs(a.cs, fs, c, cs0);
+        double D0 = 0.0, Dn = 0.0, cs[NS];
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++) {
+            cs[sp] = qu.res[sp * qu.cap + slot];
+            D0 += cs0[sp];
+            Dn += cs[sp];
+        }
+        const double Tc = qu.res[NS * qu.cap + slot];
+        const int inf = qu.info[slot];
+        // the energy the integrator ran at (as k_sur_fallback formed it)
+        double Esub;
+        {
+            const double iD = 1.0 / D0;
+            const double U = cs0[NS] * iD, V = cs0[NS + 1] * iD, W = cs0[NS + 2] * iD;
+            Esub = (cs0[NS + 3] - 0.5 * D0 * (U * U + V * V + W * W)) * iD;
+        }
+        double Y0[NS], dY[NS];
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++) {
+            Y0[sp] = cs0[sp] / D0;
+            dY[sp] = cs[sp] / Dn - Y0[sp];
+        }
+        elem_project(Y0, dY, a.proj_eps);
+        const double iD = 1.0 / D0;
+#pragma unroll
+        for (int sp = 0; sp < NS; sp++) cs0[sp] = fmax(D0 * (cs0[sp] * iD + dY[sp]), 0.0);
+        int cp = 0;
+        Decoded o;
+        decode(cs0, Tc, Esub, qk, o, cp);
+        store_cs(a.cs, fs, c, cs0);
+        a.T[c] = o.T;
+        a.E[c] = o.E;
+        store_prims<P>(o, q, fs, c);
+        warp_sum(&a.st->substeps, (unsigned long long)(inf & (SUR_CAPPED - 1)));
+        warp_count(&a.st->newton_capped, cp || (inf & SUR_CAPPED));
+        if (inf & SUR_FORCED) atomicAdd(&a.st->substep_capped, 1);
+        warp_count(&a.st->nonfinite, !(isfinite(o.D) && isfinite(o.T)));
+        if (audit || faudit) {
+            const double d = fabs(qu.audit[slot] - o.T);
+            unsigned long long *mx = audit ? &a.st->audit_max_dT_bits : &a.st->frozen_audit_max_dT_bits;
+            atomicAdd(audit ? &a.st->audit_cells : &a.st->frozen_audit_cells, 1ull);
+            if (isfinite(d)) atomicMax(mx, (unsigned long long)__double_as_longlong(d));
+            else atomicMax(mx, 0x7ff0000000000000ull);
         }
     }
 }
