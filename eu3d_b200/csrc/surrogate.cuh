@@ -910,15 +910,16 @@ __global__ void __launch_bounds__(GATE_THREADS) k_sur_gate(CellArgs a, const P *
     bool frozen = false;
     double T = 0.0;
     if (fluid) {
+        // T and the radicals are loaded together (one memory round trip;
+        // the radicals of hot cells are read and not needed)
         T = a.T[c];
-        frozen = T < g.T_frozen;
-        if (frozen && g.mask) {
-            float y = 0.f;
+        float y = 0.f;
+        if (g.mask) {
 #pragma unroll
             for (int s = 0; s < NS; s++)
                 if ((g.mask >> s) & 1u) y += fmaxf((float)q[(PY + s) * L.fs + c], 0.f);
-            frozen = y <= g.y_max_f;
         }
+        frozen = T < g.T_frozen && (!g.mask || y <= g.y_max_f);
     }
     const bool active = fluid && !frozen;
     __shared__ int wact[GATE_THREADS / 32], base_s;
