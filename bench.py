@@ -327,13 +327,14 @@ def roofline(prof, units, hbm, tflops, src, pb=4, kernel=None):
 
 
 # DRAM bytes of a flux launch per fluid cell (ncu dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch of k_flux_ring on the 256 x 128 x 64 ODW,
-# 2.10 M cells of which 1.30 M fluid, all-solid tiles skipped; the full
+# dram__bytes_write.sum of one launch of k_flux_ring on the 512 x 256 x 64 ODW
+# at 64 planes per block, the benchmark's cross-section and tile depth,
+# 8.39 M cells of which 5.22 M fluid, all-solid tiles skipped; the full
 # 33.5 M-cell case is too large to capture under the profiling rule, and the
-# kernel's traffic grows with the fluid cells): 125.7 MB read + 50.4 MB written
-TRAFFIC_PER_CELL = {"advection": (125739008 + 50361600) / 1303488}
-TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on a 2.10 M-cell case (1.30 M fluid), per fluid cell, "
-                             "times the fluid cells"}
+# kernel's traffic grows with the fluid cells): 535.2 MB read + 275.4 MB written
+TRAFFIC_PER_CELL = {"advection": (535170560 + 275366912) / 5217088}
+TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on the 512x256x64 case (5.22 M fluid cells), per fluid "
+                             "cell, times the fluid cells"}
 
 
 def fluid_cells(case, i0=0, n_loc=None):

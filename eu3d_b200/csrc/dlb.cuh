@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "cell.cuh"
+#include "surrogate.cuh"
 
 namespace eu3d {
 
@@ -171,6 +172,102 @@ __global__ void k_dlb_unpack(CellArgs a, DlbSegs sg, const double *__restrict__ 
 #pragma unroll
         for (int f = 0; f < NPRIM; f++) q[f * fs + c] = (P)o[(NV + 2 + f) * cells];
         a.nchem[c] = (int)o[(NV + 2 + NPRIM) * cells];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Load balancing of the learned chemistry's FP64 fallback (new).  The sender
+// gives away the last list slots: segment p of the transfers holds slots
+// keep + [first[p], first[p + 1]).  Packets, field-major per segment:
+//   out  (owner -> guest): CS[NV], T, audit T, list flags     SDLB_OUT fields
+//   back (guest -> owner): CS[NV], T, E, prims[NPRIM]          SDLB_BACK fields
+constexpr int SDLB_OUT = NV + 3;
+constexpr int SDLB_BACK = NV + 2 + NPRIM;
+
+__global__ void k_sdlb_pack(CellArgs a, SurQueue qu, DlbGuestSegs sg, long long keep, double *__restrict__ buf)
+{
+    const long long total = sg.first[sg.n], fs = a.L.fs;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int p = dlb_seg(sg.first, sg.n, g);
+        const long long cells = sg.first[p + 1] - sg.first[p], s = g - sg.first[p];
+        const long long slot = keep + g;
+        const unsigned ent = (unsigned)qu.list[slot];
+        const long long c = (long long)(ent & (unsigned)SUR_CELL_MASK);
+        double *o = buf + sg.off_in[p] + s;
+#pragma unroll
+        for (int v = 0; v < NV; v++) o[v * cells] = a.cs[v * fs + c];
+        o[NV * cells] = a.T[c];
+        o[(NV + 1) * cells] = qu.audit[slot];
+        o[(NV + 2) * cells] = (double)(ent >> 30);
+    }
+}
+
+// the owner keeps list slots [0, keep) for its own fallback work
+__global__ void k_sdlb_keep(int *__restrict__ count, int keep)
+{
+    count[0] = keep;
+    count[1] = 0;
+}
+
+// received cells into the guest store (field stride gcap) and the guest's
+// fallback list (entry g with the sender's flags)
+__global__ void k_sdlb_guest_in(DlbGuestSegs sg, const double *__restrict__ in, long long gcap, double *__restrict__ cs,
+                                double *__restrict__ T, double *__restrict__ audit, int *__restrict__ list)
+{
+    const long long total = sg.first[sg.n];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int p = dlb_seg(sg.first, sg.n, g);
+        const long long cells = sg.first[p + 1] - sg.first[p], s = g - sg.first[p];
+        const double *o = in + sg.off_in[p] + s;
+#pragma unroll
+        for (int v = 0; v < NV; v++) cs[v * gcap + g] = o[v * cells];
+        T[g] = o[NV * cells];
+        audit[g] = o[(NV + 1) * cells];
+        list[g] = (int)((unsigned)g | ((unsigned)o[(NV + 2) * cells] << 30));
+    }
+}
+
+// the integrated guest cells into the return packets
+template <class P>
+__global__ void k_sdlb_guest_out(DlbGuestSegs sg, long long gcap, const double *__restrict__ cs,
+                                 const double *__restrict__ T, const double *__restrict__ E, const P *__restrict__ q,
+                                 double *__restrict__ out)
+{
+    const long long total = sg.first[sg.n];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int p = dlb_seg(sg.first, sg.n, g);
+        const long long cells = sg.first[p + 1] - sg.first[p], s = g - sg.first[p];
+        double *o = out + sg.off_out[p] + s;
+#pragma unroll
+        for (int v = 0; v < NV; v++) o[v * cells] = cs[v * gcap + g];
+        o[NV * cells] = T[g];
+        o[(NV + 1) * cells] = E[g];
+#pragma unroll
+        for (int f = 0; f < NPRIM; f++) o[(NV + 2 + f) * cells] = (double)q[f * gcap + g];
+    }
+}
+
+// the returned cells back into the owner's fields
+template <class P>
+__global__ void k_sdlb_unpack(CellArgs a, SurQueue qu, DlbGuestSegs sg, long long keep, const double *__restrict__ back,
+                              P *__restrict__ q)
+{
+    const long long total = sg.first[sg.n], fs = a.L.fs;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int p = dlb_seg(sg.first, sg.n, g);
+        const long long cells = sg.first[p + 1] - sg.first[p], s = g - sg.first[p];
+        const long long c = (long long)((unsigned)qu.list[keep + g] & (unsigned)SUR_CELL_MASK);
+        const double *o = back + sg.off_out[p] + s;
+#pragma unroll
+        for (int v = 0; v < NV; v++) a.cs[v * fs + c] = o[v * cells];
+        a.T[c] = o[NV * cells];
+        a.E[c] = o[(NV + 1) * cells];
+#pragma unroll
+        for (int f = 0; f < NPRIM; f++) q[f * fs + c] = (P)o[(NV + 2 + f) * cells];
     }
 }
 

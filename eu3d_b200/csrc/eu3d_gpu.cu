@@ -138,6 +138,14 @@ struct eu3d_handle {
     double *g_cs = nullptr, *g_T = nullptr, *g_E = nullptr;
     int *g_nchem = nullptr, *g_list = nullptr, *g_bins = nullptr;
     void *g_prim = nullptr;
+    // ... and its learned-chemistry fallback queue: audit temperatures,
+    // per-slot results, list counts
+    double *g_audit = nullptr, *g_res = nullptr;
+    int *g_info = nullptr, *g_count = nullptr;
+    // fallback load balancing: the list length of the last eu3d_sur_load, the
+    // slots kept, the transfers this rank sends (segments of list slots)
+    long long sdlb_total = 0, sdlb_keep = 0;
+    DlbGuestSegs sdlb_segs{};
 };
 
 namespace {
@@ -747,7 +755,7 @@ void free_handle(eu3d_handle *h)
                     h->status,  h->inflow, h->stage,  h->sur_out, h->sur_list,  h->sur_count,
                     h->sur_audit, h->qlist,   h->qbins,  h->wedge_band, h->dlb_rowload, h->g_cs,
                     h->g_T,     h->g_E,    h->g_nchem, h->g_list, h->g_bins,  h->g_prim, h->sur_active,
-                    h->sur_res, h->sur_info};
+                    h->sur_res, h->sur_info, h->g_audit, h->g_res, h->g_info, h->g_count};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->writer.joinable()) h->writer.join();
@@ -770,7 +778,12 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
     return EU3D_OK;
 }
 
-int sur_chem_op(eu3d_handle *h, bool decoded);  // learned chemistry step, sur_host.cuh
+// learned chemistry step (sur_host.cuh), whole or one half: SUR_HALF_PREDICT
+// runs everything up to the fallback list (the flux update, gate, network and
+// apply), SUR_HALF_WORK the fallback queue on the list slots kept (all of
+// them unless eu3d_sdlb_pack sent some away)
+constexpr int SUR_HALF_PREDICT = 1, SUR_HALF_WORK = 2, SUR_HALF_BOTH = 3;
+int sur_chem_op(eu3d_handle *h, bool decoded, int half = SUR_HALF_BOTH);
 
 bool is_rk(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 || timeadv == EU3D_ADV_SSPRK3; }
 int rk_stages(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 ? 2 : timeadv == EU3D_ADV_SSPRK3 ? 3 : 1; }
@@ -1492,6 +1505,10 @@ int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part)
             return fail(EU3D_ERR_ARG, "the chemistry halves exist for the adaptive trapezoid (type 1) only");
         if (!h->chem_queue || !h->qlist) return fail(EU3D_ERR_STATE, "the chemistry halves need the work queue");
         return trap1_part(h, part == EU3D_PART_CHEM_WORK ? 1 : 0);
+    case EU3D_PART_SUR_PREDICT:
+    case EU3D_PART_SUR_WORK:
+        if (s->react != EU3D_REACT_SURROGATE) return fail(EU3D_ERR_ARG, "the surrogate halves need react SURROGATE");
+        return sur_chem_op(h, is_rk(s->timeadv), part == EU3D_PART_SUR_WORK ? SUR_HALF_WORK : SUR_HALF_PREDICT);
     default: return fail(EU3D_ERR_ARG, "unknown step part");
     }
 }
@@ -1603,11 +1620,11 @@ int ensure_guest(eu3d_handle *h, long long cells)
     const long long cap = std::max<long long>(cells, 2 * h->g_cap);
     // earlier guest work queued on the handle's stream may still read the old store
     CK(cudaStreamSynchronize(h->st));
-    void *old[] = {h->g_cs, h->g_T, h->g_E, h->g_nchem, h->g_list, h->g_prim};
+    void *old[] = {h->g_cs, h->g_T, h->g_E, h->g_nchem, h->g_list, h->g_prim, h->g_audit, h->g_res, h->g_info};
     for (void *p : old)
         if (p) cudaFree(p);
-    h->g_cs = h->g_T = h->g_E = nullptr;
-    h->g_nchem = h->g_list = nullptr;
+    h->g_cs = h->g_T = h->g_E = h->g_audit = h->g_res = nullptr;
+    h->g_nchem = h->g_list = h->g_info = nullptr;
     h->g_prim = nullptr;
     h->g_cap = 0;
     CK(cudaMalloc(&h->g_cs, (size_t)NV * cap * sizeof(double)));
@@ -1616,7 +1633,11 @@ int ensure_guest(eu3d_handle *h, long long cells)
     CK(cudaMalloc(&h->g_nchem, (size_t)cap * sizeof(int)));
     CK(cudaMalloc(&h->g_list, (size_t)cap * sizeof(int)));
     CK(cudaMalloc(&h->g_prim, (size_t)NPRIM * cap * prim_bytes(h)));
+    CK(cudaMalloc(&h->g_audit, (size_t)cap * sizeof(double)));
+    CK(cudaMalloc(&h->g_res, (size_t)(NS + 1) * cap * sizeof(double)));
+    CK(cudaMalloc(&h->g_info, (size_t)cap * sizeof(int)));
     if (!h->g_bins) CK(cudaMalloc(&h->g_bins, (3 * QBINS + 2) * sizeof(int)));
+    if (!h->g_count) CK(cudaMalloc(&h->g_count, 4 * sizeof(int)));
     h->g_cap = cap;
     return EU3D_OK;
 }
@@ -1705,6 +1726,150 @@ int eu3d_dlb_unpack(eu3d_handle *h, const double *back)
             k_dlb_unpack<double><<<blocks, 256, 0, h->st>>>(cell_args(h), sg, back, (double *)h->prim);
         else
             k_dlb_unpack<float><<<blocks, 256, 0, h->st>>>(cell_args(h), sg, back, (float *)h->prim);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Load balancing of the learned chemistry's FP64 fallback across ranks
+int eu3d_sur_load(eu3d_handle *h, long long *load)
+{
+    if (!h || !load) return fail(EU3D_ERR_ARG, "null argument");
+    if (!h->sur_count) return fail(EU3D_ERR_STATE, "no fallback list on this handle");
+    CK(cudaSetDevice(h->dev));
+    int cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, h->sur_count, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->sdlb_total = std::min<long long>(cnt, h->L.interior_cells());
+    h->sdlb_keep = h->sdlb_total;
+    h->sdlb_segs = DlbGuestSegs{};
+    *load = h->sdlb_total;
+    return EU3D_OK;
+}
+
+int eu3d_sdlb_select(eu3d_handle *h, int ntransfers, const long long *amount, long long *cells)
+{
+    if (!h || ntransfers < 0 || ntransfers > DLB_MAXSEG || (ntransfers && (!amount || !cells)))
+        return fail(EU3D_ERR_ARG, "bad arguments");
+    DlbGuestSegs &sg = h->sdlb_segs;
+    sg = DlbGuestSegs{};
+    sg.n = ntransfers;
+    long long left = h->sdlb_total;
+    for (int p = 0; p < ntransfers; p++) {
+        if (amount[p] < 0) return fail(EU3D_ERR_ARG, "negative amount");
+        cells[p] = std::min(amount[p], left);
+        left -= cells[p];
+    }
+    // the transfers take the last slots, segment p after segment p - 1
+    h->sdlb_keep = left;
+    for (int p = 0; p < ntransfers; p++) {
+        sg.off_in[p] = SDLB_OUT * sg.first[p];
+        sg.off_out[p] = SDLB_BACK * sg.first[p];
+        sg.first[p + 1] = sg.first[p] + cells[p];
+    }
+    return EU3D_OK;
+}
+
+int eu3d_sdlb_pack(eu3d_handle *h, double *buf)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    const DlbGuestSegs &sg = h->sdlb_segs;
+    const long long total = sg.first[sg.n];
+    if (total == 0) return EU3D_OK;
+    if (!buf) return fail(EU3D_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(h->dev));
+    const SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, h->L.interior_cells(), h->sur_res, h->sur_info};
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    {
+        ProfScope ps(h, "sdlb_pack");
+        k_sdlb_pack<<<blocks, 256, 0, h->st>>>(cell_args(h), qu, sg, h->sdlb_keep, buf);
+        k_sdlb_keep<<<1, 1, 0, h->st>>>(h->sur_count, (int)h->sdlb_keep);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+extern "C++" {
+namespace {
+template <class P, bool SPEC>
+void sdlb_guest_work(eu3d_handle *h, const DlbGuestSegs &sg, const double *in, double *out)
+{
+    const long long total = sg.first[sg.n];
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    k_sdlb_guest_in<<<blocks, 256, 0, h->st>>>(sg, in, h->g_cap, h->g_cs, h->g_T, h->g_audit, h->g_list);
+    k_sdlb_keep<<<1, 1, 0, h->st>>>(h->g_count, (int)total);
+    // the store as a field of g_cap cells: the fallback kernels read only the
+    // field stride of the layout and the cell of each list entry
+    CellArgs a = cell_args(h);
+    a.L.fs = h->g_cap;
+    a.cs = h->g_cs;
+    a.T = h->g_T;
+    a.E = h->g_E;
+    a.rhs = nullptr;
+    a.cs0 = nullptr;
+    a.wedge_on = 0;
+    const SurQueue qu{h->g_list, h->g_count, h->g_audit, h->g_cap, h->g_res, h->g_info};
+    {
+        ProfScope ps(h, "sdlb_guest_work");
+        k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(a, (P *)h->g_prim, qu);
+        k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(a, (P *)h->g_prim, qu);
+    }
+    k_sdlb_guest_out<P><<<blocks, 256, 0, h->st>>>(sg, h->g_cap, h->g_cs, h->g_T, h->g_E, (const P *)h->g_prim, out);
+}
+}  // namespace
+}  // extern "C++"
+
+int eu3d_sdlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *in, double *out)
+{
+    if (!h || nseg < 0 || nseg > DLB_MAXSEG || (nseg && !seg_cells)) return fail(EU3D_ERR_ARG, "bad arguments");
+    if (!h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached (eu3d_set_surrogate)");
+    DlbGuestSegs sg{};
+    sg.n = nseg;
+    for (int p = 0; p < nseg; p++) {
+        if (seg_cells[p] < 0) return fail(EU3D_ERR_ARG, "negative segment size");
+        sg.off_in[p] = SDLB_OUT * sg.first[p];
+        sg.off_out[p] = SDLB_BACK * sg.first[p];
+        sg.first[p + 1] = sg.first[p] + seg_cells[p];
+    }
+    const long long total = sg.first[nseg];
+    if (total == 0) return EU3D_OK;
+    if (!in || !out) return fail(EU3D_ERR_ARG, "null buffer");
+    if (total > (long long)SUR_CELL_MASK) return fail(EU3D_ERR_ARG, "too many received cells");
+    CK(cudaSetDevice(h->dev));
+    int rc = ensure_guest(h, total);
+    if (rc) return rc;
+    if (h->flux_bits == 64) {
+        if (h->spec)
+            sdlb_guest_work<double, true>(h, sg, in, out);
+        else
+            sdlb_guest_work<double, false>(h, sg, in, out);
+    } else {
+        if (h->spec)
+            sdlb_guest_work<float, true>(h, sg, in, out);
+        else
+            sdlb_guest_work<float, false>(h, sg, in, out);
+    }
+    CK(cudaGetLastError());
+    return EU3D_OK;
+}
+
+int eu3d_sdlb_unpack(eu3d_handle *h, const double *back)
+{
+    if (!h) return fail(EU3D_ERR_ARG, "null handle");
+    const DlbGuestSegs &sg = h->sdlb_segs;
+    const long long total = sg.first[sg.n];
+    if (total == 0) return EU3D_OK;
+    if (!back) return fail(EU3D_ERR_ARG, "null buffer");
+    CK(cudaSetDevice(h->dev));
+    const SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, h->L.interior_cells(), h->sur_res, h->sur_info};
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148 * 16);
+    {
+        ProfScope ps(h, "sdlb_unpack");
+        if (h->flux_bits == 64)
+            k_sdlb_unpack<double><<<blocks, 256, 0, h->st>>>(cell_args(h), qu, sg, h->sdlb_keep, back, (double *)h->prim);
+        else
+            k_sdlb_unpack<float><<<blocks, 256, 0, h->st>>>(cell_args(h), qu, sg, h->sdlb_keep, back, (float *)h->prim);
     }
     CK(cudaGetLastError());
     return EU3D_OK;

@@ -226,7 +226,7 @@ int sur_set_attrs()
 
 // ---------------------------------------------------------- coupled step
 template <class P, bool SPEC>
-void sur_chem_t(eu3d_handle *h, bool decoded)
+void sur_predict_t(eu3d_handle *h, bool decoded, const SurQueue &qu)
 {
     eu3d_surrogate *s = h->sur;
     const Layout &L = h->L;
@@ -237,7 +237,6 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
     // split step: the flux update and its decode first (Update_after_Adv),
     // unless the time scheme left the state decoded with the update in
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);
-    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n, h->sur_res, h->sur_info};
     SurApplyArgs a{cell_args(h), s->norm_d, h->sur_out, n, qu, h->sur_audit_stride};
     const SurSrcField<P> src{L, h->T, q, h->scal, h->sur_out, n, (L.ni + 127) / 128};
     const long long ntiles = src.ntiles();
@@ -280,22 +279,32 @@ void sur_chem_t(eu3d_handle *h, bool decoded)
         ProfScope ps(h, "sur_apply");
         k_sur_apply<P><<<cell_grid(L, 128), 128, 0, h->st>>>(a, q);
     }
-    {
+}
+
+template <class P, bool SPEC>
+void sur_chem_t(eu3d_handle *h, bool decoded, int half)
+{
+    const Layout &L = h->L;
+    const long long n = L.interior_cells();
+    P *q = (P *)h->prim;
+    SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n, h->sur_res, h->sur_info};
+    if (half & SUR_HALF_PREDICT) sur_predict_t<P, SPEC>(h, decoded, qu);
+    if (half & SUR_HALF_WORK) {
         ProfScope ps(h, "sur_fallback");
         k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
         k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
     }
 }
 
-int sur_chem_op(eu3d_handle *h, bool decoded)
+int sur_chem_op(eu3d_handle *h, bool decoded, int half)
 {
     if (!h->sur) return fail(EU3D_ERR_STATE, "no surrogate attached (eu3d_set_surrogate)");
     if (h->flux_bits == 64) {
-        if (h->spec) sur_chem_t<double, true>(h, decoded);
-        else sur_chem_t<double, false>(h, decoded);
+        if (h->spec) sur_chem_t<double, true>(h, decoded, half);
+        else sur_chem_t<double, false>(h, decoded, half);
     } else {
-        if (h->spec) sur_chem_t<float, true>(h, decoded);
-        else sur_chem_t<float, false>(h, decoded);
+        if (h->spec) sur_chem_t<float, true>(h, decoded, half);
+        else sur_chem_t<float, false>(h, decoded, half);
     }
     CK(cudaGetLastError());
     return EU3D_OK;

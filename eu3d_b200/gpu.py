@@ -45,10 +45,13 @@ EXPORTS = ["eu3d_last_error", "eu3d_create", "eu3d_destroy", "eu3d_upload_field"
            "eu3d_halo_unpack", "eu3d_cfl_local", "eu3d_dt_device", "eu3d_advance_time", "eu3d_wedge_fill",
            "eu3d_step_part", "eu3d_write_tecplot", "eu3d_write_wait", "eu3d_tecplot_write_host", "eu3d_dlb_plan",
            "eu3d_dlb_select_rows", "eu3d_chem_load", "eu3d_dlb_select", "eu3d_dlb_pack", "eu3d_dlb_guest",
-           "eu3d_dlb_unpack"]
+           "eu3d_dlb_unpack", "eu3d_sur_load", "eu3d_sdlb_select", "eu3d_sdlb_pack", "eu3d_sdlb_guest",
+           "eu3d_sdlb_unpack"]
 
 PART_STAGE1, PART_STAGE2, PART_REACT, PART_STAGE3, PART_CHEM_PREDICT, PART_CHEM_WORK = 0, 1, 2, 3, 4, 5
+PART_SUR_PREDICT, PART_SUR_WORK = 6, 7
 DLB_OUT_FIELDS, DLB_BACK_FIELDS, DLB_MAX_TRANSFERS = 15, 32, 64
+SDLB_OUT_FIELDS, SDLB_BACK_FIELDS = 16, 31
 
 SUR_NPARAM = 37264
 SUR_NORM_LEN = 80
@@ -183,6 +186,11 @@ def load_library(path: Optional[str] = None):
     L.eu3d_dlb_pack.argtypes = h + [C.c_void_p]
     L.eu3d_dlb_guest.argtypes = h + [C.c_int, _lp, C.c_void_p, C.c_void_p]
     L.eu3d_dlb_unpack.argtypes = h + [C.c_void_p]
+    L.eu3d_sur_load.argtypes = h + [_lp]
+    L.eu3d_sdlb_select.argtypes = h + [C.c_int, _lp, _lp]
+    L.eu3d_sdlb_pack.argtypes = h + [C.c_void_p]
+    L.eu3d_sdlb_guest.argtypes = h + [C.c_int, _lp, C.c_void_p, C.c_void_p]
+    L.eu3d_sdlb_unpack.argtypes = h + [C.c_void_p]
     L.eu3d_profile_enable.argtypes = h + [C.c_int]
     L.eu3d_profile_read.argtypes = h + [C.c_char_p, C.c_size_t, _dp, C.POINTER(C.c_longlong), C.c_int,
                                         C.POINTER(C.c_int)]
@@ -415,6 +423,33 @@ class DeviceFlowfield:
 
     def dlb_unpack(self, src_ptr: int):
         _check(self.L.eu3d_dlb_unpack(self.h, C.c_void_p(src_ptr)))
+
+    # ---- load balancing of the learned chemistry's FP64 fallback across ranks
+    def sur_load(self) -> int:
+        """The fallback list length after PART_SUR_PREDICT (synchronises)."""
+        v = C.c_longlong()
+        _check(self.L.eu3d_sur_load(self.h, C.byref(v)))
+        return v.value
+
+    def sdlb_select(self, amounts):
+        """Cells of this rank's transfers, taken from the end of its fallback list."""
+        n = len(amounts)
+        a = np.ascontiguousarray(amounts, dtype=np.int64)
+        cells = np.zeros(n, dtype=np.int64)
+        lp = C.POINTER(C.c_longlong)
+        _check(self.L.eu3d_sdlb_select(self.h, n, a.ctypes.data_as(lp), cells.ctypes.data_as(lp)))
+        return cells
+
+    def sdlb_pack(self, dst_ptr: int):
+        _check(self.L.eu3d_sdlb_pack(self.h, C.c_void_p(dst_ptr)))
+
+    def sdlb_guest(self, seg_cells, src_ptr: int, dst_ptr: int):
+        s = np.ascontiguousarray(seg_cells, dtype=np.int64)
+        _check(self.L.eu3d_sdlb_guest(self.h, len(s), s.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                      C.c_void_p(src_ptr), C.c_void_p(dst_ptr)))
+
+    def sdlb_unpack(self, src_ptr: int):
+        _check(self.L.eu3d_sdlb_unpack(self.h, C.c_void_p(src_ptr)))
 
     def cfl_local(self, cfl: float, final_time: float):
         """This rank's CFL dt into the device scalar (time not advanced)."""

@@ -31,6 +31,12 @@ DynamicLoadBalancer does it (src/LoadBalance.cpp:8-159, src/Euler.cpp:380-700):
     all-reduce the cells per transfer -> packets to the receivers -> own cells
     -> received cells -> results back to the senders -> unpacked
 
+With `dlb` set and the learned chemistry (react SURROGATE) the same protocol
+balances its FP64 fallback: the predict half is the gate, network and apply,
+a rank's load the length of its fallback list, and the transfers take the
+last slots of that list (the rejected cells gather at the detonation front,
+so the slabs it crosses carry most of them).
+
 The result equals the unbalanced step bit for bit.
 
 Layouts: "partition" gives every interior cell to one rank; "reference"
@@ -91,7 +97,7 @@ class StepSpec:
     bc_kind: int = gpu.BC_RSBI
     cfl: float = 0.0
     final_time: float = 1.0
-    dlb: bool = False       # balance the adaptive trapezoid across ranks
+    dlb: bool = False       # balance the adaptive trapezoid / the learned chemistry's fallback across ranks
     dlb_tol: float = 0.0    # ... when the load degree exceeds this
 
     def kw(self) -> dict:
@@ -100,7 +106,12 @@ class StepSpec:
         return d
 
     def balanced(self) -> bool:
-        return self.dlb and self.react == gpu.REACT_TRAPEZOID and self.type_ == 1
+        return self.dlb and ((self.react == gpu.REACT_TRAPEZOID and self.type_ == 1)
+                             or self.react == gpu.REACT_SURROGATE)
+
+    def balance_kind(self) -> str:
+        """"sur": the learned chemistry's fallback list; "trap": the adaptive trapezoid's rows."""
+        return "sur" if self.react == gpu.REACT_SURROGATE else "trap"
 
 
 class Slab:
@@ -108,6 +119,7 @@ class Slab:
 
     def __init__(self, rank: int, nranks: int, overlap: int, wedge: bool):
         self.rank, self.nranks, self.overlap, self.wedge = rank, nranks, overlap, wedge
+        self.kind = "trap"  # what the balancing operations move (StepSpec.balance_kind)
 
     def sides(self):
         """Faces with a neighbour: 0 (low x) and/or 1 (high x)."""
@@ -131,9 +143,10 @@ class Slab:
     def recv_buffer(self, side): raise NotImplementedError
     def unpack(self, side): raise NotImplementedError
     def part(self, part, spec: StepSpec): raise NotImplementedError
-    # load balancing: chem_load() -> int; dlb_select(amounts) -> cells per
-    # transfer; dlb_pack(); dlb_guest(seg_cells); dlb_unpack(); and the packet
-    # segments out_seg(t) / in_seg(t) / guest_seg(t) / back_seg(t) of transfer t
+    # load balancing (of self.kind): chem_load() -> int; dlb_select(amounts)
+    # -> cells per transfer; dlb_pack(); dlb_guest(seg_cells); dlb_unpack();
+    # and the packet segments out_seg(t) / in_seg(t) / guest_seg(t) /
+    # back_seg(t) of transfer t
     def chem_load(self): raise NotImplementedError
     def dlb_select(self, amounts): raise NotImplementedError
     def dlb_alloc(self, n_out, n_in): raise NotImplementedError
@@ -161,14 +174,18 @@ class Slab:
             self.part(gpu.PART_REACT, spec)
 
     def _balanced_chemistry(self, spec):
-        self.part(gpu.PART_CHEM_PREDICT, spec)
+        self.kind = spec.balance_kind()
+        sur = self.kind == "sur"
+        predict = gpu.PART_SUR_PREDICT if sur else gpu.PART_CHEM_PREDICT
+        work = gpu.PART_SUR_WORK if sur else gpu.PART_CHEM_WORK
+        self.part(predict, spec)
         self.load = int(self.chem_load())
         yield "loads"  # -> self.loads, every rank's load in rank order
         plan = gpu.dlb_plan(self.loads) if gpu.load_degree(self.loads) > spec.dlb_tol else []
         self.plan = plan
         self.last_plan = plan
         if not plan:
-            self.part(gpu.PART_CHEM_WORK, spec)
+            self.part(work, spec)
             return
         self.mine = [t for t, (s, _, _) in enumerate(plan) if s == self.rank]
         self.theirs = [t for t, (_, r, _) in enumerate(plan) if r == self.rank]
@@ -182,7 +199,7 @@ class Slab:
         # reference overlaps its non-blocking sends the same way,
         # src/Euler.cpp:488-518); the guest work waits for them
         yield "dlb_out_start"
-        self.part(gpu.PART_CHEM_WORK, spec)
+        self.part(work, spec)
         yield "dlb_out_wait"
         self.dlb_guest([c[t] for t in self.theirs])
         yield "dlb_back"
@@ -259,33 +276,43 @@ class DeviceSlab(Slab):
     def part(self, part, spec):
         self.d.step_part(part, **spec.kw())
 
-    # load balancing: packets are torch CUDA tensors of doubles
+    # load balancing: packets are torch CUDA tensors of doubles; self.kind
+    # picks the trapezoid's rows or the learned chemistry's fallback list
     def chem_load(self):
-        return self.d.chem_load()
+        return self.d.sur_load() if self.kind == "sur" else self.d.chem_load()
 
     def dlb_select(self, amounts):
+        if self.kind == "sur":
+            return self.d.sdlb_select(amounts)
         cells, _ = self.d.dlb_select(amounts)
         return cells
 
+    def _fields(self):
+        if self.kind == "sur":
+            return gpu.SDLB_OUT_FIELDS, gpu.SDLB_BACK_FIELDS
+        return gpu.DLB_OUT_FIELDS, gpu.DLB_BACK_FIELDS
+
     def dlb_alloc(self, n_out, n_in):
         dev, f64 = f"cuda:{self.d.device}", self.torch.float64
-        self._out = self.torch.empty(max(1, n_out * gpu.DLB_OUT_FIELDS), dtype=f64, device=dev)
-        self._back_in = self.torch.empty(max(1, n_out * gpu.DLB_BACK_FIELDS), dtype=f64, device=dev)
-        self._in = self.torch.empty(max(1, n_in * gpu.DLB_OUT_FIELDS), dtype=f64, device=dev)
-        self._guest = self.torch.empty(max(1, n_in * gpu.DLB_BACK_FIELDS), dtype=f64, device=dev)
-        self._o_out = self._offsets(self.mine, gpu.DLB_OUT_FIELDS)
-        self._o_back = self._offsets(self.mine, gpu.DLB_BACK_FIELDS)
-        self._o_in = self._offsets(self.theirs, gpu.DLB_OUT_FIELDS)
-        self._o_guest = self._offsets(self.theirs, gpu.DLB_BACK_FIELDS)
+        fo, fb = self._fields()
+        self._out = self.torch.empty(max(1, n_out * fo), dtype=f64, device=dev)
+        self._back_in = self.torch.empty(max(1, n_out * fb), dtype=f64, device=dev)
+        self._in = self.torch.empty(max(1, n_in * fo), dtype=f64, device=dev)
+        self._guest = self.torch.empty(max(1, n_in * fb), dtype=f64, device=dev)
+        self._o_out = self._offsets(self.mine, fo)
+        self._o_back = self._offsets(self.mine, fb)
+        self._o_in = self._offsets(self.theirs, fo)
+        self._o_guest = self._offsets(self.theirs, fb)
 
     def dlb_pack(self):
-        self.d.dlb_pack(self._out.data_ptr())
+        (self.d.sdlb_pack if self.kind == "sur" else self.d.dlb_pack)(self._out.data_ptr())
 
     def dlb_guest(self, seg_cells):
-        self.d.dlb_guest(seg_cells, self._in.data_ptr(), self._guest.data_ptr())
+        guest = self.d.sdlb_guest if self.kind == "sur" else self.d.dlb_guest
+        guest(seg_cells, self._in.data_ptr(), self._guest.data_ptr())
 
     def dlb_unpack(self):
-        self.d.dlb_unpack(self._back_in.data_ptr())
+        (self.d.sdlb_unpack if self.kind == "sur" else self.d.dlb_unpack)(self._back_in.data_ptr())
 
     def out_seg(self, t):
         a, b = self._o_out[t]

@@ -225,6 +225,13 @@ int eu3d_wedge_fill(eu3d_handle *h);
    PREDICT then WORK equals REACT. */
 #define EU3D_PART_CHEM_PREDICT 4
 #define EU3D_PART_CHEM_WORK 5
+/* the learned chemistry (react SURROGATE) in two halves, for load balancing of its FP64
+   fallback (new): SUR_PREDICT = the flux update (unless the stages left it decoded), the
+   frozen-chemistry gate, the network and its apply, ending with the fallback list;
+   SUR_WORK = the fallback integration of the list slots kept (all of them unless
+   eu3d_sdlb_pack sent some away).  SUR_PREDICT then SUR_WORK equals REACT. */
+#define EU3D_PART_SUR_PREDICT 6
+#define EU3D_PART_SUR_WORK 7
 int eu3d_step_part(eu3d_handle *h, const eu3d_step_desc *s, int part);
 
 /* Dynamic load balancing of the adaptive trapezoid across ranks (replaces the reference's
@@ -266,6 +273,31 @@ int eu3d_dlb_pack(eu3d_handle *h, double *dev_out);
    writes the return segments, concatenated in the same order, to dev_back */
 int eu3d_dlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *dev_in, double *dev_back);
 int eu3d_dlb_unpack(eu3d_handle *h, const double *dev_back);
+
+/* Load balancing of the learned chemistry's FP64 fallback across ranks (new: the reference
+   has no learned chemistry; the protocol is the one above, with the fallback list in place
+   of the trapezoid's rows).  The rejected and audited cells gather at the detonation front,
+   so the slabs it crosses carry most of the fallback.  A rank's load is the length of its
+   fallback list.  Per step, on every rank:
+     eu3d_step_part(SUR_PREDICT); eu3d_sur_load -> all-gather the loads; eu3d_dlb_plan;
+     senders: eu3d_sdlb_select (cells per transfer, taken from the end of the list) and
+     eu3d_sdlb_pack (EU3D_SDLB_OUT_FIELDS doubles per cell, segments in plan order);
+     eu3d_step_part(SUR_WORK) on the slots kept;
+     receivers: eu3d_sdlb_guest -> EU3D_SDLB_BACK_FIELDS doubles per cell, sent back;
+     senders: eu3d_sdlb_unpack.
+   Packets are field-major per segment: out CS[13], T, the audit temperature, the list
+   flags; back CS[13], T, E, the 16 primitives.  The result equals the unbalanced step bit
+   for bit; the receivers' status counts the fallback work they did.  Device buffers, the
+   handle's stream; eu3d_sur_load synchronises it. */
+#define EU3D_SDLB_OUT_FIELDS 16
+#define EU3D_SDLB_BACK_FIELDS 31
+/* the fallback list length after SUR_PREDICT */
+int eu3d_sur_load(eu3d_handle *h, long long *load);
+/* cells per transfer (amounts in plan order), taken as consecutive list slots from its end */
+int eu3d_sdlb_select(eu3d_handle *h, int ntransfers, const long long *amount, long long *cells);
+int eu3d_sdlb_pack(eu3d_handle *h, double *dev_out);
+int eu3d_sdlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *dev_in, double *dev_back);
+int eu3d_sdlb_unpack(eu3d_handle *h, const double *dev_back);
 
 /* Launch settings picked per handle (new): z planes walked by one flux block
    (default: 64, halved while the flux grid has fewer than four waves),

@@ -62,10 +62,14 @@ def test_constants_match_quirk_header():
     assert {k: int(v) for k, v in parts.items()} == {
         "EU3D_PART_STAGE1": gpu.PART_STAGE1, "EU3D_PART_STAGE2": gpu.PART_STAGE2, "EU3D_PART_REACT": gpu.PART_REACT,
         "EU3D_PART_STAGE3": gpu.PART_STAGE3, "EU3D_PART_CHEM_PREDICT": gpu.PART_CHEM_PREDICT,
-        "EU3D_PART_CHEM_WORK": gpu.PART_CHEM_WORK}
+        "EU3D_PART_CHEM_WORK": gpu.PART_CHEM_WORK, "EU3D_PART_SUR_PREDICT": gpu.PART_SUR_PREDICT,
+        "EU3D_PART_SUR_WORK": gpu.PART_SUR_WORK}
     dlb = dict(re.findall(r"#define (EU3D_DLB_\w+) (\d+)", text))
     assert (int(dlb["EU3D_DLB_OUT_FIELDS"]), int(dlb["EU3D_DLB_BACK_FIELDS"]), int(dlb["EU3D_DLB_MAX_TRANSFERS"])) == \
         (gpu.DLB_OUT_FIELDS, gpu.DLB_BACK_FIELDS, gpu.DLB_MAX_TRANSFERS)
+    sdlb = dict(re.findall(r"#define (EU3D_SDLB_\w+) (\d+)", text))
+    assert (int(sdlb["EU3D_SDLB_OUT_FIELDS"]), int(sdlb["EU3D_SDLB_BACK_FIELDS"])) == \
+        (gpu.SDLB_OUT_FIELDS, gpu.SDLB_BACK_FIELDS)
 
 
 def test_null_arguments_are_rejected_without_a_device(lib):

@@ -204,6 +204,50 @@ def test_dlb_odw_wedge_slabs_equal_single_domain(mech):
     assert any(plans), plans
 
 
+@pytest.mark.parametrize("flux_bits", [32, 64])
+def test_dlb_surrogate_fallback_slabs_equal_single_domain(mech, flux_bits):
+    """The learned chemistry's FP64 fallback balanced across three slabs with
+    the immersed wedge: every accepted cell is audited (audit stride 1, the
+    same cells on the slabs as on the single domain), so each slab's fallback
+    list holds its fluid cells and the slabs the wedge takes cells from carry
+    less.  The loaded slab hands the last cells of its list to the others,
+    which integrate them and send them back -- bit for bit the unbalanced
+    single domain; the fallback, audit and substep counts summed over the
+    slabs equal the single domain's, and so does the largest audit
+    difference."""
+    case = odw_case(mech, 128, 48, 6, L=0.05)
+    model = S.SurrogateModel.load(S.DEFAULT_MODEL)
+
+    def setup(d):
+        setup_odw(d, case)
+        d._model_sur = model.attach(d, 1)
+
+    full = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=flux_bits)
+    setup(full)
+    warm = StepSpec(react=gpu.REACT_IMEX, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0, final_time=1.0)
+    full.dt = 4e-8
+    for _ in range(30):
+        full.step(**warm.kw())
+    full.synchronize()
+    pieces = _cut(full, mech, case.grid, 3, "partition", flux_bits, setup)
+    spec = StepSpec(react=gpu.REACT_SURROGATE, timeadv=gpu.ADV_SSPRK2, bc_kind=gpu.BC_ODM, cfl=0.0, final_time=1.0,
+                    dlb=True)
+    full.reset_status()
+    for _, _, d in pieces:
+        d.reset_status()
+    slabs, plans = _dlb_run(full, pieces, spec, 2, wedge=True)
+    _compare(full, pieces, names=("CS", "T", "P", "Yi", "E"))
+    assert all(plans), plans
+    assert plans[0][0][0] == 0, plans  # the inflow slab has no wedge cells: the most fallback
+    assert sum(slabs[0].counts[t] for t in slabs[0].mine) > 0
+    st = [d.status() for _, _, d in pieces]
+    sf = full.status()
+    for key in ("surrogate_fallback", "surrogate_audited", "surrogate_cells", "substeps", "newton_capped"):
+        assert sum(x[key] for x in st) == sf[key], key
+    assert max(x["surrogate_audit_max_dT"] for x in st) == sf["surrogate_audit_max_dT"]
+    assert sf["surrogate_audited"] > 0
+
+
 @pytest.mark.parametrize("flux_bits", [64, 32])
 def test_weno_rk3_slabs_equal_single_domain(mech, flux_bits):
     """WENO + SSP-RK3 on three device slabs equal the single domain bit for bit."""
