@@ -567,7 +567,7 @@ def run_ours(a, rank, world, local):
     return out
 
 
-def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
+def run_e2e(dev, step, K, cells, torch, world=1, dist=None, chemistry="surrogate chemistry"):
     """The same metric through the C ABI with host buffers: upload CS, T, E
     from pinned host memory, decode, K steps each followed by a status read,
     download CS and T -- all inside the timed region (N > 1: each rank its
@@ -600,7 +600,7 @@ def run_e2e(dev, step, K, cells, torch, world=1, dist=None):
     d2h = host["CS"].nbytes + host["T"].nbytes + K * 96
     return {"value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
             "d2h_bytes_per_step": d2h // K, "ms": ms,
-            "protocol": "upload CS,T,E (pinned) + decode, K eu3d_step calls (surrogate chemistry) each with a status "
+            "protocol": f"upload CS,T,E (pinned) + decode, K eu3d_step calls ({chemistry}) each with a status "
                         "read, download CS,T; the state stays on the device between steps (the drop-in's design), "
                         "so the host copies are amortised over the K steps and the value depends on K"}
 
@@ -742,7 +742,7 @@ def run_znd(a):
     units = {k: cells for k in kernel_work(8)}
     timing, profs, stats, clocks, rf, rates = _case_run(dev, forms, K, W, torch, cells, units, 8, "imex")
     reset()
-    e2e = run_e2e(dev, forms["imex"][1], K, cells, torch)
+    e2e = run_e2e(dev, forms["imex"][1], K, cells, torch, chemistry="FP64 IMEX")
     dev.close()
 
     def make():
@@ -820,7 +820,7 @@ def run_odw2d(a):
         rates_all.update(rates)
         if bits == 32:
             reset(0)
-            e2e = run_e2e(dev, forms["imex_fp32"][1], K, cells, torch)
+            e2e = run_e2e(dev, forms["imex_fp32"][1], K, cells, torch, chemistry="FP64 IMEX, FP32 flux")
         dev.close()
     src.close()
     rf, clocks, stats = results[32]
@@ -888,7 +888,7 @@ def run_rsbi(a):
         if bits == 32:
             rf, clocks, stats32 = r, clk, stats["fp32"]
             reset()
-            e2e = run_e2e(dev, base, K, cells, torch)
+            e2e = run_e2e(dev, base, K, cells, torch, chemistry="FP64 IMEX, FP32 flux")
         dev.close()
     finite = np.isfinite(fields[64]["T"]) & np.isfinite(fields[32]["T"])
     err = field_errors(fields[64], fields[32], finite, mech.species)
