@@ -391,7 +391,8 @@ def chem_roofline(profs, stats, fluid, steps_run, K):
 
 # kernels of the step that make up its chemistry (the rest: ghost fills, CFL,
 # flux sweeps and stage updates)
-CHEM_KERNELS = {"cell_imex", "cell_adapt", "sur_gate", "sur_mlp", "sur_apply", "sur_fallback", "sur_mlp_apply"}
+CHEM_KERNELS = {"cell_imex", "cell_adapt", "sur_gate", "sur_mlp", "sur_apply", "sur_fallback", "sur_fallback_finish",
+                "sur_mlp_apply"}
 
 
 def developed_state(mech, ni, nj, nk, steps2d, seed):
@@ -824,7 +825,7 @@ def run_odw2d(a):
         dev.close()
     src.close()
     rf, clocks, stats = results[32]
-    chem = {f: sum(v[0] for k, v in profs_all[f].items() if k in CHEM_KERNELS | {"adapt_list", "adapt_queue"}) / K
+    chem = {f: sum(v[0] for k, v in profs_all[f].items() if k in CHEM_KERNELS | {"adapt_list", "adapt_queue", "adapt_finish"}) / K
             for f in ("adaptive_thread_per_cell", "adaptive_queue")}
     cb = cpu_baseline(slab=(64, 32, 2))
     return _line("Mcell-steps/s, 2D ODW 1024x512, FP32 flux / FP64 state, IMEX", rates_all["imex_fp32"], UNIT, K, W,

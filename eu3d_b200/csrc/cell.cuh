@@ -628,7 +628,10 @@ __device__ __forceinline__ void cell_body(const CellArgs &a, P *__restrict__ q)
     const double dt = a.scal[0];
     double cs[NV];
     load_cs(a.cs, fs, c, cs);
-    double T = a.T[c], Eold = a.E[c];
+    // the previous decode's energy is the Newton target only under the
+    // stale-energy quirk; otherwise it is not read
+    double T = a.T[c];
+    const double Eold = (qk & EU3D_Q_STALE_E) ? a.E[c] : 0.0;
     Decoded o;
     int capped = 0, capped_any = 0;
 

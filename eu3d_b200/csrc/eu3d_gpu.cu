@@ -860,8 +860,11 @@ void adapt_queue_t(eu3d_handle *h, bool decoded)
         ProfScope ps(h, "adapt_list");
         k_list_fluid<<<cell_grid(L, 256), 256, 0, h->st>>>(cell_args(h), qu);
     }
-    ProfScope ps(h, "adapt_queue");
-    k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+    {
+        ProfScope ps(h, "adapt_queue");
+        k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+    }
+    ProfScope ps(h, "adapt_finish");
     k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
 }
 
@@ -1813,6 +1816,9 @@ void sdlb_guest_work(eu3d_handle *h, const DlbGuestSegs &sg, const double *in, d
     {
         ProfScope ps(h, "sdlb_guest_work");
         k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(a, (P *)h->g_prim, qu);
+    }
+    {
+        ProfScope ps(h, "sdlb_guest_finish");
         k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(a, (P *)h->g_prim, qu);
     }
     k_sdlb_guest_out<P><<<blocks, 256, 0, h->st>>>(sg, h->g_cap, h->g_cs, h->g_T, h->g_E, (const P *)h->g_prim, out);

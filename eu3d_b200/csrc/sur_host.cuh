@@ -290,8 +290,11 @@ void sur_chem_t(eu3d_handle *h, bool decoded, int half)
     SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, n, h->sur_res, h->sur_info};
     if (half & SUR_HALF_PREDICT) sur_predict_t<P, SPEC>(h, decoded, qu);
     if (half & SUR_HALF_WORK) {
-        ProfScope ps(h, "sur_fallback");
-        k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+        {
+            ProfScope ps(h, "sur_fallback");
+            k_sur_fallback<P, SPEC><<<h->nparts, 128, 0, h->st>>>(cell_args(h), q, qu);
+        }
+        ProfScope ps(h, "sur_fallback_finish");
         k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
     }
 }

@@ -133,3 +133,110 @@ def make_slabs(nranks, rows=12, width=5, seed=0):
 
 def unbalanced(slabs_data):
     return [np.where(s, v, chem(v, predict(v))) for v, s in slabs_data]
+
+
+# ----------------------------------------------------------------------------
+# The learned chemistry's fallback list (the "sur" kind of the protocol): the
+# cells above a threshold are "rejected" and listed; the stand-in integration
+# depends only on the cell's own value; a sender's transfers take the last
+# slots of its list, as eu3d_sdlb_select does.  One field per packet cell.
+def rejected(vals, solid):
+    return (vals > 0.6) & ~solid
+
+
+def chem_one(v):
+    out = v.copy()
+    for n in range(6):
+        out = out * 0.997 + 0.25 / (n + 1) * np.sin(out)
+    return out
+
+
+class HostListSlab(Slab):
+    def __init__(self, vals, solid, rank, nranks, order_seed=0):
+        super().__init__(rank, nranks, 0, False)
+        self.vals = np.array(vals, dtype=np.float64)
+        self.solid = np.array(solid, dtype=bool)
+        self.rng = np.random.default_rng(order_seed + 7 * rank)
+        self.list = np.zeros(0, dtype=np.int64)
+        self.keep = 0
+
+    def step(self, spec):
+        if spec.balanced():
+            yield from self._balanced_chemistry(spec)
+        else:
+            self.part(gpu.PART_REACT, spec)
+
+    def part(self, part, spec):
+        flat = self.vals.reshape(-1)
+        if part in (gpu.PART_SUR_PREDICT, gpu.PART_REACT):
+            # the device appends with atomics: the list order is arbitrary
+            self.list = self.rng.permutation(np.flatnonzero(rejected(self.vals, self.solid).reshape(-1)))
+            self.keep = len(self.list)
+        if part in (gpu.PART_SUR_WORK, gpu.PART_REACT):
+            kept = self.list[:self.keep]
+            flat[kept] = chem_one(flat[kept])
+
+    def chem_load(self):
+        return len(self.list)
+
+    def dlb_select(self, amounts):
+        left, cells = len(self.list), []
+        for a in amounts:
+            c = min(int(a), left)
+            cells.append(c)
+            left -= c
+        self.keep = left
+        self.seg = np.concatenate([[0], np.cumsum(cells)]).astype(np.int64)
+        return np.array(cells, dtype=np.int64)
+
+    def dlb_alloc(self, n_out, n_in):
+        z = lambda n: torch.zeros(max(1, n), dtype=torch.float64)
+        self._out, self._back, self._in, self._guest = z(n_out), z(n_out), z(n_in), z(n_in)
+        self._o_out = self._offsets(self.mine, 1)
+        self._o_in = self._offsets(self.theirs, 1)
+
+    def dlb_pack(self):
+        flat = self.vals.reshape(-1)
+        for p, t in enumerate(self.mine):
+            a, b = self._o_out[t]
+            slots = self.list[self.keep + self.seg[p]:self.keep + self.seg[p + 1]]
+            self._out[a:b] = torch.from_numpy(flat[slots].copy())
+
+    def dlb_guest(self, seg_cells):
+        for t in self.theirs:
+            a, b = self._o_in[t]
+            self._guest[a:b] = torch.from_numpy(chem_one(self._in[a:b].numpy()))
+
+    def dlb_unpack(self):
+        flat = self.vals.reshape(-1)
+        for p, t in enumerate(self.mine):
+            a, b = self._o_out[t]
+            slots = self.list[self.keep + self.seg[p]:self.keep + self.seg[p + 1]]
+            flat[slots] = self._back[a:b].numpy()
+
+    def out_seg(self, t):
+        a, b = self._o_out[t]
+        return self._out[a:b]
+
+    def back_seg(self, t):
+        a, b = self._o_out[t]
+        return self._back[a:b]
+
+    def in_seg(self, t):
+        a, b = self._o_in[t]
+        return self._in[a:b]
+
+    def guest_seg(self, t):
+        a, b = self._o_in[t]
+        return self._guest[a:b]
+
+
+def unbalanced_list(slabs_data, steps=1):
+    out = []
+    for v, s in slabs_data:
+        v = v.copy()
+        for _ in range(steps):
+            m = rejected(v, s)
+            v[m] = chem_one(v[m])
+        out.append(v)
+    return out

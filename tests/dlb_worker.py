@@ -2,7 +2,10 @@
 (tests/_dlb_host.py) stepped through SlabRun with torch.distributed (gloo);
 its values and the plan are written to an .npz for the parent test.
 
-    python tests/dlb_worker.py RANK WORLD PORT OUT STEPS"""
+    python tests/dlb_worker.py RANK WORLD PORT OUT STEPS [KIND]
+
+KIND "trap" (default): the adaptive trapezoid's rows (HostSlab); "sur": the
+learned chemistry's fallback list (HostListSlab)."""
 import os
 import sys
 
@@ -15,7 +18,7 @@ from datetime import timedelta  # noqa: E402
 import numpy as np  # noqa: E402
 import torch.distributed as dist  # noqa: E402
 
-from _dlb_host import HostSlab, make_slabs  # noqa: E402
+from _dlb_host import HostListSlab, HostSlab, make_slabs  # noqa: E402
 from eu3d_b200 import gpu  # noqa: E402
 from eu3d_b200.slabs import SlabRun, StepSpec, TorchTransport  # noqa: E402
 
@@ -24,9 +27,14 @@ def main():
     rank, world, port, out, steps = int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]), sys.argv[4], int(sys.argv[5])
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
                             timeout=timedelta(seconds=60))
+    kind = sys.argv[6] if len(sys.argv) > 6 else "trap"
     vals, solid = make_slabs(world)[rank]
-    slab = HostSlab(vals, solid, rank, world)
-    spec = StepSpec(react=gpu.REACT_TRAPEZOID, type_=1, dlb=True)
+    if kind == "sur":
+        slab = HostListSlab(vals, solid, rank, world)
+        spec = StepSpec(react=gpu.REACT_SURROGATE, dlb=True)
+    else:
+        slab = HostSlab(vals, solid, rank, world)
+        spec = StepSpec(react=gpu.REACT_TRAPEZOID, type_=1, dlb=True)
     SlabRun([slab], TorchTransport()).run(steps, spec)
     plan = np.array(slab.last_plan, dtype=np.int64).reshape(-1, 3)
     np.savez(out, vals=slab.vals, plan=plan, loads=np.array(slab.loads))

@@ -20,7 +20,7 @@ import sys
 import numpy as np
 import pytest
 
-from _dlb_host import HostSlab, chem, make_slabs, predict
+from _dlb_host import HostListSlab, HostSlab, chem, make_slabs, predict, unbalanced_list
 from dlb_oracle import dlb_plan as oracle_plan
 from eu3d_b200 import gpu
 from eu3d_b200.slabs import LoopbackTransport, SlabRun, StepSpec
@@ -145,6 +145,41 @@ def test_three_gloo_ranks_equal_unbalanced(tmp_path):
         assert np.array_equal(res[r]["vals"], want), r
     assert len(res[0]["plan"]) > 0
     assert all(np.array_equal(res[0]["plan"], x["plan"]) for x in res)
+
+
+def test_loopback_fallback_list_slabs_equal_unbalanced():
+    """The learned chemistry's kind of the protocol on host slabs: the hot
+    rank's fallback list is the longest, its last slots travel (in an
+    arbitrary list order, as the device's atomic appends leave it), and
+    every cell ends as the unbalanced step leaves it."""
+    _library_or_skip()
+    data = make_slabs(3)
+    slabs = [HostListSlab(v, s, r, 3) for r, (v, s) in enumerate(data)]
+    spec = StepSpec(react=gpu.REACT_SURROGATE, dlb=True)
+    assert spec.balanced() and spec.balance_kind() == "sur"
+    SlabRun(slabs, LoopbackTransport()).run(2, spec)
+    plan = slabs[0].last_plan
+    assert plan and all(p[0] == 0 for p in plan)
+    assert sum(slabs[0].counts[t] for t in slabs[0].mine) > 0
+    for got, want in zip([s.vals for s in slabs], unbalanced_list(data, 2)):
+        assert np.array_equal(got, want)
+
+
+def test_three_gloo_ranks_fallback_list_equal_unbalanced(tmp_path):
+    """The same as three gloo processes (torch.distributed collectives)."""
+    _library_or_skip()
+    port, world, steps = _free_port(), 3, 2
+    outs = [str(tmp_path / f"rank{r}.npz") for r in range(world)]
+    procs = [subprocess.Popen([sys.executable, os.path.join(HERE, "dlb_worker.py"), str(r), str(world), str(port),
+                               outs[r], str(steps), "sur"], stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+             for r in range(world)]
+    for p in procs:
+        out, _ = p.communicate(timeout=240)
+        assert p.returncode == 0, out.decode(errors="replace")[-2000:]
+    res = [np.load(o) for o in outs]
+    for r, want in enumerate(unbalanced_list(make_slabs(world), steps)):
+        assert np.array_equal(res[r]["vals"], want), r
+    assert len(res[0]["plan"]) > 0
 
 
 def test_entry_points_reject_bad_arguments():
