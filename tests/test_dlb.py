@@ -205,6 +205,11 @@ def test_entry_points_reject_bad_arguments():
     assert L.eu3d_dlb_select(None, 0, None, None, None) == -1
     assert L.eu3d_dlb_guest(None, 0, None, None, None) == -1
     assert b"null" in L.eu3d_last_error() or b"bad" in L.eu3d_last_error()
+    # the learned chemistry's fallback balancing
+    for fn in ("eu3d_sur_load", "eu3d_sdlb_pack", "eu3d_sdlb_unpack"):
+        assert getattr(L, fn)(None, None) == -1, fn
+    assert L.eu3d_sdlb_select(None, 0, None, None) == -1
+    assert L.eu3d_sdlb_guest(None, 0, None, None, None) == -1
 
 
 @pytest.mark.parametrize("nranks,seed", [(2, 1), (3, 2), (4, 3), (5, 4), (5, 5)])

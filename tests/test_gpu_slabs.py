@@ -271,3 +271,22 @@ def test_weno_rk3_slabs_equal_single_domain(mech, flux_bits):
     for _, _, d in pieces:
         d.synchronize()
     _compare(full, pieces)
+
+
+def test_sdlb_entry_points_reject_misuse(mech):
+    """The fallback balancing calls refuse what they cannot do: a fallback
+    list length without a list, negative amounts, a guest without an
+    attached network; an empty plan is a no-op."""
+    case = odw_case(mech, 32, 16, 4, L=0.05 * 31 / 127)
+    d = gpu.DeviceFlowfield(mech, case.grid, gpu.QUIRKS_FIXED, flux_bits=32)
+    setup_odw(d, case)
+    with pytest.raises(gpu.Eu3dError):
+        d.sur_load()
+    with pytest.raises(gpu.Eu3dError):
+        d.sdlb_select([-1])
+    with pytest.raises(gpu.Eu3dError):
+        d.sdlb_guest([4], 0, 0)
+    assert list(d.sdlb_select([])) == []
+    d.sdlb_pack(0)    # nothing selected: no packet, no pointer needed
+    d.sdlb_unpack(0)
+    d.close()
