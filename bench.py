@@ -71,6 +71,8 @@ def parse():
                     help="also compare on the benchmark's full grid (about 2.5 more minutes)")
     ap.add_argument("--develop", type=int, default=1500, help="2D steps that develop the timed state")
     ap.add_argument("--model", default=os.path.join(ROOT, "eu3d_b200", "data", "sur_h2_ja919.npz"))
+    ap.add_argument("--dlb", action="store_true",
+                    help="N > 1: balance the learned chemistry's FP64 fallback across the slabs (off by default)")
     ap.add_argument("--config", choices=list(CONFIGS), default="odw3d",
                     help="odw3d: the headline (3D ODW 512x256x256); znd, odw2d, rsbi, surrogate: the other "
                          "benchmark configurations, one GPU")
@@ -451,7 +453,9 @@ def run_ours(a, rank, world, local):
     def stepper(step):
         if run is None:
             return step
-        spec = StepSpec(**step)
+        # --dlb: the surrogate form balances its fallback list across the
+        # slabs (the other forms have nothing to balance in this protocol)
+        spec = StepSpec(**step, dlb=a.dlb and step["react"] == gpu.REACT_SURROGATE)
         return lambda: run.step(spec)
 
     W = max(a.warmup, 3)
@@ -514,7 +518,8 @@ def run_ours(a, rank, world, local):
                    "time": f"SSP-RK2, CFL {CFL}",
                    "state": f"developed: 2D case advanced {a.develop} steps with the FP64 adaptive integrator, "
                             f"extruded along z",
-                   "parallelism": (f"{world} x slabs of {n_loc} cells (NCCL halo send/recv, all-reduce MIN of dt)"
+                   "parallelism": (f"{world} x slabs of {n_loc} cells (NCCL halo send/recv, all-reduce MIN of dt"
+                                   + (", the surrogate's FP64 fallback balanced across the slabs)" if a.dlb else ")")
                                    if world > 1 else "1 GPU"),
                    "l2": "state ~12 GB per GPU >> 126 MB L2 (no flush needed)",
                    "graph": "one CUDA graph per step" if world == 1 else "per-op launches (halo exchanges between)",
