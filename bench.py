@@ -339,6 +339,21 @@ TRAFFIC_NOTE = {"advection": "ncu DRAM bytes of one launch on the 512x256x64 cas
                              "cell, times the fluid cells"}
 
 
+def step_roofline(ms, cells, fluid, hbm, src, stages=2):
+    """The flux-and-update part of a step against the HBM roofline, by the
+    per-step definition of the algorithmic bytes: per cell and RK stage the
+    conserved state read and written (13 x 8 B each) and T read and written
+    (2 x 8 B), 224 B; ms the step's non-chemistry time (flux, stage updates,
+    ghost fills, CFL)."""
+    per = 224 * stages
+    out = {"bound": "hbm", "per_cell": f"224 B x {stages} stages", "ms": ms, "peak": hbm, "unit": "GB/s",
+           "peak_source": src}
+    for name, n in (("all_cells", cells), ("fluid_cells", fluid)):
+        ach = per * n / (ms * 1e-3) / 1e9
+        out[name] = {"cells": n, "achieved": ach, "frac": ach / hbm}
+    return out
+
+
 def fluid_cells(case, i0=0, n_loc=None):
     """Interior cells of the case (or of the x slab i0 .. i0 + n_loc) outside its wedge."""
     g = case.grid
@@ -545,6 +560,7 @@ def run_ours(a, rank, world, local):
         "roofline": rf,
         "roofline_other_kernels": rf_more,
         "roofline_chemistry": chem_roofline(profs, statuses, fluid, a.steps + W, a.steps),
+        "roofline_step": step_roofline(split["surrogate"]["non_chemistry_ms"], n_loc * nj * nk, fluid, hbm, src),
         "status": {k: st[k] for k in ("nonfinite_cells", "newton_capped", "dt", "time")},
     }
     if clocks:
