@@ -2111,8 +2111,9 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     // the TMA ring needs the tensor map; without it the staged kernel runs (and is reported)
     h->flux_stage = (t->flux_stage == 2 && !h->tq_ok) ? 1 : t->flux_stage;
     h->sur_fused = t->sur_fused ? 1 : 0;
-    // (a build for 6 blocks, at 85 registers, scheduled the decode's
-    // arithmetic differently and changed results in the last bits: left out)
+    // (builds for 5 and 6 blocks, at 96 and 85 registers, scheduled the
+    // decode's arithmetic differently and changed results in the last bits:
+    // left out)
     if (t->cell_blocks != 3 && t->cell_blocks != 4) return fail(EU3D_ERR_ARG, "cell_blocks must be 3 or 4");
     h->cell_blocks = t->cell_blocks;
     h->adapt_queue = t->adapt_queue ? 1 : 0;
