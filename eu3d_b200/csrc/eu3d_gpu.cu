@@ -144,7 +144,7 @@ struct eu3d_handle {
     int *g_info = nullptr, *g_count = nullptr;
     // fallback load balancing: the list length of the last eu3d_sur_load, the
     // slots kept, the transfers this rank sends (segments of list slots)
-    long long sdlb_total = 0, sdlb_keep = 0;
+    long long sdlb_total = -1, sdlb_keep = 0;  // -1: no eu3d_sur_load since the last SUR_PREDICT
     DlbGuestSegs sdlb_segs{};
 };
 
@@ -1755,6 +1755,7 @@ int eu3d_sdlb_select(eu3d_handle *h, int ntransfers, const long long *amount, lo
 {
     if (!h || ntransfers < 0 || ntransfers > DLB_MAXSEG || (ntransfers && (!amount || !cells)))
         return fail(EU3D_ERR_ARG, "bad arguments");
+    if (h->sdlb_total < 0) return fail(EU3D_ERR_STATE, "eu3d_sur_load after the step's SUR_PREDICT first");
     DlbGuestSegs &sg = h->sdlb_segs;
     sg = DlbGuestSegs{};
     sg.n = ntransfers;

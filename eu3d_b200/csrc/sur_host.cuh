@@ -234,6 +234,10 @@ void sur_predict_t(eu3d_handle *h, bool decoded, const SurQueue &qu)
     P *q = (P *)h->prim;
     // [0] fallback list length, [1] its work cursor, [2] active list length
     cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
+    // a new list: the balancing of the previous one is void until eu3d_sur_load
+    h->sdlb_total = -1;
+    h->sdlb_keep = 0;
+    h->sdlb_segs = DlbGuestSegs{};
     // split step: the flux update and its decode first (Update_after_Adv),
     // unless the time scheme left the state decoded with the update in
     if (!decoded) launch_cell_t<P, SPEC>(h, M_ADV);

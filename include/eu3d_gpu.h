@@ -293,7 +293,8 @@ int eu3d_dlb_unpack(eu3d_handle *h, const double *dev_back);
 #define EU3D_SDLB_BACK_FIELDS 31
 /* the fallback list length after SUR_PREDICT */
 int eu3d_sur_load(eu3d_handle *h, long long *load);
-/* cells per transfer (amounts in plan order), taken as consecutive list slots from its end */
+/* cells per transfer (amounts in plan order), taken as consecutive list slots from its end;
+   EU3D_ERR_STATE unless eu3d_sur_load ran after the step's SUR_PREDICT */
 int eu3d_sdlb_select(eu3d_handle *h, int ntransfers, const long long *amount, long long *cells);
 int eu3d_sdlb_pack(eu3d_handle *h, double *dev_out);
 int eu3d_sdlb_guest(eu3d_handle *h, int nseg, const long long *seg_cells, const double *dev_in, double *dev_back);
