@@ -19,14 +19,41 @@ struct GhostArgs {
     int kind;
 };
 
+// Every fill loads all the values it copies before its first store.  The
+// destination of a fill is never a source of the same launch (ghost cells
+// take interior cells; the wedge band's solid cells take fluid ones), so the
+// order changes nothing but the timing: the compiler, which cannot prove
+// that the stores miss the later loads, would otherwise issue each load only
+// after the store before it, one memory round trip per field.
 template <class P>
-__device__ __forceinline__ void ghost_copy(const GhostArgs &a, P *q, long long d, long long s)
+__device__ __forceinline__ void ghost_load(const GhostArgs &a, const P *q, long long s, P v[NPRIM], double &T,
+                                           double &E)
 {
     const long long fs = a.L.fs;
 #pragma unroll
-    for (int f = 0; f < NPRIM; f++) q[f * fs + d] = q[f * fs + s];
-    a.T[d] = a.T[s];
-    a.E[d] = a.E[s];
+    for (int f = 0; f < NPRIM; f++) v[f] = q[f * fs + s];
+    T = a.T[s];
+    E = a.E[s];
+}
+
+template <class P>
+__device__ __forceinline__ void ghost_store(const GhostArgs &a, P *q, long long d, const P v[NPRIM], double T,
+                                            double E)
+{
+    const long long fs = a.L.fs;
+#pragma unroll
+    for (int f = 0; f < NPRIM; f++) q[f * fs + d] = v[f];
+    a.T[d] = T;
+    a.E[d] = E;
+}
+
+template <class P>
+__device__ __forceinline__ void ghost_copy(const GhostArgs &a, P *q, long long d, long long s)
+{
+    P v[NPRIM];
+    double T, E;
+    ghost_load(a, q, s, v, T, E);
+    ghost_store(a, q, d, v, T, E);
 }
 
 // mirror with the wall-side thermodynamic recompute of the reflective faces
@@ -35,19 +62,23 @@ template <class P>
 __device__ __forceinline__ void ghost_wall(const GhostArgs &a, P *q, long long d, long long s, bool flipv, bool flipw)
 {
     const long long fs = a.L.fs;
-    q[PU * fs + d] = q[PU * fs + s];
-    q[PV * fs + d] = flipv ? -q[PV * fs + s] : q[PV * fs + s];
-    q[PW * fs + d] = flipw ? -q[PW * fs + s] : q[PW * fs + s];
+    const P u = q[PU * fs + s], v = q[PV * fs + s], w = q[PW * fs + s];
     const P Pp = q[PP * fs + s];
-    q[PP * fs + d] = Pp;
+    P ys[NS];
+#pragma unroll
+    for (int sp = 0; sp < NS; sp++) ys[sp] = q[(PY + sp) * fs + s];
     const double T = a.T[s];
+    q[PU * fs + d] = u;
+    q[PV * fs + d] = flipv ? -v : v;
+    q[PW * fs + d] = flipw ? -w : w;
+    q[PP * fs + d] = Pp;
     a.T[d] = T;
     const TPow p = tpow(T, a.quirks);
     double Y[NS], rg = 0.0, cp = 0.0, h = 0.0, e = 0.0;
 #pragma unroll
     for (int sp = 0; sp < NS; sp++) {
-        Y[sp] = (double)q[(PY + sp) * fs + s];
-        q[(PY + sp) * fs + d] = q[(PY + sp) * fs + s];
+        Y[sp] = (double)ys[sp];
+        q[(PY + sp) * fs + d] = ys[sp];
     }
 #pragma unroll
     for (int sp = 0; sp < NS; sp++) {
@@ -94,17 +125,21 @@ __global__ void k_ghost_x(GhostArgs a, P *q)
         if (lower) {
             const long long p = (long long)(k - L.bc) * L.nj + (j - L.bc), pl = (long long)L.nj * L.nk;
             const long long fs = L.fs;
-            q[PU * fs + d] = (P)a.inflow[0 * pl + p];
-            q[PV * fs + d] = (P)a.inflow[1 * pl + p];
-            q[PW * fs + d] = (P)a.inflow[2 * pl + p];
-            q[PP * fs + d] = (P)a.inflow[3 * pl + p];
-            q[PD * fs + d] = (P)a.inflow[4 * pl + p];
-            a.T[d] = a.inflow[5 * pl + p];
-            q[PH * fs + d] = (P)a.inflow[6 * pl + p];
-            a.E[d] = a.inflow[7 * pl + p];
-            q[PG * fs + d] = (P)a.inflow[8 * pl + p];
+            // the inflow values are all loaded before the first store
+            double in[9 + NS];
 #pragma unroll
-            for (int s = 0; s < NS; s++) q[(PY + s) * fs + d] = (P)a.inflow[(9 + s) * pl + p];
+            for (int f = 0; f < 9 + NS; f++) in[f] = a.inflow[f * pl + p];
+            q[PU * fs + d] = (P)in[0];
+            q[PV * fs + d] = (P)in[1];
+            q[PW * fs + d] = (P)in[2];
+            q[PP * fs + d] = (P)in[3];
+            q[PD * fs + d] = (P)in[4];
+            a.T[d] = in[5];
+            q[PH * fs + d] = (P)in[6];
+            a.E[d] = in[7];
+            q[PG * fs + d] = (P)in[8];
+#pragma unroll
+            for (int s = 0; s < NS; s++) q[(PY + s) * fs + d] = (P)in[9 + s];
         } else {
             ghost_wall(a, q, d, L.at(2 * (L.ni + L.bc) - 1 - i, j, k), false, false);
         }
@@ -176,11 +211,14 @@ __global__ void k_wedge_band(GhostArgs a, P *q, const int4 *__restrict__ band, i
     const Layout &L = a.L;
     const long long fs = L.fs;
     const long long d = L.at(b.x, b.y, k), s = L.at(b.z, b.w, k);
-    ghost_copy(a, q, d, s);
-    const double u = (double)q[PU * fs + s], v = (double)q[PV * fs + s];
+    P w[NPRIM];
+    double T, E;
+    ghost_load(a, q, s, w, T, E);
+    const double u = (double)w[PU], v = (double)w[PV];
     const double un = u * nx + v * ny;
-    q[PU * fs + d] = (P)(u - 2.0 * un * nx);
-    q[PV * fs + d] = (P)(v - 2.0 * un * ny);
+    w[PU] = (P)(u - 2.0 * un * nx);
+    w[PV] = (P)(v - 2.0 * un * ny);
+    ghost_store(a, q, d, w, T, E);
 }
 
 // CFL: block minima of min(dx/(|U|+C), dy/(|V|+C)[, dz/(|W|+C)]) over the

@@ -251,7 +251,7 @@ void sur_predict_t(eu3d_handle *h, bool decoded, const SurQueue &qu)
         {
             ProfScope ps(h, "sur_gate");
             const SurGate g{h->gate_T, (float)h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, acount};
-            const dim3 gg(L.nj * L.nk, (L.ni + GATE_THREADS - 1) / GATE_THREADS);
+            const dim3 gg(L.nj * L.nk, (L.ni + GATE_ROW - 1) / GATE_ROW);
             k_sur_gate<P><<<gg, GATE_THREADS, 0, h->st>>>(cell_args(h), q, g, qu);
         }
         const SurSrcList<P> lsrc{L, h->T, q, h->scal, h->sur_out, h->sur_active, acount, n};

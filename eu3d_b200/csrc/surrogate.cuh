@@ -883,13 +883,17 @@ struct SurGate {
     int *acount;       // list length
 };
 
-// One block of GATE_THREADS threads per x row (of up to GATE_THREADS cells),
-// blocks over the (j, k) rows in blockIdx.x (no 65535 limit); the block
-// appends its active cells with one global atomic.  The kernel is bound by
-// instruction issue, so the per-cell work is kept small: the radical test in
-// FP32 (the primitives' precision of the benchmark path) and the audit
-// sample drawn by a multiplicative hash instead of a division.
-constexpr int GATE_THREADS = 512;
+// One block of GATE_THREADS threads per x segment of GATE_ROW cells of a row,
+// each thread taking GATE_CPT cells GATE_THREADS apart with all their loads
+// issued before the first test; blocks over the (j, k) rows in blockIdx.x
+// (no 65535 limit).  The block appends its active cells, in x order, with one
+// global atomic.  A block's life is a chain of round trips (node coordinates,
+// T and the radicals, the list atomic, the list stores), so the kernel is
+// bound by latency: four cells a thread keep four times the loads in flight
+// per resident thread.  The radical test runs in FP32 (the primitives'
+// precision of the benchmark path) and the audit sample is drawn by a
+// multiplicative hash instead of a division.
+constexpr int GATE_THREADS = 128, GATE_CPT = 4, GATE_ROW = GATE_THREADS * GATE_CPT;
 
 // deterministic sample of about one cell in `stride` (Knuth's multiplicative hash)
 __device__ __forceinline__ bool gate_sample(long long idx, unsigned stride)
@@ -902,48 +906,72 @@ __global__ void __launch_bounds__(GATE_THREADS) k_sur_gate(CellArgs a, const P *
                                                            SurQueue qu)
 {
     const Layout &L = a.L;
-    const int i = L.bc + blockIdx.y * blockDim.x + threadIdx.x;
     const int r = blockIdx.x;
     const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
-    const bool fluid = i < L.ni + L.bc && !solid_cell(a, i, j);
-    const long long c = L.at(min(i, L.ni + L.bc - 1), j, k);
-    bool frozen = false;
-    double T = 0.0;
-    if (fluid) {
-        // T and the radicals are loaded together (one memory round trip;
-        // the radicals of hot cells are read and not needed)
-        T = a.T[c];
-        float y = 0.f;
-        if (g.mask) {
+    const int i0 = L.bc + blockIdx.y * GATE_ROW + threadIdx.x;
+    bool fluid[GATE_CPT], frozen[GATE_CPT];
+    long long c[GATE_CPT];
+    double T[GATE_CPT];
 #pragma unroll
-            for (int s = 0; s < NS; s++)
-                if ((g.mask >> s) & 1u) y += fmaxf((float)q[(PY + s) * L.fs + c], 0.f);
-        }
-        frozen = T < g.T_frozen && (!g.mask || y <= g.y_max_f);
+    for (int s = 0; s < GATE_CPT; s++) {
+        const int i = i0 + s * GATE_THREADS;
+        fluid[s] = i < L.ni + L.bc && !solid_cell(a, i, j);
+        c[s] = L.at(min(i, L.ni + L.bc - 1), j, k);
     }
-    const bool active = fluid && !frozen;
-    __shared__ int wact[GATE_THREADS / 32], base_s;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const unsigned ma = __ballot_sync(0xffffffffu, active), mf = __ballot_sync(0xffffffffu, frozen);
-    __shared__ int nfrz;
-    if (threadIdx.x == 0) nfrz = 0;
-    if (lane == 0) wact[w] = __popc(ma);
-    __syncthreads();
-    if (lane == 0 && mf) atomicAdd(&nfrz, __popc(mf));
-    if (threadIdx.x == 0) {
-        int ta = 0;
-        for (int v = 0; v < nw; v++) {
-            const int n = wact[v];
-            wact[v] = ta;  // exclusive offsets
-            ta += n;
+    float y[GATE_CPT];
+#pragma unroll
+    for (int s = 0; s < GATE_CPT; s++) {
+        // T and the radicals of a cell are loaded together (the radicals of
+        // hot cells are read and not needed)
+        T[s] = 0.0;
+        y[s] = 0.f;
+        if (fluid[s]) {
+            T[s] = a.T[c[s]];
+            if (g.mask) {
+#pragma unroll
+                for (int v = 0; v < NS; v++)
+                    if ((g.mask >> v) & 1u) y[s] += fmaxf((float)q[(PY + v) * L.fs + c[s]], 0.f);
+            }
         }
+    }
+    __shared__ int wact[GATE_CPT][GATE_THREADS / 32], base_s, nfrz;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned ma[GATE_CPT];
+    int nf = 0;
+#pragma unroll
+    for (int s = 0; s < GATE_CPT; s++) {
+        frozen[s] = fluid[s] && T[s] < g.T_frozen && (!g.mask || y[s] <= g.y_max_f);
+        ma[s] = __ballot_sync(0xffffffffu, fluid[s] && !frozen[s]);
+        nf += __popc(__ballot_sync(0xffffffffu, frozen[s]));
+        if (lane == 0) wact[s][w] = __popc(ma[s]);
+    }
+    if (threadIdx.x == 0) nfrz = 0;
+    __syncthreads();
+    if (lane == 0 && nf) atomicAdd(&nfrz, nf);
+    if (threadIdx.x == 0) {
+        // exclusive offsets, cell slot outer and warp inner: the x order
+        int ta = 0;
+        for (int s = 0; s < GATE_CPT; s++)
+            for (int v = 0; v < GATE_THREADS / 32; v++) {
+                const int n = wact[s][v];
+                wact[s][v] = ta;
+                ta += n;
+            }
         base_s = ta ? atomicAdd(g.acount, ta) : 0;
     }
     __syncthreads();
     if (threadIdx.x == 0 && nfrz) atomicAdd(&a.st->sur_frozen, (unsigned long long)nfrz);
-    if (active) g.active[base_s + wact[w] + __popc(ma & ((1u << lane) - 1u))] = (int)c;
-    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
-    sur_push(qu, frozen && gate_sample(idx, (unsigned)g.audit_stride), (int)((unsigned)c | SUR_FROZEN_AUDIT), T);
+    const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+    for (int s = 0; s < GATE_CPT; s++)
+        if ((ma[s] >> lane) & 1u) g.active[base_s + wact[s][w] + __popc(ma[s] & below)] = (int)c[s];
+#pragma unroll
+    for (int s = 0; s < GATE_CPT; s++) {
+        const int i = i0 + s * GATE_THREADS;
+        const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+        sur_push(qu, frozen[s] && gate_sample(idx, (unsigned)g.audit_stride),
+                 (int)((unsigned)c[s] | SUR_FROZEN_AUDIT), T[s]);
+    }
 }
 
 // Lists every fluid interior cell (the queued adaptive chemistry's work).
