@@ -16,7 +16,9 @@ learned chemistry surrogate (value; its frozen-chemistry gate on, launch
 settings from the project's autotuner); the same steps with the plain FP64
 IMEX integrator and with the FP64 adaptive integrator (the surrogate's
 teacher) are timed on the same GPU and state and reported beside it, with
-the per-step split of chemistry and the rest, and the coupled accuracy of
+the per-step split of chemistry and the rest; so is the all-FP64 GPU path
+(FP64 reconstruction, AUSM and residual with FP64 IMEX, on a handle of its
+own, `all_fp64_imex`); and the coupled accuracy of
 the FP32-flux, surrogate and IMEX forms against the all-FP64 run (errors in
 rho, p, T and each Y_k, peak T, detonation front) on the 2D case and a
 spanwise slice of the 3D one.
@@ -66,6 +68,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-all-fp64", action="store_true", help="skip the all-FP64 IMEX arm of the headline")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--accuracy-full", action="store_true",
                     help="also compare on the benchmark's full grid (about 2.5 more minutes)")
@@ -491,6 +494,23 @@ def run_ours(a, rank, world, local):
         statuses[name] = dev.status()
         timing[name] = ms
         profs[name] = profiled(dev, step, a.steps)
+    all64 = None
+    if world == 1 and a.flux_bits == 32 and not a.no_all_fp64:
+        # the all-FP64 GPU path (FP64 reconstruction and residual, FP64 IMEX)
+        # on a handle of its own, from the same developed state
+        d64 = gpu.DeviceFlowfield(mech, grid, quirks=gpu.QUIRKS_FIXED, flux_bits=64, device=local)
+        setup_odw(d64, case)
+        extrude_state(d2, d64)
+        d64.set_time(0.0)
+        step64 = dict(base, react=gpu.REACT_IMEX)
+        ms64, _ = timed_steps(d64, step64, a.steps, W, torch, world, dist, local=local)
+        p64 = profiled(d64, step64, a.steps)
+        chem64 = sum(v[0] for k, v in p64.items() if k in CHEM_KERNELS) / a.steps
+        all64 = {"value": cells * a.steps / (ms64 * 1e-3) / 1e6, "ms_per_step": ms64 / a.steps,
+                 "split_ms_per_step": {"chemistry_ms": chem64,
+                                       "non_chemistry_ms": sum(v[0] for v in p64.values()) / a.steps - chem64},
+                 "status": {k: d64.status()[k] for k in ("nonfinite_cells", "newton_capped")}}
+        d64.close()
     hbm, tfl, src = peaks()
     prof = profs["surrogate"]
     st = statuses["surrogate"]
@@ -548,6 +568,11 @@ def run_ours(a, rank, world, local):
                                       "reach against plain IMEX with the same flux, stage and boundary kernels",
                        "note": "same GPU, same state and step; imex = the reference's one-step FP64 IMEX, "
                                "adaptive = FP64 adaptive integrator (the surrogate's teacher and fallback)"},
+        "all_fp64_imex": (dict(all64, ratio=value / all64["value"],
+                               note="the all-FP64 GPU path: FP64 reconstruction, AUSM and residual with the "
+                                    "reference's FP64 IMEX, same state and step (the imex arm above keeps the "
+                                    "FP32 flux of the timed form)")
+                          if all64 else None),
         "surrogate": {"fallback_frac": st["surrogate_fallback"] / max(tot, 1),
                       "frozen_frac": st["surrogate_frozen"] / max(tot, 1), "rejects": st["surrogate_rejects"],
                       "audited": st["surrogate_audited"], "audit_max_dT_K": st["surrogate_audit_max_dT"],

@@ -712,13 +712,15 @@ __device__ __forceinline__ void sur_push(const SurQueue &qu, bool push, int valu
 // network output, energy residual, failed decode).
 constexpr int SUR_NFLAGS = 6;
 
-template <class P, bool COUNT = true>
+// SOLID false: the caller passes fluid cells only (the gate's list), so the
+// wedge test and its node-coordinate loads are left out.
+template <class P, bool COUNT = true, bool SOLID = true>
 __device__ __forceinline__ unsigned sur_apply_cell(const SurApplyArgs &s, P *__restrict__ q, int i, int j, int k,
                                                    const float net[SUR_NOUT])
 {
     const CellArgs &a = s.a;
     const Layout &L = a.L;
-    if (solid_cell(a, i, j)) return 0u;
+    if (SOLID && solid_cell(a, i, j)) return 0u;
     const long long c = L.at(i, j, k);
     const long long fs = L.fs;
     const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
@@ -1009,7 +1011,7 @@ __global__ void __launch_bounds__(128, 7) k_sur_apply_list(SurApplyArgs s, P *__
         float o[SUR_NOUT];
 #pragma unroll
         for (int v = 0; v < SUR_NOUT; v++) o[v] = s.out[v * s.n + pos];
-        flags = sur_apply_cell<P, false>(s, q, i, j, k, o);
+        flags = sur_apply_cell<P, false, false>(s, q, i, j, k, o);  // listed cells are fluid
     }
     bc.add(flags);
     Status *st = s.a.st;
