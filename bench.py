@@ -548,7 +548,8 @@ def run_ours(a, rank, world, local):
                                       "included; the kernels skip solid cells (and the flux kernel all-solid "
                                       "tiles), so per fluid cell the rate is value x cells / fluid cells",
                    "chemistry": "learned surrogate (BF16 tcgen05 MLP) with FP64 adaptive fallback; frozen-chemistry "
-                                "gate: cells below 600 K with radicals <= 1e-6 skip the network",
+                                "gate: cells below 600 K with radicals <= 1e-6 skip the network (the gate runs "
+                                "inside the SSP-RK2 stage 2 kernel, so its time is in the non-chemistry split)",
                    "flux": f"MUSCL_2/minmod + AUSM, FP{a.flux_bits} reconstruction, FP64 state",
                    "time": f"SSP-RK2, CFL {CFL}",
                    "state": f"developed: 2D case advanced {a.develop} steps with the FP64 adaptive integrator, "

@@ -209,7 +209,6 @@ __global__ void k_wedge_band(GhostArgs a, P *q, const int4 *__restrict__ band, i
     if (n >= nband) return;
     const int4 b = band[n];
     const Layout &L = a.L;
-    const long long fs = L.fs;
     const long long d = L.at(b.x, b.y, k), s = L.at(b.z, b.w, k);
     P w[NPRIM];
     double T, E;

@@ -613,8 +613,20 @@ __device__ __forceinline__ int adapt_split_step(const CellArgs &a, long long c, 
 //  M_RK_STAGE1/2  SSP-RK2 stage updates (new); M_RK_STAGE1 is also SSP-RK3's first
 //  M_RK3_STAGE2/3 SSP-RK3 stage updates (new)
 //  M_NOCHEM  Update_after_Adv, Explicit() (Euler::DNN, src/Euler.cpp:773-780)
-template <class P, int MODE, bool SPEC>
-__device__ __forceinline__ void cell_body(const CellArgs &a, P *__restrict__ q)
+// What the SSP-RK2 stage 2 with the fused frozen-chemistry gate needs of a
+// cell (cell_body with GOUT): its index, decoded T and the FP32 sum of the
+// mass fractions of the species in `mask`, each rounded to the primitives'
+// precision first (the values the separate gate kernel loads).
+struct CellGate {
+    unsigned mask;
+    bool valid;
+    long long c;
+    double T;
+    float y;
+};
+
+template <class P, int MODE, bool SPEC, bool GOUT = false>
+__device__ __forceinline__ void cell_body(const CellArgs &a, P *__restrict__ q, CellGate *gout = nullptr)
 {
     const Layout &L = a.L;
     const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
@@ -762,6 +774,18 @@ __device__ __forceinline__ void cell_body(const CellArgs &a, P *__restrict__ q)
     a.T[c] = o.T;
     a.E[c] = o.E;
     store_prims<P>(o, q, fs, c);
+    if constexpr (GOUT) {
+        float y = 0.f;
+        if (gout->mask) {
+#pragma unroll
+            for (int s = 0; s < NS; s++)
+                if ((gout->mask >> s) & 1u) y += fmaxf((float)(P)o.Y[s], 0.f);
+        }
+        gout->valid = true;
+        gout->c = c;
+        gout->T = o.T;
+        gout->y = y;
+    }
     warp_count(&a.st->newton_capped, capped_any != 0);
     warp_count(&a.st->nonfinite, !(isfinite(o.D) && isfinite(o.T)));
 }

@@ -93,6 +93,8 @@ struct eu3d_handle {
     unsigned wait_tries = 1u << 19;  // bound of the flux ring's copy waits (eu3d_set_wait_limit)
     int adapt_queue = 0;   // FP64 adaptive chemistry on the persistent queue (1) or one thread per cell (0)
     int cell_blocks = 3;   // resident blocks per SM of the FP32-path SSP-RK2 stage updates (3 or 4)
+    int gate_fused = 1;    // surrogate with its gate: the gate runs inside SSP-RK2's stage 2 (1) or on its own (0)
+    bool sur_gated = false;  // the last stage 2 listed the active cells; the next surrogate step uses that list
     AdaptCfg acfg{0.02, 0.5, 1024};  // adaptive chemistry (EU3D_REACT_ADAPTIVE, surrogate fallback)
     double proj_eps = 1e-4;
     bool elements = false;  // element matrix loaded (eu3d_set_elements)
@@ -784,6 +786,8 @@ int ensure_stage(eu3d_handle *h, size_t bytes)
 // them unless eu3d_sdlb_pack sent some away)
 constexpr int SUR_HALF_PREDICT = 1, SUR_HALF_WORK = 2, SUR_HALF_BOTH = 3;
 int sur_chem_op(eu3d_handle *h, bool decoded, int half = SUR_HALF_BOTH);
+// SSP-RK2 stage 2 with the surrogate's frozen-chemistry gate fused in (sur_host.cuh)
+int rk2_gate_op(eu3d_handle *h);
 
 bool is_rk(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 || timeadv == EU3D_ADV_SSPRK3; }
 int rk_stages(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 ? 2 : timeadv == EU3D_ADV_SSPRK3 ? 3 : 1; }
@@ -795,6 +799,7 @@ int rk_stages(int timeadv) { return timeadv == EU3D_ADV_SSPRK2 ? 2 : timeadv == 
 int stage1_op(eu3d_handle *h, const eu3d_step_desc *s)
 {
     int rc;
+    h->sur_gated = false;
     if (is_rk(s->timeadv)) {
         if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
         return cell_op(h, M_RK_STAGE1);
@@ -808,7 +813,12 @@ int stage_op(eu3d_handle *h, const eu3d_step_desc *s, int stage)
     int rc;
     if ((rc = adv_op(h, EU3D_ADV_EE, s->diff))) return rc;
     const int mode = s->timeadv == EU3D_ADV_SSPRK2 ? M_RK_STAGE2 : stage == 2 ? M_RK3_STAGE2 : M_RK3_STAGE3;
-    if ((rc = cell_op(h, mode))) return rc;
+    // a surrogate step with its gate on lists its active cells in stage 2
+    if (mode == M_RK_STAGE2 && s->react == EU3D_REACT_SURROGATE && h->sur && h->gate_T > 0.0 && h->gate_fused)
+        rc = rk2_gate_op(h);
+    else
+        rc = cell_op(h, mode);
+    if (rc) return rc;
     if (stage == rk_stages(s->timeadv))
         CK(cudaMemsetAsync(h->rhs, 0, (size_t)NV * h->L.fs * prim_bytes(h), h->st));
     return EU3D_OK;
@@ -2117,6 +2127,7 @@ int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t)
     // left out)
     if (t->cell_blocks != 3 && t->cell_blocks != 4) return fail(EU3D_ERR_ARG, "cell_blocks must be 3 or 4");
     h->cell_blocks = t->cell_blocks;
+    h->gate_fused = t->gate_fused ? 1 : 0;
     h->adapt_queue = t->adapt_queue ? 1 : 0;
     if (h->adapt_queue) {
         int rc = ensure_cell_list(h);
@@ -2147,6 +2158,7 @@ int eu3d_get_tuning(eu3d_handle *h, eu3d_tuning *t)
     t->sur_fused = h->sur_fused;
     t->adapt_queue = h->adapt_queue;
     t->cell_blocks = h->cell_blocks;
+    t->gate_fused = h->gate_fused;
     return EU3D_OK;
 }
 
@@ -2156,7 +2168,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
     if (steps < 1) return fail(EU3D_ERR_ARG, "steps must be >= 1");
     CK(cudaSetDevice(h->dev));
     const eu3d_tuning start{h->flux_kz,   h->chem_queue,  h->queue_blocks, h->flux_stage,
-                            h->sur_fused, h->adapt_queue, h->cell_blocks};
+                            h->sur_fused, h->adapt_queue, h->cell_blocks, h->gate_fused};
     // the trials advance the state: keep a copy and put it back after each
     const size_t fs = (size_t)h->L.fs;
     const size_t nprim = (size_t)NPRIM * fs * prim_bytes(h);
@@ -2197,7 +2209,7 @@ int eu3d_autotune(eu3d_handle *h, const eu3d_step_desc *s, int steps, eu3d_tunin
                             // the stage occupancy is tuned at the default flux setting
                             if (rk2 && cb != start.cell_blocks && (fst != start.flux_stage || kz != start.flux_kz))
                                 continue;
-                            cands.push_back({kz, cq, qb, fst, start.sur_fused, ad, cb});
+                            cands.push_back({kz, cq, qb, fst, start.sur_fused, ad, cb, start.gate_fused});
                         }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);

@@ -232,8 +232,12 @@ void sur_predict_t(eu3d_handle *h, bool decoded, const SurQueue &qu)
     const Layout &L = h->L;
     const long long n = L.interior_cells();
     P *q = (P *)h->prim;
-    // [0] fallback list length, [1] its work cursor, [2] active list length
-    cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
+    // [0] fallback list length, [1] its work cursor, [2] active list length;
+    // an SSP-RK2 stage 2 with the gate fused in has listed the active cells
+    // (and the gate's audit sample) already, from counts it set to zero
+    const bool gated = h->sur_gated;
+    h->sur_gated = false;
+    if (!gated) cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st);
     // a new list: the balancing of the previous one is void until eu3d_sur_load
     h->sdlb_total = -1;
     h->sdlb_keep = 0;
@@ -248,7 +252,7 @@ void sur_predict_t(eu3d_handle *h, bool decoded, const SurQueue &qu)
         // frozen-chemistry gate: the network and its apply take the listed
         // (active) cells only
         int *acount = h->sur_count + 2;
-        {
+        if (!gated) {
             ProfScope ps(h, "sur_gate");
             const SurGate g{h->gate_T, (float)h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, acount};
             const dim3 gg(L.nj * L.nk, (L.ni + GATE_ROW - 1) / GATE_ROW);
@@ -301,6 +305,39 @@ void sur_chem_t(eu3d_handle *h, bool decoded, int half)
         ProfScope ps(h, "sur_fallback_finish");
         k_sur_fallback_finish<P, SPEC><<<FALLBACK_FINISH_BLOCKS, 128, 0, h->st>>>(cell_args(h), q, qu);
     }
+}
+
+template <class P, bool SPEC>
+void rk2_gate_t(eu3d_handle *h)
+{
+    const Layout &L = h->L;
+    const CellArgs a = cell_args(h);
+    P *q = (P *)h->prim;
+    const SurQueue qu{h->sur_list, h->sur_count, h->sur_audit, L.interior_cells(), h->sur_res, h->sur_info};
+    const SurGate g{h->gate_T, (float)h->gate_y, h->gate_mask, h->gate_audit, h->sur_active, h->sur_count + 2};
+    const dim3 grid = cell_grid(L, 128);
+    ProfScope ps(h, "cell_rk2");
+    if (sizeof(P) == 4 && h->cell_blocks == 4)
+        k_rk2_gate<P, SPEC, 4><<<grid, 128, 0, h->st>>>(a, q, g, qu);
+    else
+        k_rk2_gate<P, SPEC, 3><<<grid, 128, 0, h->st>>>(a, q, g, qu);
+}
+
+int rk2_gate_op(eu3d_handle *h)
+{
+    // the new lists start empty; the stage appends the active cells and the
+    // audit sample, and the surrogate step that follows keeps them
+    CK(cudaMemsetAsync(h->sur_count, 0, 4 * sizeof(int), h->st));
+    if (h->flux_bits == 64) {
+        if (h->spec) rk2_gate_t<double, true>(h);
+        else rk2_gate_t<double, false>(h);
+    } else {
+        if (h->spec) rk2_gate_t<float, true>(h);
+        else rk2_gate_t<float, false>(h);
+    }
+    CK(cudaGetLastError());
+    h->sur_gated = true;
+    return EU3D_OK;
 }
 
 int sur_chem_op(eu3d_handle *h, bool decoded, int half)
@@ -645,6 +682,7 @@ int eu3d_set_surrogate(eu3d_handle *h, eu3d_surrogate *s, int audit_stride)
         if (rc) return rc;
     }
     h->sur = s;
+    h->sur_gated = false;
     h->sur_audit_stride = audit_stride;
     if (s) h->elements = true;  // eu3d_sur_create loaded the element matrix on this device
     // recorded step graphs hold the previous surrogate's buffers and settings
@@ -660,6 +698,7 @@ int eu3d_set_surrogate_gate(eu3d_handle *h, double t_frozen, double y_max, unsig
     if (species_mask >> NS) return fail(EU3D_ERR_ARG, "species mask names a species past NS");
     if (audit_stride < 0) return fail(EU3D_ERR_ARG, "audit stride must be >= 0");
     h->gate_T = t_frozen;
+    h->sur_gated = false;
     h->gate_y = y_max;
     h->gate_mask = species_mask;
     h->gate_audit = audit_stride;

@@ -976,6 +976,39 @@ __global__ void __launch_bounds__(GATE_THREADS) k_sur_gate(CellArgs a, const P *
     }
 }
 
+// SSP-RK2 stage 2 with the frozen-chemistry gate fused into it (tuning
+// gate_fused): the stage update and decode of k_cell<M_RK_STAGE2>, then the
+// gate's test on the T and radicals the decode just produced, each warp's
+// active cells appended to the list in x order with one global atomic, and
+// the hashed audit sample of frozen cells pushed to the fallback list -- the
+// separate gate kernel's decisions and list (in another order), without
+// reading T and the radicals back from memory.  Every lane reaches its
+// warp's append (cell_body returns to this kernel for cells past the row or
+// in the wedge).
+template <class P, bool SPEC, int NB>
+__global__ void __launch_bounds__(128, NB) k_rk2_gate(CellArgs a, P *__restrict__ q, SurGate g, SurQueue qu)
+{
+    CellGate gc{g.mask, false, 0, 0.0, 0.f};
+    cell_body<P, M_RK_STAGE2, SPEC, true>(a, q, &gc);
+    const Layout &L = a.L;
+    const int i = L.bc + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = L.bc + blockIdx.y, k = L.bc + blockIdx.z;
+    const bool frozen = gc.valid && gc.T < g.T_frozen && (!g.mask || gc.y <= g.y_max_f);
+    const bool active = gc.valid && !frozen;
+    // one list atomic per warp, no block barrier: a barrier would hold every
+    // warp of the block for the slowest decode and the atomic's round trip
+    const int lane = threadIdx.x & 31;
+    const unsigned ma = __ballot_sync(0xffffffffu, active), mf = __ballot_sync(0xffffffffu, frozen);
+    if (lane == 0 && mf) atomicAdd(&a.st->sur_frozen, (unsigned long long)__popc(mf));
+    int base = 0;
+    if (lane == 0 && ma) base = atomicAdd(g.acount, __popc(ma));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (active) g.active[base + __popc(ma & ((1u << lane) - 1u))] = (int)gc.c;
+    const long long idx = ((long long)(k - L.bc) * L.nj + (j - L.bc)) * L.ni + (i - L.bc);
+    sur_push(qu, frozen && gate_sample(idx, (unsigned)g.audit_stride), (int)((unsigned)gc.c | SUR_FROZEN_AUDIT),
+             gc.T);
+}
+
 // Lists every fluid interior cell (the queued adaptive chemistry's work).
 __global__ void __launch_bounds__(256) k_list_fluid(CellArgs a, SurQueue qu)
 {

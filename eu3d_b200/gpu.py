@@ -91,7 +91,8 @@ class Status(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("flux_kz", C.c_int), ("chem_queue", C.c_int), ("queue_blocks", C.c_int), ("flux_stage", C.c_int),
-                ("sur_fused", C.c_int), ("adapt_queue", C.c_int), ("cell_blocks", C.c_int)]
+                ("sur_fused", C.c_int), ("adapt_queue", C.c_int), ("cell_blocks", C.c_int),
+                ("gate_fused", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -477,8 +478,10 @@ class DeviceFlowfield:
         return t.as_dict()
 
     def set_tuning(self, flux_kz=None, chem_queue=None, queue_blocks=None, flux_stage=None, sur_fused=None,
-                   adapt_queue=None, cell_blocks=None):
+                   adapt_queue=None, cell_blocks=None, gate_fused=None):
         t = Tuning(**self.tuning())
+        if gate_fused is not None:
+            t.gate_fused = 1 if gate_fused else 0
         if cell_blocks is not None:
             t.cell_blocks = int(cell_blocks)
         if adapt_queue is not None:

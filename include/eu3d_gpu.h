@@ -314,7 +314,11 @@ int eu3d_sdlb_unpack(eu3d_handle *h, const double *dev_back);
    with refill; 0 (default): one thread per cell.  cell_blocks (3, default,
    or 4): resident blocks of 128 threads per SM the SSP-RK2 stage updates of
    the FP32-flux path are compiled for (more blocks, fewer registers a
-   thread; the same results).  Changing them drops the recorded step graphs. */
+   thread; the same results).  gate_fused (1, default): in an SSP-RK2 step
+   with the learned chemistry and its frozen-chemistry gate on, the gate runs
+   inside stage 2 on the state the stage has just decoded, instead of as a
+   kernel of its own that reads T and the radicals back (0); the same list
+   and results.  Changing them drops the recorded step graphs. */
 typedef struct {
     int flux_kz;
     int chem_queue;
@@ -323,6 +327,7 @@ typedef struct {
     int sur_fused;
     int adapt_queue;
     int cell_blocks;
+    int gate_fused;
 } eu3d_tuning;
 int eu3d_set_tuning(eu3d_handle *h, const eu3d_tuning *t);
 /* Bound of the waits of the TMA-fed flux kernel for its plane copies (new), in

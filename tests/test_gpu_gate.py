@@ -139,3 +139,34 @@ def test_gate_argument_errors(mech):
     with pytest.raises(gpu.Eu3dError):
         d.set_surrogate_gate(600.0, 1e-6, audit_stride=-1)
     d.close()
+
+
+@pytest.mark.parametrize("flux_bits", [32, 64])
+def test_gate_fused_into_stage2_equals_gate_kernel(mech, flux_bits):
+    """The gate inside SSP-RK2's stage 2 (tuning gate_fused 1, the default)
+    takes the separate gate kernel's decisions on the state the stage has
+    just decoded: the same counts (accepted, fallen back, rejected, audited,
+    frozen) and the same state after three coupled steps."""
+    case = odw_case(mech, 160, 64, 3, L=0.05)
+    model = S.SurrogateModel.load(S.DEFAULT_MODEL)
+    gate = dict(S.GATE, audit_stride=7)
+    out = []
+    for fused in (0, 1):
+        d = _developed(mech, case, flux_bits)
+        d.set_tuning(gate_fused=fused)
+        assert d.tuning()["gate_fused"] == fused
+        s = model.attach(d, 0, gate=gate)
+        d.reset_status()
+        d.run(3, react=gpu.REACT_SURROGATE, **KW)
+        d.synchronize()
+        out.append(({f: d.download(f) for f in ("CS", "T", "E", "P", "Yi")}, d.status()))
+        d.set_surrogate(None)
+        s.close()
+        d.close()
+    (a, sa), (b, sb) = out
+    assert sa["surrogate_frozen"] > 0 and sa["frozen_audited"] > 0 and sa["surrogate_cells"] > 0, sa
+    for k in ("surrogate_cells", "surrogate_fallback", "surrogate_rejects", "surrogate_audited", "surrogate_frozen",
+              "frozen_audited", "frozen_audit_max_dT", "nonfinite_cells", "newton_capped"):
+        assert sa[k] == sb[k], k
+    for f in a:
+        assert np.array_equal(a[f], b[f]), f
