@@ -69,6 +69,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-all-fp64", action="store_true", help="skip the all-FP64 IMEX arm of the headline")
+    ap.add_argument("--tuning", default="",
+                    help="fixed launch settings instead of the autotuner, e.g. flux_kz=64,cell_blocks=4")
     ap.add_argument("--accuracy-steps", type=int, default=2000)
     ap.add_argument("--accuracy-full", action="store_true",
                     help="also compare on the benchmark's full grid (about 2.5 more minutes)")
@@ -478,7 +480,13 @@ def run_ours(a, rank, world, local):
 
     W = max(a.warmup, 3)
     tuned = None
-    if world == 1:
+    if a.tuning:
+        # fixed launch settings instead of the autotuner (a profiler's
+        # serialised launches would mislead the autotuner's timing)
+        fixed = {k: int(v) for k, v in (kv.split("=") for kv in a.tuning.split(","))}
+        dev.set_tuning(**fixed)
+        tuned = {"setting": dev.tuning(), "fixed": True}
+    elif world == 1:
         # the project's autotuner picks the flux tile depth and kernel on this
         # state (restored after every trial), outside the timed region
         reset()
