@@ -251,6 +251,8 @@ __device__ __forceinline__ void cfl_speeds(float D, float Pp, float G, float U, 
     az = (double)__fadd_rn(fabsf(W), C);
 }
 
+constexpr int CFL_U = 4;  // cells a lane has in flight in k_cfl_partial
+
 template <class P>
 __global__ void k_cfl_partial(Layout L, const P *__restrict__ q, int use_z, const double *__restrict__ xn,
                               const double *__restrict__ yn, double x0, double y0, double tn, int wedge_on,
@@ -264,19 +266,39 @@ __global__ void k_cfl_partial(Layout L, const P *__restrict__ q, int use_z, cons
         const int j = L.bc + r % L.nj, k = L.bc + r / L.nj;
         const double y = yn[j];
         const long long base = L.at(0, j, k);
-        for (int i = L.bc + lane; i < L.ni + L.bc; i += 32) {
-            if (wedge_on) {
-                const double x = xn[i];
-                if (x > x0 && (y - y0) < (x - x0) * tn) continue;
+        // CFL_U cells a lane at a time, all their loads issued before the
+        // first speed is formed (the maxima do not depend on the order)
+        for (int i0 = L.bc + lane; i0 < L.ni + L.bc; i0 += 32 * CFL_U) {
+            bool ok[CFL_U];
+            P vd[CFL_U], vp[CFL_U], vg[CFL_U], vu[CFL_U], vv[CFL_U], vw[CFL_U];
+#pragma unroll
+            for (int u = 0; u < CFL_U; u++) {
+                const int i = i0 + 32 * u;
+                ok[u] = i < L.ni + L.bc;
+                if (ok[u] && wedge_on) {
+                    const double x = xn[i];
+                    ok[u] = !(x > x0 && (y - y0) < (x - x0) * tn);
+                }
+                if (ok[u]) {
+                    const long long c = base + i;
+                    vd[u] = q[PD * fs + c];
+                    vp[u] = q[PP * fs + c];
+                    vg[u] = q[PG * fs + c];
+                    vu[u] = q[PU * fs + c];
+                    vv[u] = q[PV * fs + c];
+                    vw[u] = q[PW * fs + c];
+                }
             }
-            const long long c = base + i;
-            double ax, ay, az;
-            cfl_speeds(q[PD * fs + c], q[PP * fs + c], q[PG * fs + c], q[PU * fs + c], q[PV * fs + c],
-                       q[PW * fs + c], ax, ay, az);
-            if (isnan(ax)) continue;
-            sx = fmax(sx, ax);
-            sy = fmax(sy, ay);
-            if (use_z) sz = fmax(sz, az);
+#pragma unroll
+            for (int u = 0; u < CFL_U; u++) {
+                if (!ok[u]) continue;
+                double ax, ay, az;
+                cfl_speeds(vd[u], vp[u], vg[u], vu[u], vv[u], vw[u], ax, ay, az);
+                if (isnan(ax)) continue;
+                sx = fmax(sx, ax);
+                sy = fmax(sy, ay);
+                if (use_z) sz = fmax(sz, az);
+            }
         }
     }
     __shared__ double sm[3][32];
